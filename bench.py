@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""SCFT inner-loop benchmark: iterations/s on the 128^3, Ns = 200 diblock workload.
+
+Workload (one step = one SCFT iteration): AB diblock melt, 128^3 grid, box
+8.0 Rg, f_A = 0.35, chiN = 25, Ns = 200 (70 + 130 contour steps per sweep, two
+sweeps), Anderson mixing of depth 10, mixed precision (FP32 propagators and
+FFTs; FP64 Q, F, quadrature and Anderson normal equations).  Synthetic seeded
+fields (U(-0.05, 0.05) plus a hexagonal-cylinder seed).
+
+Our arm prints one JSON line with the device-timed whole-job rate (`value`),
+the end-to-end rate through the public API with host buffers (`e2e`), the
+roofline of the propagator step (CUDA events around the sweeps inside the
+timed iterations), the CPU baseline (the FP64 oracle on the host cores) and
+the SM clocks sampled during the timed region.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+For N > 1 each rank runs an independent replica (the single-instance path
+does not shard; weak scaling), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "SCFT iter/s at 128³ Ns=200: mixed vs FP64 at |ΔF/F|<1e-6; % HBM roofline"
+UNIT = "iter/s"
+WORKLOAD = ("diblock128: AB diblock melt 128^3, box 8.0 Rg, f_A=0.35, chiN=25, Ns=200, "
+            "Anderson depth 10, mixed precision")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="grid extent (128 is the benchmark)")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(n: int, precision: str):
+    """DRAM bytes per propagator step from the committed ncu summary, or None."""
+    f = ROOT / "profiles" / f"propagator_step_{n}cubed_{precision}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_step:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = [r.split(",") for r in Path(self.tmp.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_config(n: int):
+    from polyswift_plusplus_b200 import workloads as W
+    cfg, w = W.diblock128(precision="fp64", n=n)
+    return cfg, w
+
+
+def cpu_baseline_full_iteration(n: int) -> dict:
+    """One full FP64 oracle iteration of the same workload on all host threads."""
+    import oracle as O
+    threads = O.set_threads(cpu_threads())
+    cfg, w = oracle_config(n)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    t0 = time.perf_counter()
+    o.update(1)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one full FP64 iteration of the {n}^3 workload ({dt:.2f} s wall) by the C "
+                      "restatement of the reference dataflow (c2c FFT pairs, OpenMP)"}
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU path (its C restatement; the reference itself cannot be built)."""
+    if world > 1 and rank != 0:
+        return
+    import oracle as O
+    threads = O.set_threads(cpu_threads())
+    cfg, w = oracle_config(args.n)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.update(1)                        # warm-up: one full iteration, gives the non-sweep time
+    t_sweeps, t_total = o.last_timing()
+    t_rest = max(t_total - t_sweeps, 0.0)
+    steps_per_iter = sum(o.block_steps(0, b) for b in range(len(cfg.polymers[0].blocks))) * 2
+    chunk = 16
+    for _ in range(args.warmup):
+        o.propagate_sample(chunk)
+    samples = [o.propagate_sample(chunk) for _ in range(args.steps)]
+    per_step = statistics.mean(samples) / chunk
+    t_iter = steps_per_iter * per_step + t_rest
+    value = 1.0 / t_iter
+    sample = (f"each timed step = {chunk} of the {steps_per_iter} propagator steps of one FP64 "
+              f"iteration (c2c FFT pairs); quadrature + field update ({t_rest:.3f} s) timed once "
+              f"in warm-up and added per iteration")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(samples),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {"workload": WORKLOAD.replace("mixed precision", "FP64"),
+                                           "grid": args.n, "ns": 200},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftSolver
+
+    torch.cuda.set_device(local)
+    cfg, w = W.diblock128(precision=args.precision, n=args.n)
+    cfg.device = local
+    solver = ScftSolver(cfg)
+    solver.restore(w)
+    stream = torch.cuda.ExternalStream(solver.stream_ptr, device=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    def max_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (first iteration runs eagerly, the second captures the graph)
+    solver.update(args.warmup)
+    solver.enable_sweep_timing(args.steps)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.update(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_ranks(e0.elapsed_time(e1))
+    value = world * args.steps / (ms / 1000.0)
+    sweep_ms, sweep_bytes, sweep_steps = solver.sweep_timing()
+    launches = solver.launches_per_iteration * args.steps
+
+    # end to end through the public API: host (pinned) fields in, scalars out, every step
+    n_e2e = max(1, min(args.e2e_steps, args.steps))
+    N = cfg.n_total
+    host_w = [torch.from_numpy(x.copy()).pin_memory() for x in w]
+    host_p = torch.zeros(N, dtype=torch.float64).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    last = None
+    for _ in range(n_e2e):
+        for i, hw in enumerate(host_w):
+            solver.set_field(0, i, hw)
+        solver.set_field(2, 0, host_p)
+        solver.update(1)
+        last = solver.scalars()
+    f1.record(stream)
+    f1.synchronize()
+    barrier()
+    ms_e2e = max_ranks(f0.elapsed_time(f1))
+    e2e_value = world * n_e2e / (ms_e2e / 1000.0)
+    h2d = (len(host_w) + 1) * N * 8
+    d2h = 120  # sizeof(ps_scalars)
+
+    peak, peak_kind = peaks()
+    mean_sweep = statistics.mean(sweep_ms) if sweep_ms else float("nan")
+    achieved = sweep_bytes / (mean_sweep / 1000.0) / 1e9 if sweep_ms else None
+    per_step_ms = mean_sweep / max(sweep_steps, 1)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": profile_traffic(args.n, args.precision),
+                "kernel": "propagator step (plane_kernel + pencil_kernel per step of every sweep)",
+                "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                "algorithmic_bytes_per_step": 3 * N * (4 if args.precision == "mixed" else 8),
+                "step_us": per_step_ms * 1000.0, "samples": len(sweep_ms)}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 propagators + f64 reductions" if args.precision == "mixed" else "f64",
+           "data": "synthetic",
+           "config": {"workload": WORKLOAD if args.precision == "mixed" else
+                      WORKLOAD.replace("mixed precision", "FP64"),
+                      "grid": args.n, "ns": 200, "precision": args.precision, "updater": "anderson10",
+                      "parallelism": f"replicas x{world}",
+                      "l2": "inputs larger than L2: 3.4 GB of propagator slices per iteration"},
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h},
+           "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+           "free_energy": last["free_energy"] if last else None}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_full_iteration(args.n)
+    solver.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

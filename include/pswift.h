@@ -1,0 +1,204 @@
+/*
+ * pswift.h -- C-ABI of the B200 SCFT inner loop (PolySwift++ hot path).
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross this boundary and no C++ exception escapes it.  Fields cross the
+ * boundary as contiguous row-major (x slowest, z fastest) arrays of double,
+ * whatever precision the device path computes in.  Status codes mirror the
+ * reference's PS_ERR codes (polyswift/polyswift/polyswift.cxx:115-125).
+ *
+ * Reference interfaces replaced (paths inside the PolySwift++ tree):
+ *   ps_gpu_create          PsDomain::buildData/buildSolvers      pstrol/PsDomain.cpp:207-285
+ *   ps_gpu_set_fields      PsPhysFldFuncs::restore (dens, conj)  psphysf/PsPhysFldFuncs.cpp:150-166
+ *   ps_gpu_init_random     PsMonomerDens::initialize "random"    psphysf/PsMonomerDens.cpp:116-127
+ *   ps_gpu_iterate         PsDomain::update(t)                   pstrol/PsDomain.cpp:332-372
+ *                          (PsBlockCopolymer::update pspolymer/PsBlockCopolymer.cpp:189-239 +
+ *                           PsSteepDUpdater::update pseffhamil/PsSteepDUpdater.cpp:159-203)
+ *   ps_gpu_get_scalars     PsPolymerUpdater::getFreeE / PsBlockCopolymer::getLogBigQ
+ *                          pseffhamil/PsPolymerUpdater.h:124, pspolymer/PsBlockCopolymer.h:114-116
+ *   ps_gpu_get_propagator  PsBlock qs/qts storage                pspolymer/PsBlock.cpp:131-134
+ *   ps_fft_scaled_pair     PsFFTBase::scaledFFTPair              psbase/PsFFTBase.h:105,
+ *                                                               psfft/PsFFTW.cpp:196-224
+ */
+#ifndef PSWIFT_H
+#define PSWIFT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_MAX_BLOCKS 8
+#define PS_MAX_JOINS 4
+#define PS_MAX_POLYMERS 4
+#define PS_MAX_FIELDS 4
+#define PS_MAX_INTERACTIONS 6
+
+/* Status codes: same numbers as the reference's quitPolyswift() codes. */
+enum {
+  PS_OK = 0,
+  PS_ATTRIB_ERR = 3, /* bad attribute / configuration                    */
+  PS_RUN_ERR = 4,    /* NaN/Inf in Q or F (PsBlock::calcBigQ throw)      */
+  PS_INPUT_ERR = 6,  /* block steps, fractions, unsupported grid         */
+  PS_GPU_ERR = 7     /* CUDA error or missing device                     */
+};
+
+/* Arithmetic of the propagator sweeps.  Q, F, the contour quadrature and the
+ * field update are FP64 in both modes. */
+enum { PS_PREC_FP64 = 0, PS_PREC_MIXED = 1 };
+
+/* Updater kinds: "steepestDescent" (pseffhamil/PsSteepDUpdater.cpp) and
+ * Anderson mixing (added; the reference has no Anderson updater). */
+enum { PS_UPD_STEEPEST = 0, PS_UPD_ANDERSON = 1 };
+
+/* Field selectors for get/set: conjugate field w_i, density phi_i, pressure p. */
+enum { PS_FIELD_W = 0, PS_FIELD_PHI = 1, PS_FIELD_PRES = 2 };
+
+/* Block end selectors for propagator access. */
+enum { PS_FROM_HEAD = 0, PS_FROM_TAIL = 1 };
+
+/* <Block name> kind = flexPseudoSpec (psbase/PsBlockBase.cpp:67-145,
+ * pspolymer/PsFlexPseudoSpec.cpp:58-82). */
+typedef struct ps_block_config {
+  int field;               /* scfield: index of the monomerDens PhysField   */
+  double lengthfrac;       /* lengthfrac                                    */
+  double ds;               /* ds                                            */
+  double bseg_ratio;       /* bSegRatio (1.0 by default)                    */
+  int force_block_steps;   /* forceBlockSteps option                        */
+  int n_head;              /* number of entries in head_joined (0 = freeEnd)*/
+  int n_tail;              /* number of entries in tail_joined (0 = freeEnd)*/
+  int head_joined[PS_MAX_JOINS]; /* block indices inside the same polymer   */
+  int tail_joined[PS_MAX_JOINS];
+} ps_block_config;
+
+/* <Polymer name> kind = blockCopolymer (psbase/PsPolymer.cpp:42-73). */
+typedef struct ps_polymer_config {
+  double volfrac;          /* volfrac                                       */
+  int length;              /* length (statistical units)                    */
+  int n_blocks;
+  ps_block_config blocks[PS_MAX_BLOCKS];
+} ps_polymer_config;
+
+/* <Interaction name> kind = flory (pseffhamil/PsFloryInteraction.cpp:65-89). */
+typedef struct ps_interaction_config {
+  int field_a;             /* scfields[0]                                   */
+  int field_b;             /* scfields[1]                                   */
+  double chi;              /* chi; chiN = chi * length of the first polymer */
+} ps_interaction_config;
+
+/* <Updater name> (pseffhamil/PsSteepDUpdater.cpp:47-76). */
+typedef struct ps_updater_config {
+  int kind;                /* PS_UPD_STEEPEST or PS_UPD_ANDERSON            */
+  double lambda0;          /* relaxlambdas[0]                               */
+  double lambda1;          /* relaxlambdas[1]                               */
+  double noise;            /* noise (Gaussian strength)                     */
+  int anderson_depth;      /* history depth m (Anderson only)               */
+  double anderson_mix;     /* mixing applied to the combined residual       */
+  int anderson_start;      /* plain steps before the history is used        */
+} ps_updater_config;
+
+typedef struct ps_config {
+  int n[3];                /* numCellsGlobal                                */
+  double cell[3];          /* cellSizes (Rg units)                          */
+  int precision;           /* PS_PREC_FP64 or PS_PREC_MIXED                 */
+  int n_fields;            /* monomerDens PhysFields (2 or 3)               */
+  int n_polymers;
+  ps_polymer_config polymers[PS_MAX_POLYMERS];
+  int n_interactions;
+  ps_interaction_config interactions[PS_MAX_INTERACTIONS];
+  ps_updater_config updater;
+  unsigned long long seed; /* randomSeed (MT19937 init_genrand(seed+rank)) */
+  int calc_disorder;       /* History freeEnergy calcDisorder (default 1)   */
+  int device;              /* CUDA device ordinal                           */
+} ps_config;
+
+typedef struct ps_scalars {
+  double free_energy;        /* sumFe, disorder term subtracted            */
+  double free_energy_nodis;  /* sumFeNoDis                                 */
+  double log_q[PS_MAX_POLYMERS];
+  double q[PS_MAX_POLYMERS];
+  double max_incomp;         /* max_r |sum_i phi_i(r) - 1|                 */
+  double dh_norm;            /* sqrt(mean_r sum_i dH_i(r)^2)               */
+  double pressure_mean;      /* mean removed from p by updatePres          */
+  long long iteration;       /* number of completed iterations             */
+  int error_flags;           /* bit 0: non-finite Q, bit 1: non-finite F   */
+} ps_scalars;
+
+typedef struct ps_handle ps_handle;
+typedef struct ps_fft ps_fft;
+
+/* Library version string. */
+const char* ps_version(void);
+
+/* Message for the last error of a handle (or of the calling thread when the
+ * handle is NULL, e.g. after a failed create). */
+const char* ps_gpu_last_error(const ps_handle* h);
+
+/* Build the device state for one SCFT instance.  Performs the reference's
+ * setAttrib/buildData/buildSolvers checks: block-step rounding, sum of length
+ * fractions, sum of volume fractions, supported grid extents. */
+int ps_gpu_create(const ps_config* cfg, ps_handle** out);
+int ps_gpu_destroy(ps_handle* h);
+
+/* Number of contour steps a block takes (PsBlockBase::setBlockSteps). */
+int ps_gpu_block_steps(const ps_handle* h, int polymer, int block, int* steps);
+
+/* Copy a field in or out.  which = PS_FIELD_W / PS_FIELD_PHI (index = field)
+ * or PS_FIELD_PRES (index ignored).  on_device != 0: data is a device pointer
+ * on the handle's device.  Sizes are n[0]*n[1]*n[2] doubles. */
+int ps_gpu_set_fields(ps_handle* h, int which, int index, const double* data, int on_device);
+int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_device);
+
+/* Reference initialisation: every monomerDens w_i = U[0,1) - 0.5 drawn from
+ * MT19937 seeded with cfg->seed, fields in declaration order; p = 0. */
+int ps_gpu_init_random(ps_handle* h);
+
+/* Run n_iter SCFT iterations (PsDomain::update order). */
+int ps_gpu_iterate(ps_handle* h, int n_iter);
+
+/* Scalars of the last completed iteration (copies a few doubles to host). */
+int ps_gpu_get_scalars(ps_handle* h, ps_scalars* out);
+
+/* Read one stored propagator slice q(r, s_n) of a block: end = PS_FROM_HEAD
+ * gives qs[n], PS_FROM_TAIL gives qts[n] (values of the last iteration). */
+int ps_gpu_get_propagator(ps_handle* h, int polymer, int block, int end, int n,
+                          double* out);
+
+/* Wait for all work of the handle (stream synchronise). */
+int ps_gpu_synchronize(ps_handle* h);
+
+/* Number of this library's kernel launches one iteration issues (0 before the
+ * first iteration).  No reference counterpart: launch accounting for benchmarks. */
+long long ps_gpu_launches_per_iteration(const ps_handle* h);
+
+/* Sweep timing (no reference counterpart; the reference only times whole
+ * updates, polyswift/polyswift/polyswift.cxx:540-600).  After enabling, the
+ * next max_samples iterations record CUDA events on the handle's stream
+ * around their propagator sweeps.  ps_gpu_sweep_timing returns those
+ * durations in ms (and clears them), the algorithmic bytes of one iteration's
+ * sweeps (3 * N * sizeof(slice element) per propagator step) and the number
+ * of propagator steps per iteration. */
+int ps_gpu_enable_sweep_timing(ps_handle* h, int max_samples);
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or events against the handle's iterations. */
+void* ps_gpu_stream(const ps_handle* h);
+int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
+                        double* bytes_per_iter, long long* steps_per_iter);
+
+/* --- FFT plugin: PsFFTBase<T,3>::scaledFFTPair with host pointers ---------
+ * res = Re(IFFT(kdata * FFT(data))), both transforms unnormalised, as the
+ * reference's FFTW c2c pair.  Inputs and outputs are host arrays of n[0]*n[1]*n[2]
+ * doubles; the call copies them over PCIe (a correct plugin, not the fast path). */
+int ps_fft_create(const int n[3], int precision, int device, ps_fft** out);
+int ps_fft_destroy(ps_fft* f);
+int ps_fft_size(const ps_fft* f, size_t* n_total);
+int ps_fft_scaled_pair(ps_fft* f, const double* data, const double* kdata, double* res);
+/* Message for the last FFT-plugin error of the calling thread. */
+const char* ps_fft_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSWIFT_H */

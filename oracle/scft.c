@@ -1,0 +1,924 @@
+/*
+ * FP64 CPU restatement of the PolySwift++ SCFT inner loop (TEST INFRASTRUCTURE).
+ *
+ * PARITY UNPINNED: the reference cannot be built here and ships no golden
+ * data; this file restates its algorithm from the sources and is checked by
+ * known-answer tests and an independent numpy restatement.  It is loaded only
+ * by tests, by the smoke check and by the benchmark's CPU-baseline leg.
+ *
+ * One update(t) follows pstrol/PsDomain.cpp:332-372:
+ *   phi_i = 0                                   psphysf/PsMonomerDens.cpp:105-110,167-171
+ *   PsBlockCopolymer::update                    pspolymer/PsBlockCopolymer.cpp:189-239
+ *     reset: wfac = exp(-ds/2 w)                pspolymer/PsFlexPseudoSpec.cpp:158-181
+ *     dependency-driven solveQ / publishQFrom   pspolymer/PsBlockCopolymer.cpp:248-313
+ *     solveQ step loop                          pspolymer/PsFlexPseudoSpec.cpp:244-293
+ *     Q = <qHeadInitial qHeadFinal>             pspolymer/PsBlock.cpp:205-237
+ *     Simpson (0.33333) + trapezoid tail        pspolymer/PsBlock.cpp:256-380
+ *     phi += vf/alpha * qqt                     pspolymer/PsBlock.cpp:154-196
+ *   PsSteepDUpdater::update                     pseffhamil/PsSteepDUpdater.cpp:159-203
+ *     dH_i = p - w_i + sum chiN(phi_j - avg_j)  :174-184, :208-236,
+ *                                               pseffhamil/PsFloryInteraction.cpp:204-269
+ *     w update, noise, pressure (2 / 3 fields)  :250-333, :350-453,
+ *                                               pseffhamil/PsPolymerUpdater.cpp:244-295
+ *     p -= mean(p)                              psphysf/PsConstraint.cpp:184-262
+ *     F with the updated w                      pseffhamil/PsPolymerUpdater.cpp:173-226,303-341,
+ *                                               pseffhamil/PsFloryInteraction.cpp:275-321
+ * Bulk systems only: the constraint field phi0 is identically zero (no walls
+ * or particles), so every mask is 1 and every volume is N.
+ *
+ * Anderson mixing has no counterpart in the reference; it is restated here
+ * from the published method (D. G. Anderson 1965; as used for SCFT by
+ * R. B. Thompson et al. 2004 and M. W. Matsen 2009) in exactly the form the
+ * device updater uses (Gram-matrix normal equations, partial-pivot solve).
+ */
+#define _POSIX_C_SOURCE 199309L
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mt19937.h"
+#include "oracle.h"
+
+void oracle_fftnd_inplace(const int n[3], double* c, int sign);
+void oracle_scaled_pair_buf(const int n[3], const double* data, const double* kdata,
+                            double* res, double* c);
+
+enum { HEAD = 0, TAIL = 1 };
+
+typedef struct oblock {
+  ps_block_config cfg;
+  int steps;
+  /* connections: index of the joined block and the joined end of that block */
+  int ncnt[2];
+  int cnt_idx[2][PS_MAX_JOINS];
+  int cnt_end[2][PS_MAX_JOINS];
+  /* junction maps keyed by the joined block index (std::map order = ascending) */
+  int njnt[2];
+  int jnt_key[2][PS_MAX_JOINS];
+  int jnt_set[2][PS_MAX_JOINS];
+  double* jnt_q[2][PS_MAX_JOINS];
+  double* q_init[2];
+  double* q_final[2];
+  int init_set[2];
+  int final_set[2];
+  double* qs;  /* solved from HEAD: (steps+1) slices */
+  double* qts; /* solved from TAIL */
+  double* wfac;
+  double* k2;
+  double* qqt;
+} oblock;
+
+typedef struct opolymer {
+  ps_polymer_config cfg;
+  double length_ratio;
+  int nb;
+  oblock b[PS_MAX_BLOCKS];
+  double bigq;
+} opolymer;
+
+struct oracle_state {
+  ps_config cfg;
+  int n[3];
+  long N;
+  int nf;
+  double* w[PS_MAX_FIELDS];
+  double* phi[PS_MAX_FIELDS];
+  double* p;
+  double dens_avg[PS_MAX_FIELDS];
+  double chin[PS_MAX_INTERACTIONS];
+  int npol;
+  opolymer pol[PS_MAX_POLYMERS];
+  double scale_length;
+  mt_state rng;
+  long long iter;
+  /* scratch */
+  double* cwork;  /* 2N complex scratch for the FFT pair */
+  double* qw;
+  double* res;
+  double* dh[PS_MAX_FIELDS];
+  /* Anderson history (ring of depth m+1) */
+  int am_m;
+  double* am_w;   /* (m+1) * nf * N */
+  double* am_d;   /* (m+1) * nf * N */
+  double* am_g;   /* (m+1)^2 Gram matrix indexed by ring slots */
+  long long am_k;
+  /* wall time of the last iteration: propagator sweeps and total (seconds) */
+  double t_sweeps;
+  double t_total;
+};
+
+#include <time.h>
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static void* xcalloc(size_t n, size_t sz) {
+  void* p = calloc(n ? n : 1, sz);
+  if (!p) { fprintf(stderr, "oracle: out of memory\n"); abort(); }
+  return p;
+}
+
+/* PsBlockBase::setBlockSteps (psbase/PsBlockBase.cpp:252-326). */
+static int set_block_steps(double bs, int force, int* out, char* err, int errlen) {
+  long bsint;
+  double intpart = (double)((long)bs);
+  double dx = bs - intpart;
+  if (force) {
+    bsint = (long)floor(bs + 0.5);
+  } else {
+    if ((dx > 0.0001) && (dx < 0.9999)) {
+      snprintf(err, errlen, "non-integer # of block steps: blockSteps = %.17g", bs);
+      return PS_INPUT_ERR;
+    }
+    long c = (long)ceil(bs), f = (long)floor(bs);
+    if (c == f) bsint = c;
+    else if (fabs(bs - (double)c) < fabs(bs - (double)f)) bsint = c;
+    else bsint = f;
+  }
+  if (bsint < 4) {
+    snprintf(err, errlen, "# of block steps too small: %ld < 4", bsint);
+    return PS_INPUT_ERR;
+  }
+  *out = (int)bsint;
+  return PS_OK;
+}
+
+/* PsGridField::calck2 (psbase/PsGridField.cpp:66-104) then
+ * PsFlexPseudoSpec::build_k2 (pspolymer/PsFlexPseudoSpec.cpp:188-206). */
+static void build_k2(const oracle_state* s, const oblock* b, double* k2) {
+  const double twopi = 2.0 * acos(-1.0);
+  double n2[3];
+  for (int d = 0; d < 3; ++d) n2[d] = (double)s->n[d] / 2.0;
+  long idx = 0;
+  for (int i = 0; i < s->n[0]; ++i)
+    for (int j = 0; j < s->n[1]; ++j)
+      for (int k = 0; k < s->n[2]; ++k) {
+        double nk2 = n2[2] - fabs((double)k - n2[2]);
+        double nk1 = n2[1] - fabs((double)j - n2[1]);
+        double nk0 = n2[0] - fabs((double)i - n2[0]);
+        double kv2 = twopi * nk2 / (double)s->n[2];
+        double kv1 = twopi * nk1 / (double)s->n[1];
+        double kv0 = twopi * nk0 / (double)s->n[0];
+        kv2 = kv2 / s->cfg.cell[2];
+        kv1 = kv1 / s->cfg.cell[1];
+        kv0 = kv0 / s->cfg.cell[0];
+        double k2val = kv0 * kv0 + kv1 * kv1 + kv2 * kv2;
+        k2[idx++] = exp(-1.0 * b->cfg.ds * k2val * b->cfg.bseg_ratio * b->cfg.bseg_ratio);
+      }
+}
+
+int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errlen) {
+  char dummy[8];
+  if (!err) { err = dummy; errlen = (int)sizeof(dummy); }
+  *out = NULL;
+  if (cfg->n_fields < 2 || cfg->n_fields > 3) {
+    snprintf(err, errlen, "n_fields must be 2 or 3 (PsSteepDUpdater supports 2 or 3)");
+    return PS_ATTRIB_ERR;
+  }
+  if (cfg->n_polymers < 1 || cfg->n_polymers > PS_MAX_POLYMERS) {
+    snprintf(err, errlen, "n_polymers out of range");
+    return PS_ATTRIB_ERR;
+  }
+  oracle_state* s = (oracle_state*)xcalloc(1, sizeof(oracle_state));
+  s->cfg = *cfg;
+  for (int d = 0; d < 3; ++d) s->n[d] = cfg->n[d];
+  s->N = (long)cfg->n[0] * cfg->n[1] * cfg->n[2];
+  s->nf = cfg->n_fields;
+  long N = s->N;
+  for (int i = 0; i < s->nf; ++i) {
+    s->w[i] = (double*)xcalloc((size_t)N, sizeof(double));
+    s->phi[i] = (double*)xcalloc((size_t)N, sizeof(double));
+    s->dh[i] = (double*)xcalloc((size_t)N, sizeof(double));
+  }
+  s->p = (double*)xcalloc((size_t)N, sizeof(double));
+  s->cwork = (double*)xcalloc((size_t)(2 * N), sizeof(double));
+  s->qw = (double*)xcalloc((size_t)N, sizeof(double));
+  s->res = (double*)xcalloc((size_t)N, sizeof(double));
+  /* scaleLength = length of the first polymer (pspolymer/PsPolymerHldr.cpp:67-83) */
+  s->scale_length = (double)cfg->polymers[0].length;
+  s->npol = cfg->n_polymers;
+  int rc = PS_OK;
+  for (int ip = 0; ip < s->npol && rc == PS_OK; ++ip) {
+    opolymer* P = &s->pol[ip];
+    P->cfg = cfg->polymers[ip];
+    P->nb = P->cfg.n_blocks;
+    P->length_ratio = (double)P->cfg.length / s->scale_length;
+    if (P->nb < 1 || P->nb > PS_MAX_BLOCKS) {
+      snprintf(err, errlen, "polymer %d: n_blocks out of range", ip);
+      rc = PS_ATTRIB_ERR;
+      break;
+    }
+    /* |sum f - 1| <= 1e-5 (pspolymer/PsBlockCopolymer.cpp:113-127) */
+    double tot = 0.0;
+    for (int ib = 0; ib < P->nb; ++ib) tot = tot + P->cfg.blocks[ib].lengthfrac;
+    if (fabs(tot - 1.0) > 0.00001) {
+      snprintf(err, errlen, "polymer %d: |totalFrac - 1.0| = %g > tolerance", ip, fabs(tot - 1.0));
+      rc = PS_INPUT_ERR;
+      break;
+    }
+    for (int ib = 0; ib < P->nb && rc == PS_OK; ++ib) {
+      oblock* B = &P->b[ib];
+      B->cfg = P->cfg.blocks[ib];
+      if (B->cfg.field < 0 || B->cfg.field >= s->nf) {
+        snprintf(err, errlen, "polymer %d block %d: field index out of range", ip, ib);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+      if (!(B->cfg.ds > 0.0)) {
+        snprintf(err, errlen, "polymer %d block %d: ds not set", ip, ib);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+      /* psbase/PsBlockBase.cpp:187-198 */
+      s->dens_avg[B->cfg.field] = s->dens_avg[B->cfg.field] + 1.0 * B->cfg.lengthfrac * P->cfg.volfrac;
+      double bstmp = P->length_ratio * B->cfg.lengthfrac / B->cfg.ds;
+      char e2[200];
+      rc = set_block_steps(bstmp, B->cfg.force_block_steps, &B->steps, e2, sizeof(e2));
+      if (rc != PS_OK) {
+        snprintf(err, errlen, "polymer %d block %d: %s", ip, ib, e2);
+        break;
+      }
+      B->qs = (double*)xcalloc((size_t)(B->steps + 1) * N, sizeof(double));
+      B->qts = (double*)xcalloc((size_t)(B->steps + 1) * N, sizeof(double));
+      B->wfac = (double*)xcalloc((size_t)N, sizeof(double));
+      B->k2 = (double*)xcalloc((size_t)N, sizeof(double));
+      B->qqt = (double*)xcalloc((size_t)N, sizeof(double));
+      for (int e = 0; e < 2; ++e) {
+        B->q_init[e] = (double*)xcalloc((size_t)N, sizeof(double));
+        B->q_final[e] = (double*)xcalloc((size_t)N, sizeof(double));
+      }
+    }
+    if (rc != PS_OK) break;
+    /* setCntToLists (psbase/PsBlockBase.cpp:214-245) */
+    for (int ib = 0; ib < P->nb; ++ib) {
+      oblock* B = &P->b[ib];
+      B->ncnt[HEAD] = B->cfg.n_head;
+      B->ncnt[TAIL] = B->cfg.n_tail;
+      for (int e = 0; e < 2; ++e) {
+        const int* lst = (e == HEAD) ? B->cfg.head_joined : B->cfg.tail_joined;
+        for (int c = 0; c < B->ncnt[e]; ++c) {
+          if (lst[c] < 0 || lst[c] >= P->nb) {
+            snprintf(err, errlen, "polymer %d block %d: joined block index out of range", ip, ib);
+            rc = PS_ATTRIB_ERR;
+          }
+          B->cnt_idx[e][c] = lst[c];
+          B->cnt_end[e][c] = HEAD;
+        }
+        /* junction map in ascending key order */
+        int keys[PS_MAX_JOINS];
+        int nk = 0;
+        for (int c = 0; c < B->ncnt[e]; ++c) {
+          int key = lst[c], dup = 0;
+          for (int t = 0; t < nk; ++t) dup |= (keys[t] == key);
+          if (!dup) keys[nk++] = key;
+        }
+        for (int a = 0; a < nk; ++a)
+          for (int c = a + 1; c < nk; ++c)
+            if (keys[c] < keys[a]) { int t = keys[a]; keys[a] = keys[c]; keys[c] = t; }
+        B->njnt[e] = nk;
+        for (int a = 0; a < nk; ++a) {
+          B->jnt_key[e][a] = keys[a];
+          B->jnt_q[e][a] = (double*)xcalloc((size_t)N, sizeof(double));
+        }
+      }
+    }
+    /* buildCntBlockType (pspolymer/PsBlockCopolymer.cpp:157-182) */
+    for (int ib = 0; ib < P->nb; ++ib) {
+      for (int e = 0; e < 2; ++e) {
+        oblock* B = &P->b[ib];
+        for (int c = 0; c < B->ncnt[e]; ++c) {
+          int j = B->cnt_idx[e][c];
+          oblock* J = &P->b[j];
+          for (int t = 0; t < J->ncnt[TAIL]; ++t)
+            if (J->cnt_idx[TAIL][t] == ib) B->cnt_end[e][c] = TAIL;
+        }
+      }
+    }
+    for (int ib = 0; ib < P->nb; ++ib) build_k2(s, &P->b[ib], P->b[ib].k2);
+  }
+  if (rc == PS_OK) {
+    /* sum of volume fractions (psphysf/PsPhysFieldHldr.cpp check) */
+    double vt = 0.0;
+    for (int ip = 0; ip < s->npol; ++ip) vt += cfg->polymers[ip].volfrac;
+    if (fabs(vt - 1.0) > 0.00001) {
+      snprintf(err, errlen, "sum of volume fractions %g != 1", vt);
+      rc = PS_INPUT_ERR;
+    }
+  }
+  for (int it = 0; it < cfg->n_interactions && rc == PS_OK; ++it) {
+    const ps_interaction_config* I = &cfg->interactions[it];
+    if (I->field_a < 0 || I->field_a >= s->nf || I->field_b < 0 || I->field_b >= s->nf ||
+        I->field_a == I->field_b) {
+      snprintf(err, errlen, "interaction %d: bad scfields", it);
+      rc = PS_ATTRIB_ERR;
+    }
+    /* chiN = chi * Nlen (pseffhamil/PsFloryInteraction.cpp:159-161) */
+    s->chin[it] = I->chi * s->scale_length;
+  }
+  if (rc == PS_OK && cfg->updater.kind == PS_UPD_ANDERSON) {
+    int m = cfg->updater.anderson_depth;
+    if (m < 0 || m > 64) {
+      snprintf(err, errlen, "anderson_depth out of range");
+      rc = PS_ATTRIB_ERR;
+    } else {
+      s->am_m = m;
+      s->am_w = (double*)xcalloc((size_t)(m + 1) * s->nf * N, sizeof(double));
+      s->am_d = (double*)xcalloc((size_t)(m + 1) * s->nf * N, sizeof(double));
+      s->am_g = (double*)xcalloc((size_t)(m + 1) * (m + 1), sizeof(double));
+    }
+  }
+  /* psSrandom(randomSeed + rank), rank 0 (pstrol/PsDomain.cpp:213) */
+  mt_seed(&s->rng, (uint32_t)(cfg->seed & 0xffffffffULL));
+  if (rc != PS_OK) {
+    oracle_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return PS_OK;
+}
+
+void oracle_destroy(oracle_state* s) {
+  if (!s) return;
+  for (int i = 0; i < PS_MAX_FIELDS; ++i) { free(s->w[i]); free(s->phi[i]); free(s->dh[i]); }
+  free(s->p); free(s->cwork); free(s->qw); free(s->res);
+  for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip)
+    for (int ib = 0; ib < PS_MAX_BLOCKS; ++ib) {
+      oblock* B = &s->pol[ip].b[ib];
+      free(B->qs); free(B->qts); free(B->wfac); free(B->k2); free(B->qqt);
+      for (int e = 0; e < 2; ++e) {
+        free(B->q_init[e]); free(B->q_final[e]);
+        for (int a = 0; a < PS_MAX_JOINS; ++a) free(B->jnt_q[e][a]);
+      }
+    }
+  free(s->am_w); free(s->am_d); free(s->am_g);
+  free(s);
+}
+
+int oracle_block_steps(const oracle_state* s, int ip, int ib) { return s->pol[ip].b[ib].steps; }
+
+/* PsMonomerDens::initialize "random" then PsConstraint::initialize (p = 0):
+ * psphysf/PsMonomerDens.cpp:116-127, psbase/PsGridField.cpp:389-401,
+ * psphysf/PsConstraint.cpp:146-152. */
+void oracle_init_random(oracle_state* s) {
+  for (int i = 0; i < s->nf; ++i)
+    for (long r = 0; r < s->N; ++r) {
+      double u = mt_real(&s->rng);
+      s->w[i][r] = 1.0 * (u + (-0.5));
+    }
+  memset(s->p, 0, sizeof(double) * (size_t)s->N);
+}
+
+void oracle_set_field(oracle_state* s, int which, int index, const double* data) {
+  double* dst = (which == PS_FIELD_W) ? s->w[index] : (which == PS_FIELD_PHI ? s->phi[index] : s->p);
+  memcpy(dst, data, sizeof(double) * (size_t)s->N);
+}
+
+void oracle_get_field(const oracle_state* s, int which, int index, double* data) {
+  const double* src =
+      (which == PS_FIELD_W) ? s->w[index] : (which == PS_FIELD_PHI ? s->phi[index] : s->p);
+  memcpy(data, src, sizeof(double) * (size_t)s->N);
+}
+
+void oracle_get_propagator(const oracle_state* s, int ip, int ib, int end, int n, double* out) {
+  const oblock* B = &s->pol[ip].b[ib];
+  const double* src = (end == PS_FROM_HEAD) ? B->qs : B->qts;
+  memcpy(out, src + (size_t)n * s->N, sizeof(double) * (size_t)s->N);
+}
+
+void oracle_get_k2(const oracle_state* s, int ip, int ib, double* out) {
+  memcpy(out, s->pol[ip].b[ib].k2, sizeof(double) * (size_t)s->N);
+}
+
+/* ---------------------------------------------------------------------------
+ * Propagators
+ * ------------------------------------------------------------------------- */
+
+/* PsFlexPseudoSpec::solveQ (pspolymer/PsFlexPseudoSpec.cpp:244-293). */
+static void solve_q(oracle_state* s, oblock* B, int from) {
+  const long N = s->N;
+  double* dst = (from == HEAD) ? B->qs : B->qts;
+  const double scale_fft = 1.0 / ((double)N);
+  double* qx = dst; /* slice 0 */
+  memcpy(qx, B->q_init[from], sizeof(double) * (size_t)N);
+  for (int ss = 1; ss <= B->steps; ++ss) {
+    const double* prev = dst + (size_t)(ss - 1) * N;
+    double* next = dst + (size_t)ss * N;
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) s->qw[n] = prev[n] * B->wfac[n];
+    oracle_scaled_pair_buf(s->n, s->qw, B->k2, s->res, s->cwork);
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) {
+      double v = s->res[n] * B->wfac[n];
+      next[n] = scale_fft * v;
+    }
+  }
+  /* setFinalQ(getOtherEnd(from), qX) */
+  int other = (from == HEAD) ? TAIL : HEAD;
+  memcpy(B->q_final[other], dst + (size_t)B->steps * N, sizeof(double) * (size_t)N);
+  B->final_set[other] = 1;
+}
+
+/* PsBlock::combineSetJnt (pspolymer/PsBlock.cpp:386-416). */
+static void combine_set_jnt(oracle_state* s, oblock* B, int end) {
+  const long N = s->N;
+  double* prod = B->q_init[end];
+  for (long r = 0; r < N; ++r) prod[r] = 1.0;
+  for (int a = 0; a < B->njnt[end]; ++a) {
+    const double* q = B->jnt_q[end][a];
+    for (long r = 0; r < N; ++r) prod[r] *= q[r];
+  }
+  B->init_set[end] = 1;
+}
+
+static int jnts_set(const oblock* B, int end) {
+  int all = 1;
+  for (int a = 0; a < B->njnt[end]; ++a)
+    if (!B->jnt_set[end][a]) all = 0;
+  return all;
+}
+
+/* PsBlockCopolymer::publishQFrom + PsBlock::setJctQ (pspolymer/PsBlockCopolymer.cpp:283-313,
+ * pspolymer/PsBlock.cpp:435-472). */
+static void publish_q_from(oracle_state* s, opolymer* P, int end, int from) {
+  oblock* F = &P->b[from];
+  if (!F->final_set[end]) return;
+  for (int c = 0; c < F->ncnt[end]; ++c) {
+    oblock* T = &P->b[F->cnt_idx[end][c]];
+    int tend = F->cnt_end[end][c];
+    for (int a = 0; a < T->njnt[tend]; ++a) {
+      if (T->jnt_key[tend][a] == from) {
+        memcpy(T->jnt_q[tend][a], F->q_final[end], sizeof(double) * (size_t)s->N);
+        T->jnt_set[tend][a] = 1;
+      }
+    }
+  }
+}
+
+/* PsBlockCopolymer::updateBlockQ (pspolymer/PsBlockCopolymer.cpp:247-272). */
+static void update_block_q(oracle_state* s, opolymer* P, int ib, int end) {
+  oblock* B = &P->b[ib];
+  int other = (end == HEAD) ? TAIL : HEAD;
+  if (!B->init_set[end]) {
+    if (jnts_set(B, end)) combine_set_jnt(s, B, end);
+  }
+  if (B->init_set[end] && !B->final_set[other]) {
+    solve_q(s, B, end);
+    publish_q_from(s, P, other, ib);
+  }
+}
+
+/* PsBlock::setCalcQQTIntegral (pspolymer/PsBlock.cpp:255-380). */
+static void calc_qqt(oracle_state* s, oblock* B, double bq) {
+  const long N = s->N;
+  const size_t num = (size_t)B->steps + 1;
+  const size_t npts = num - 1;
+  size_t numstail;
+  int even;
+  double modval = fmod((double)num, 2.0);
+  if (modval == 0.0) { even = 1; numstail = npts - 3; }
+  else { even = 0; numstail = npts - 2; }
+  const double simp = 0.33333 * B->cfg.ds;
+  const double trap = B->cfg.ds * 0.5;
+  const double inv_bq = 1.0 / bq;
+#pragma omp parallel for schedule(static)
+  for (long r = 0; r < N; ++r) {
+    double acc = 0.0;
+    for (size_t n = 0; n <= numstail; n += 2) {
+      double p1 = B->qs[n * N + r] * B->qts[(num - n - 1) * N + r];
+      double p2 = B->qs[(n + 1) * N + r] * B->qts[(num - n - 2) * N + r];
+      double p3 = B->qs[(n + 2) * N + r] * B->qts[(num - n - 3) * N + r];
+      p2 = p2 * 4.0;
+      acc = acc + p1;
+      acc = acc + p2;
+      acc = acc + p3;
+    }
+    acc = acc * simp;
+    if (even) {
+      double p1 = B->qs[(num - 2) * N + r] * B->qts[1 * N + r];
+      double p2 = B->qs[(num - 1) * N + r] * B->qts[0 * N + r];
+      double t = 0.0;
+      t = t + p1;
+      t = t + p2;
+      t = t * trap;
+      acc = acc + t;
+    }
+    B->qqt[r] = inv_bq * acc;
+  }
+}
+
+/* PsBlockCopolymer::update (pspolymer/PsBlockCopolymer.cpp:188-239). */
+static int polymer_update(oracle_state* s, opolymer* P) {
+  const long N = s->N;
+  for (int ib = 0; ib < P->nb; ++ib) {
+    oblock* B = &P->b[ib];
+    /* PsBlockBase::reset */
+    B->init_set[HEAD] = B->init_set[TAIL] = 0;
+    B->final_set[HEAD] = B->final_set[TAIL] = 0;
+    for (int e = 0; e < 2; ++e)
+      for (int a = 0; a < B->njnt[e]; ++a) B->jnt_set[e][a] = 0;
+    /* PsBlock::reset: free ends get q0 = 1 */
+    for (int e = 0; e < 2; ++e) {
+      if (B->ncnt[e] == 0) {
+        for (long r = 0; r < N; ++r) B->q_init[e][r] = 1.0;
+        B->init_set[e] = 1;
+      }
+    }
+    /* PsFlexPseudoSpec::reset: wfac = exp(-0.5 ds w) */
+    const double ds2 = -0.5 * B->cfg.ds;
+    const double* w = s->w[B->cfg.field];
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) B->wfac[n] = exp(ds2 * w[n]);
+  }
+  int guard = 0;
+  const double t0 = now_s();
+  for (;;) {
+    int all = 1;
+    for (int ib = 0; ib < P->nb; ++ib)
+      if (!(P->b[ib].final_set[HEAD] && P->b[ib].final_set[TAIL])) all = 0;
+    if (all) break;
+    if (++guard > 4 * PS_MAX_BLOCKS + 4) return PS_INPUT_ERR; /* unreachable blocks */
+    for (int ib = 0; ib < P->nb; ++ib) {
+      update_block_q(s, P, ib, HEAD);
+      update_block_q(s, P, ib, TAIL);
+    }
+  }
+  s->t_sweeps += now_s() - t0;
+  /* PsBlock::calcBigQ of block 0 (pspolymer/PsBlock.cpp:204-237) */
+  {
+    oblock* B0 = &P->b[0];
+    double tot = 0.0;
+    for (long r = 0; r < N; ++r) {
+      double v = (0.0 + B0->q_init[HEAD][r]) * B0->q_final[HEAD][r];
+      tot = tot + v;
+    }
+    double q = tot / ((double)(1 * (double)N));
+    P->bigq = q;
+    if (q != q) return PS_RUN_ERR;
+  }
+  for (int ib = 0; ib < P->nb; ++ib) calc_qqt(s, &P->b[ib], P->bigq);
+  /* PsBlock::setPhysFields (pspolymer/PsBlock.cpp:153-196) */
+  for (int ib = 0; ib < P->nb; ++ib) {
+    oblock* B = &P->b[ib];
+    double densfac = 1.0 * P->cfg.volfrac / P->length_ratio;
+    double* phi = s->phi[B->cfg.field];
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < N; ++r) {
+      double v = densfac * B->qqt[r];
+      phi[r] = phi[r] + v;
+    }
+  }
+  return PS_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Field update
+ * ------------------------------------------------------------------------- */
+
+static int interaction_has(const ps_interaction_config* I, int f) {
+  return I->field_a == f || I->field_b == f;
+}
+
+/* dH_i = p - w_i + sum_{int ∋ i} chiN (phi_other - avg_other):
+ * pseffhamil/PsSteepDUpdater.cpp:174-184, :208-236 and
+ * pseffhamil/PsFloryInteraction.cpp:204-269. */
+static void compute_dh(oracle_state* s) {
+  const long N = s->N;
+  const int nf = s->nf;
+#pragma omp parallel for schedule(static)
+  for (long r = 0; r < N; ++r) {
+    for (int i = 0; i < nf; ++i) {
+      double d = 0.0;
+      d = d + s->p[r];
+      d = d - s->w[i][r];
+      for (int it = 0; it < s->cfg.n_interactions; ++it) {
+        const ps_interaction_config* I = &s->cfg.interactions[it];
+        if (!interaction_has(I, i)) continue;
+        int other = (i == I->field_a) ? I->field_b : I->field_a;
+        double mask = -1.0 * s->dens_avg[other]; /* ((0 + wall)*-1 + 1) * -avg, wall = 0 */
+        double x = 0.0;
+        x = x + s->phi[other][r];
+        x = x + mask;
+        x = x * s->chin[it];
+        d = d + x;
+      }
+      s->dh[i][r] = d;
+    }
+  }
+}
+
+/* Pressure rebuild after the w update: setConjgFieldsToPres + mixed terms,
+ * scaled by 1/n_fields (pseffhamil/PsSteepDUpdater.cpp:283-332, :398-452),
+ * then PsConstraint::updatePres / shiftPresField (psphysf/PsConstraint.cpp:184-262). */
+static double rebuild_pressure(oracle_state* s) {
+  const long N = s->N;
+  const int nf = s->nf;
+  for (long r = 0; r < N; ++r) {
+    double pr = 0.0;
+    for (int i = 0; i < nf; ++i) pr = pr + s->w[i][r];
+    if (nf == 2) {
+      for (int it = 0; it < s->cfg.n_interactions; ++it) {
+        const ps_interaction_config* I = &s->cfg.interactions[it];
+        if (interaction_has(I, 0) && interaction_has(I, 1)) {
+          double x = 0.0; /* phi0 * chiN with phi0 = 0 */
+          x = x * s->chin[it];
+          pr = pr + x;
+        }
+      }
+      pr = 0.5 * pr;
+    } else {
+      for (int it = 0; it < s->cfg.n_interactions; ++it) {
+        const ps_interaction_config* I = &s->cfg.interactions[it];
+        for (int n = 0; n < nf; ++n) {
+          if (interaction_has(I, n)) continue;
+          double x = 0.0;
+          x = x + (s->phi[n][r] - s->dens_avg[n]);
+          x = x + 0.0; /* phi0 */
+          x = x * s->chin[it];
+          pr = pr + x;
+        }
+      }
+      double inv = 1.0 / 3.0;
+      pr = inv * pr;
+    }
+    s->p[r] = pr;
+  }
+  /* updatePres with phi0 = 0: p *= 1; p -= mean; p *= 1; p += 0 */
+  double tot = 0.0;
+  for (long r = 0; r < N; ++r) tot = tot + s->p[r];
+  double mean = tot / ((double)((double)N * 1));
+  for (long r = 0; r < N; ++r) s->p[r] = s->p[r] - mean;
+  return mean;
+}
+
+/* PsPolymerUpdater::calcFeField (pseffhamil/PsPolymerUpdater.cpp:172-226). */
+static void calc_fe(oracle_state* s, double* fe_out, double* fe_nodis_out) {
+  const long N = s->N;
+  const int nf = s->nf;
+  const double inv_vol = 1.0 / (double)N;
+  double sum_tmp = 0.0;
+  for (int ip = 0; ip < s->npol; ++ip) {
+    double logq = log(s->pol[ip].bigq);
+    double vf = s->pol[ip].cfg.volfrac;
+    double lr = s->pol[ip].length_ratio;
+    sum_tmp = sum_tmp - ((vf * logq) / lr);
+  }
+  double tot = 0.0, tot_nd = 0.0;
+  for (long r = 0; r < N; ++r) {
+    double fe = 0.0;
+    for (int i = 0; i < nf; ++i) {
+      double prod = (0.0 + s->phi[i][r]) * s->w[i][r];
+      prod = -1.0 * prod;
+      fe = fe + prod;
+    }
+    fe = fe * 1.0;
+    fe = inv_vol * fe;
+    double ft = 0.0 + fe, ftn = 0.0 + fe;
+    for (int it = 0; it < s->cfg.n_interactions; ++it) {
+      const ps_interaction_config* I = &s->cfg.interactions[it];
+      double a0 = s->dens_avg[I->field_a], a1 = s->dens_avg[I->field_b];
+      double dis = (((0.0 + 1.0) * 1.0) * a0) * a1;
+      dis = dis * s->chin[it];
+      double v = (0.0 + s->phi[I->field_a][r]) * s->phi[I->field_b][r];
+      v = v * s->chin[it];
+      double vd = v - dis;
+      ft = ft + inv_vol * vd;
+      ftn = ftn + inv_vol * v;
+    }
+    tot = tot + ft;
+    tot_nd = tot_nd + ftn;
+  }
+  *fe_out = sum_tmp + tot;
+  *fe_nodis_out = sum_tmp + tot_nd;
+}
+
+/* Gaussian elimination with partial pivoting on an m x m system (row major);
+ * returns 0 on success, 1 when a pivot is zero (caller then uses c = 0). */
+int oracle_solve_small(int m, double* a, double* b) {
+  for (int k = 0; k < m; ++k) {
+    int piv = k;
+    double best = fabs(a[k * m + k]);
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(a[i * m + k]) > best) { best = fabs(a[i * m + k]); piv = i; }
+    if (!(best > 0.0)) return 1;
+    if (piv != k) {
+      for (int j = 0; j < m; ++j) { double t = a[k * m + j]; a[k * m + j] = a[piv * m + j]; a[piv * m + j] = t; }
+      double t = b[k]; b[k] = b[piv]; b[piv] = t;
+    }
+    for (int i = k + 1; i < m; ++i) {
+      double f = a[i * m + k] / a[k * m + k];
+      for (int j = k; j < m; ++j) a[i * m + j] = a[i * m + j] - f * a[k * m + j];
+      b[i] = b[i] - f * b[k];
+    }
+  }
+  for (int i = m - 1; i >= 0; --i) {
+    double t = b[i];
+    for (int j = i + 1; j < m; ++j) t = t - a[i * m + j] * b[j];
+    b[i] = t / a[i * m + i];
+  }
+  return 0;
+}
+
+/* Steepest descent w update (pseffhamil/PsSteepDUpdater.cpp:264-278, :368-393). */
+static void sd_direction(const oracle_state* s, long r, double* dir) {
+  const int nf = s->nf;
+  const double lam1 = s->cfg.updater.lambda1;
+  for (int i = 0; i < nf; ++i) {
+    double x = 0.0;
+    for (int j = 0; j < nf; ++j)
+      if (j != i) x = x + s->dh[j][r];
+    x = x * (-1.0 * lam1);
+    x = x + s->dh[i][r];
+    dir[i] = x;
+  }
+}
+
+static void update_fields(oracle_state* s, ps_scalars* sc) {
+  const long N = s->N;
+  const int nf = s->nf;
+  compute_dh(s);
+  /* residual statistics (diagnostic only) */
+  {
+    double ss = 0.0;
+    for (long r = 0; r < N; ++r)
+      for (int i = 0; i < nf; ++i) ss = ss + s->dh[i][r] * s->dh[i][r];
+    sc->dh_norm = sqrt(ss / (double)N);
+  }
+  const ps_updater_config* U = &s->cfg.updater;
+  if (U->kind == PS_UPD_ANDERSON) {
+    const int m = s->am_m;
+    const int slots = m + 1;
+    const long long k = s->am_k;
+    const int cur = (int)(k % slots);
+    double* Wc = s->am_w + (size_t)cur * nf * N;
+    double* Dc = s->am_d + (size_t)cur * nf * N;
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < N; ++r) {
+      double dir[PS_MAX_FIELDS];
+      sd_direction(s, r, dir);
+      for (int i = 0; i < nf; ++i) {
+        Wc[(size_t)i * N + r] = s->w[i][r];
+        Dc[(size_t)i * N + r] = dir[i];
+      }
+    }
+    int nh = (int)(k < m ? k : m);
+    /* Gram row: G[cur][slot(k-j)] = D^k . D^{k-j}, j = 0..nh */
+    for (int j = 0; j <= nh; ++j) {
+      int sj = (int)((k - j) % slots);
+      const double* Dj = s->am_d + (size_t)sj * nf * N;
+      double g = 0.0;
+      for (long t = 0; t < (long)nf * N; ++t) g = g + Dc[t] * Dj[t];
+      s->am_g[cur * slots + sj] = g;
+      s->am_g[sj * slots + cur] = g;
+    }
+    double c[64];
+    int use = (k >= U->anderson_start) && nh > 0;
+    if (use) {
+      double A[64 * 64], V[64];
+      for (int a = 1; a <= nh; ++a) {
+        int sa = (int)((k - a) % slots);
+        V[a - 1] = s->am_g[cur * slots + cur] - s->am_g[cur * slots + sa];
+        for (int b = 1; b <= nh; ++b) {
+          int sb = (int)((k - b) % slots);
+          A[(a - 1) * nh + (b - 1)] = s->am_g[cur * slots + cur] - s->am_g[cur * slots + sa] -
+                                      s->am_g[cur * slots + sb] + s->am_g[sa * slots + sb];
+        }
+      }
+      if (oracle_solve_small(nh, A, V) != 0) {
+        for (int a = 0; a < nh; ++a) V[a] = 0.0;
+      }
+      for (int a = 0; a < nh; ++a) c[a] = V[a];
+    } else {
+      nh = 0;
+    }
+    const double mix = use ? U->anderson_mix : U->lambda0;
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < N; ++r) {
+      for (int i = 0; i < nf; ++i) {
+        double wk = Wc[(size_t)i * N + r];
+        double dk = Dc[(size_t)i * N + r];
+        double wh = wk, dhh = dk;
+        for (int a = 1; a <= nh; ++a) {
+          int sa = (int)((k - a) % slots);
+          wh = wh + c[a - 1] * (s->am_w[(size_t)sa * nf * N + (size_t)i * N + r] - wk);
+          dhh = dhh + c[a - 1] * (s->am_d[(size_t)sa * nf * N + (size_t)i * N + r] - dk);
+        }
+        s->w[i][r] = wh + mix * dhh;
+      }
+    }
+    s->am_k = k + 1;
+  } else {
+    const double lam0 = s->cfg.updater.lambda0;
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < N; ++r) {
+      double dir[PS_MAX_FIELDS];
+      sd_direction(s, r, dir);
+      for (int i = 0; i < nf; ++i) {
+        double x = dir[i] * lam0;
+        s->w[i][r] = s->w[i][r] + x;
+      }
+    }
+  }
+  /* addRandUpdateConjgFields (pseffhamil/PsPolymerUpdater.cpp:263-295): one
+   * Gaussian per point per field, drawn even when noise = 0. */
+  if (U->noise != 0.0) {
+    for (int i = 0; i < nf; ++i)
+      for (long r = 0; r < N; ++r) {
+        double g = U->noise * mt_gauss(&s->rng);
+        double v = 0.0 + g;
+        v = v * 1.0;
+        s->w[i][r] = s->w[i][r] + v;
+      }
+  } else {
+    for (int i = 0; i < nf; ++i)
+      for (long r = 0; r < N; ++r) (void)mt_gauss(&s->rng);
+  }
+  sc->pressure_mean = rebuild_pressure(s);
+  calc_fe(s, &sc->free_energy, &sc->free_energy_nodis);
+}
+
+int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
+  const long N = s->N;
+  for (int it = 0; it < niter; ++it) {
+    ps_scalars sc;
+    memset(&sc, 0, sizeof(sc));
+    const double t_begin = now_s();
+    s->t_sweeps = 0.0;
+    for (int i = 0; i < s->nf; ++i) memset(s->phi[i], 0, sizeof(double) * (size_t)N);
+    for (int ip = 0; ip < s->npol; ++ip) {
+      int rc = polymer_update(s, &s->pol[ip]);
+      if (rc != PS_OK) return rc;
+      sc.q[ip] = s->pol[ip].bigq;
+      sc.log_q[ip] = log(s->pol[ip].bigq);
+    }
+    double mx = 0.0;
+    for (long r = 0; r < N; ++r) {
+      double t = 0.0;
+      for (int i = 0; i < s->nf; ++i) t += s->phi[i][r];
+      double d = fabs(t - 1.0);
+      if (d > mx) mx = d;
+    }
+    sc.max_incomp = mx;
+    update_fields(s, &sc);
+    s->t_total = now_s() - t_begin;
+    s->iter++;
+    sc.iteration = s->iter;
+    if (!(sc.free_energy == sc.free_energy)) sc.error_flags |= 2;
+    if (hist) hist[it] = sc;
+  }
+  return PS_OK;
+}
+
+void oracle_last_timing(const oracle_state* s, double* t_sweeps, double* t_total) {
+  *t_sweeps = s->t_sweeps;
+  *t_total = s->t_total;
+}
+
+/* A bounded sample of the sweep work: nsteps operator-split steps of the
+ * first polymer's first block from its head (same arithmetic as solve_q),
+ * with wfac from the current w.  Returns the wall time in seconds. */
+double oracle_propagate_sample(oracle_state* s, int nsteps) {
+  const long N = s->N;
+  opolymer* P = &s->pol[0];
+  oblock* B = &P->b[0];
+  const double t0 = now_s();
+  const double ds2 = -0.5 * B->cfg.ds;
+  const double* w = s->w[B->cfg.field];
+#pragma omp parallel for schedule(static)
+  for (long n = 0; n < N; ++n) B->wfac[n] = exp(ds2 * w[n]);
+  for (long r = 0; r < N; ++r) B->qs[r] = 1.0;
+  const double scale_fft = 1.0 / ((double)N);
+  for (int ss = 1; ss <= nsteps; ++ss) {
+    const double* prev = B->qs + (size_t)((ss - 1) % B->steps) * N;
+    double* next = B->qs + (size_t)(((ss - 1) % B->steps) + 1) * N;
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) s->qw[n] = prev[n] * B->wfac[n];
+    oracle_scaled_pair_buf(s->n, s->qw, B->k2, s->res, s->cwork);
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) {
+      double v = s->res[n] * B->wfac[n];
+      next[n] = scale_fft * v;
+    }
+  }
+  return now_s() - t0;
+}
+
+void oracle_mt_reals(unsigned long long seed, long n, double* out) {
+  mt_state st;
+  mt_seed(&st, (uint32_t)(seed & 0xffffffffULL));
+  for (long i = 0; i < n; ++i) out[i] = mt_real(&st);
+}
+
+void oracle_mt_gauss(unsigned long long seed, long n, double* out) {
+  mt_state st;
+  mt_seed(&st, (uint32_t)(seed & 0xffffffffULL));
+  for (long i = 0; i < n; ++i) out[i] = mt_gauss(&st);
+}
+
+void oracle_mt_u32(unsigned long long seed, long n, unsigned int* out) {
+  mt_state st;
+  mt_seed(&st, (uint32_t)(seed & 0xffffffffULL));
+  for (long i = 0; i < n; ++i) out[i] = mt_u32(&st);
+}

@@ -1,0 +1,329 @@
+"""SCFT instance description, mirroring the reference's input-file blocks.
+
+The reference reads a txpp-expanded input file into a hierarchical attribute
+set (``<Polymer name> ... </Polymer>`` etc.) and builds objects through its
+maker maps.  The same blocks and keys are accepted here:
+
+* ``<Grid>``: ``numCellsGlobal``, ``cellSizes`` (psgrid/PsUniCartGrid.cpp:30-43); the
+  ``setupPS(nx, ny, nz, dx, dy, dz, debug)`` macro line of
+  polyswift/psutils/macros/pseudoSpecSetup.mac:34-98 is expanded to it.
+* ``<PhysField name> kind = monomerDens | constraint`` (psphysf/).
+* ``<Polymer name> kind = blockCopolymer``: ``volfrac``, ``length``
+  (psbase/PsPolymer.cpp:42-73) with ``<Block name> kind = flexPseudoSpec``:
+  ``scfield``, ``ds``, ``lengthfrac``, ``headjoined``, ``tailjoined``,
+  ``bSegRatio``, ``forceBlockSteps`` (psbase/PsBlockBase.cpp:67-145,
+  pspolymer/PsFlexPseudoSpec.cpp:58-82).
+* ``<EffHamil>`` with ``<Updater name> kind = steepestDescent``: ``relaxlambdas``,
+  ``noise``, ``updatefields``, ``interactions`` (pseffhamil/PsSteepDUpdater.cpp:47-76)
+  and ``<Interaction name> kind = flory``: ``chi``, ``scfields``
+  (pseffhamil/PsFloryInteraction.cpp:65-89).
+* top level: ``randomSeed``, ``nsteps``.
+
+Added keys: ``kind = andersonMixing`` for ``<Updater>`` (``andersonDepth``,
+``andersonMix``, ``andersonStart``), and top-level ``precision = fp64 | mixed``
+and ``device``.  ``kind`` aliases ``blockCopolymerGPU`` / ``steepestDescentGPU`` /
+``andersonGPU`` select the same device path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import re
+from dataclasses import dataclass, field
+from pathlib import Path
+
+from . import _abi as A
+
+
+@dataclass
+class Block:
+    name: str
+    scfield: str
+    ds: float
+    lengthfrac: float
+    headjoined: list[str] = field(default_factory=lambda: ["freeEnd"])
+    tailjoined: list[str] = field(default_factory=lambda: ["freeEnd"])
+    bseg_ratio: float = 1.0
+    force_block_steps: bool = False
+    kind: str = "flexPseudoSpec"
+
+
+@dataclass
+class Polymer:
+    name: str
+    volfrac: float
+    length: int
+    blocks: list[Block]
+    kind: str = "blockCopolymer"
+
+
+@dataclass
+class Interaction:
+    name: str
+    chi: float
+    scfields: list[str]
+    kind: str = "flory"
+
+
+@dataclass
+class Updater:
+    name: str = "updater"
+    kind: str = "steepestDescent"
+    relaxlambdas: tuple[float, float] = (0.1, 0.05)
+    noise: float = 0.0
+    anderson_depth: int = 10
+    anderson_mix: float = 0.1
+    anderson_start: int = 0
+
+
+@dataclass
+class ScftConfig:
+    n: tuple[int, int, int]
+    cell: tuple[float, float, float]
+    fields: list[str]                 # monomerDens PhysFields in declaration order
+    polymers: list[Polymer]
+    interactions: list[Interaction]
+    updater: Updater = field(default_factory=Updater)
+    seed: int = 0
+    precision: str = "fp64"           # "fp64" or "mixed"
+    nsteps: int = 1
+    device: int = 0
+
+    @property
+    def n_total(self) -> int:
+        return self.n[0] * self.n[1] * self.n[2]
+
+    @property
+    def box(self) -> tuple[float, float, float]:
+        return tuple(self.n[d] * self.cell[d] for d in range(3))
+
+    def field_index(self, name: str) -> int:
+        try:
+            return self.fields.index(name)
+        except ValueError as e:
+            raise ValueError(f"unknown PhysField {name!r}; declared: {self.fields}") from e
+
+    def to_ps_config(self) -> A.ps_config:
+        c = A.ps_config()
+        for d in range(3):
+            c.n[d] = int(self.n[d])
+            c.cell[d] = float(self.cell[d])
+        if self.precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        c.precision = A.PS_PREC_FP64 if self.precision == "fp64" else A.PS_PREC_MIXED
+        c.n_fields = len(self.fields)
+        if not 1 <= len(self.polymers) <= A.PS_MAX_POLYMERS:
+            raise ValueError("number of polymers out of range")
+        c.n_polymers = len(self.polymers)
+        for ip, P in enumerate(self.polymers):
+            cp = c.polymers[ip]
+            cp.volfrac = float(P.volfrac)
+            cp.length = int(P.length)
+            if not 1 <= len(P.blocks) <= A.PS_MAX_BLOCKS:
+                raise ValueError(f"polymer {P.name}: number of blocks out of range")
+            cp.n_blocks = len(P.blocks)
+            names = [b.name for b in P.blocks]
+            for ib, B in enumerate(P.blocks):
+                cb = cp.blocks[ib]
+                cb.field = self.field_index(B.scfield)
+                cb.lengthfrac = float(B.lengthfrac)
+                cb.ds = float(B.ds)
+                cb.bseg_ratio = float(B.bseg_ratio)
+                cb.force_block_steps = int(bool(B.force_block_steps))
+                heads = [names.index(x) for x in B.headjoined if x != "freeEnd"]
+                tails = [names.index(x) for x in B.tailjoined if x != "freeEnd"]
+                if len(heads) > A.PS_MAX_JOINS or len(tails) > A.PS_MAX_JOINS:
+                    raise ValueError("too many junctions on one block end")
+                cb.n_head = len(heads)
+                cb.n_tail = len(tails)
+                for k, v in enumerate(heads):
+                    cb.head_joined[k] = v
+                for k, v in enumerate(tails):
+                    cb.tail_joined[k] = v
+        if len(self.interactions) > A.PS_MAX_INTERACTIONS:
+            raise ValueError("too many interactions")
+        c.n_interactions = len(self.interactions)
+        for it, I in enumerate(self.interactions):
+            c.interactions[it].field_a = self.field_index(I.scfields[0])
+            c.interactions[it].field_b = self.field_index(I.scfields[1])
+            c.interactions[it].chi = float(I.chi)
+        U = self.updater
+        kind = U.kind.replace("GPU", "")
+        if kind in ("steepestDescent",):
+            c.updater.kind = A.PS_UPD_STEEPEST
+        elif kind in ("andersonMixing", "anderson"):
+            c.updater.kind = A.PS_UPD_ANDERSON
+        else:
+            raise ValueError(f"unknown updater kind {U.kind!r}")
+        c.updater.lambda0 = float(U.relaxlambdas[0])
+        c.updater.lambda1 = float(U.relaxlambdas[1]) if len(U.relaxlambdas) > 1 else 0.0
+        c.updater.noise = float(U.noise)
+        c.updater.anderson_depth = int(U.anderson_depth)
+        c.updater.anderson_mix = float(U.anderson_mix)
+        c.updater.anderson_start = int(U.anderson_start)
+        c.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
+        c.calc_disorder = 1
+        c.device = int(self.device)
+        return c
+
+
+# ---------------------------------------------------------------------------
+# Input-file parser (expanded .pre / .in subset)
+# ---------------------------------------------------------------------------
+_OPEN = re.compile(r"^<\s*(\w+)\s+(\w+)\s*>$")
+_CLOSE = re.compile(r"^</\s*(\w+)\s*>$")
+_SETUPPS = re.compile(r"^setupPS\s*\((.*)\)\s*$")
+
+
+class InputError(ValueError):
+    pass
+
+
+def _value(tok: str, env: dict):
+    tok = tok.strip()
+    if tok.startswith("[") and tok.endswith("]"):
+        return [_value(t, env) for t in tok[1:-1].split()]
+    if tok in env:
+        return env[tok]
+    t = tok.strip("'\"")
+    for conv in (int, float):
+        try:
+            return conv(t)
+        except ValueError:
+            pass
+    return t
+
+
+def parse_blocks(text: str) -> dict:
+    """Parse into a nested dict {'attrs': {...}, 'blocks': [(type, name, node), ...]}."""
+    env: dict = {}
+    root = {"attrs": {}, "blocks": []}
+    stack = [root]
+    for raw in text.splitlines():
+        line = raw.split("#", 1)[0].strip()
+        if not line:
+            continue
+        if line.startswith("$"):
+            body = line[1:].strip()
+            if body.startswith("import"):
+                continue
+            if "=" in body:
+                k, v = body.split("=", 1)
+                env[k.strip()] = _value(v.strip().strip('"'), env)
+            continue
+        m = _SETUPPS.match(line)
+        if m:
+            args = [_value(a, env) for a in m.group(1).split(",")]
+            if len(args) < 6:
+                raise InputError("setupPS needs nx, ny, nz, dx, dy, dz")
+            node = {"attrs": {"kind": "uniCartGrid",
+                              "numCellsGlobal": [int(a) for a in args[:3]],
+                              "cellSizes": [float(a) for a in args[3:6]]}, "blocks": []}
+            stack[-1]["blocks"].append(("Grid", "mainGrid", node))
+            continue
+        m = _OPEN.match(line)
+        if m:
+            node = {"attrs": {}, "blocks": []}
+            stack[-1]["blocks"].append((m.group(1), m.group(2), node))
+            stack.append(node)
+            continue
+        m = _CLOSE.match(line)
+        if m:
+            if len(stack) == 1:
+                raise InputError(f"unbalanced </{m.group(1)}>")
+            stack.pop()
+            continue
+        if "=" in line:
+            k, v = line.split("=", 1)
+            stack[-1]["attrs"][k.strip()] = _value(v.strip(), env)
+            continue
+        raise InputError(f"cannot parse line: {raw!r}")
+    if len(stack) != 1:
+        raise InputError("unterminated block")
+    return root
+
+
+def _find(node: dict, typ: str) -> list:
+    return [(n, b) for t, n, b in node["blocks"] if t == typ]
+
+
+def config_from_text(text: str) -> ScftConfig:
+    root = parse_blocks(text)
+    ra = root["attrs"]
+    grids = _find(root, "Grid")
+    if not grids:
+        raise InputError("no <Grid> block or setupPS(...) line")
+    g = grids[0][1]["attrs"]
+    n = tuple(int(v) for v in g["numCellsGlobal"])
+    cell = tuple(float(v) for v in g["cellSizes"])
+    fields, has_pressure = [], False
+    for name, node in _find(root, "PhysField"):
+        kind = node["attrs"].get("kind", "")
+        if kind == "monomerDens":
+            fields.append(name)
+        elif kind == "constraint":
+            has_pressure = True
+        else:
+            raise InputError(f"PhysField kind {kind!r} is not on the device path")
+    if not has_pressure:
+        raise InputError("a <PhysField defaultPressure> kind = constraint is required")
+    polymers = []
+    for pname, pnode in _find(root, "Polymer"):
+        pa = pnode["attrs"]
+        if pa.get("kind", "blockCopolymer") not in ("blockCopolymer", "blockCopolymerGPU"):
+            raise InputError(f"Polymer kind {pa.get('kind')!r} is not on the device path")
+        blocks = []
+        for bname, bnode in _find(pnode, "Block"):
+            ba = bnode["attrs"]
+            if ba.get("kind", "flexPseudoSpec") not in ("flexPseudoSpec", "flexPseudoSpecGPU"):
+                raise InputError(f"Block kind {ba.get('kind')!r} is not on the device path")
+            if "ds" not in ba:
+                raise InputError(f"PsBlockBase::setAttrib: ds not set in <Block {bname}>")
+            if "headjoined" not in ba or "tailjoined" not in ba:
+                raise InputError(f"headjoined/tailjoined not set in <Block {bname}>")
+            hj = ba["headjoined"] if isinstance(ba["headjoined"], list) else [ba["headjoined"]]
+            tj = ba["tailjoined"] if isinstance(ba["tailjoined"], list) else [ba["tailjoined"]]
+            fbs = ba.get("forceBlockSteps", 0)
+            blocks.append(Block(name=bname, scfield=str(ba["scfield"]), ds=float(ba["ds"]),
+                                lengthfrac=float(ba.get("lengthfrac", 0.0)),
+                                headjoined=[str(x) for x in hj], tailjoined=[str(x) for x in tj],
+                                bseg_ratio=float(ba.get("bSegRatio", 1.0)),
+                                force_block_steps=fbs in (1, "on", "true", "1")))
+        polymers.append(Polymer(name=pname, volfrac=float(pa.get("volfrac", 1.0)),
+                                length=int(pa.get("length", 1)), blocks=blocks))
+    interactions, updater = [], None
+    for hname, hnode in _find(root, "EffHamil"):
+        for iname, inode in _find(hnode, "Interaction"):
+            ia = inode["attrs"]
+            if ia.get("kind", "flory") != "flory":
+                raise InputError(f"Interaction kind {ia.get('kind')!r} is not on the device path")
+            interactions.append(Interaction(name=iname, chi=float(ia.get("chi", 0.01)),
+                                            scfields=[str(x) for x in ia["scfields"]]))
+        ups = _find(hnode, "Updater")
+        if ups:
+            uname, unode = ups[0]
+            ua = unode["attrs"]
+            lam = ua.get("relaxlambdas", [0.1, 0.05])
+            updater = Updater(name=uname, kind=str(ua.get("kind", "steepestDescent")),
+                              relaxlambdas=tuple(float(x) for x in lam),
+                              noise=float(ua.get("noise", 0.0)),
+                              anderson_depth=int(ua.get("andersonDepth", 10)),
+                              anderson_mix=float(ua.get("andersonMix", 0.1)),
+                              anderson_start=int(ua.get("andersonStart", 0)))
+            upf = ua.get("updatefields")
+            if upf is not None and [str(x) for x in upf] != fields:
+                raise InputError("updatefields must list the monomerDens PhysFields in declaration order")
+            names = [i.name for i in interactions]
+            wanted = ua.get("interactions")
+            if wanted is not None:
+                interactions = [interactions[names.index(str(x))] for x in wanted]
+    if updater is None:
+        raise InputError("no <Updater> found")
+    return ScftConfig(n=n, cell=cell, fields=fields, polymers=polymers, interactions=interactions,
+                      updater=updater, seed=int(ra.get("randomSeed", 0)),
+                      precision=str(ra.get("precision", "fp64")), nsteps=int(ra.get("nsteps", 1)),
+                      device=int(ra.get("device", 0)))
+
+
+def config_from_file(path: str | Path) -> ScftConfig:
+    return config_from_text(Path(path).read_text())

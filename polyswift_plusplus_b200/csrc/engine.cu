@@ -1,0 +1,1064 @@
+// Host engine and C-ABI of the B200 SCFT inner loop.
+//
+// ps_handle owns every device buffer of one SCFT instance: w, phi, p (FP64),
+// the propagator slices of each sweep (FP64 or FP32), the half spectra, the
+// Boltzmann factors, the k^2 tables, reduction scratch and the Anderson
+// history.  One CUDA stream per handle; an iteration is captured once into a
+// CUDA graph and replayed.
+//
+// Semantics follow PsDomain::update (pstrol/PsDomain.cpp:332-372): densities
+// reset, PsBlockCopolymer::update for each polymer, then the updater with F
+// evaluated on the updated w (pseffhamil/PsSteepDUpdater.cpp:200-201).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pswift.h"
+#include "field_kernels.cuh"
+#include "kernels.h"
+#include "mt19937.h"
+
+namespace psb {
+
+static thread_local std::string g_thread_err;
+
+enum { HEAD = 0, TAIL = 1 };
+
+struct Seg {
+  int block;
+  int from;   // HEAD: this sweep produces the block's qs; TAIL: its qts
+  int off;    // slice offset of the segment inside the sweep
+  int steps;
+  int wfac_id;
+  int ktab_id;
+};
+
+struct Sweep {
+  int polymer;
+  std::vector<Seg> segs;
+  int total = 0;
+  int storage = -1;  // index of the executed sweep holding its slices
+};
+
+struct BlockMap {
+  int steps;
+  int field;
+  double ds, bseg;
+  int sweep_head, off_head;  // qs[n]  = slices(sweep_head)[off_head + n]
+  int sweep_tail, off_tail;  // qts[n] = slices(sweep_tail)[off_tail + n]
+};
+
+template <typename T> struct Buffers {
+  std::vector<T*> slices;        // per executed sweep: (total+1)*N
+  std::vector<c2_t<T>*> spec;    // per executed sweep
+  std::vector<T*> wfac;          // per (field, ds) key
+  std::vector<T*> kx, kyz;       // per (ds, bseg) key
+  c2_t<T>* tw_x = nullptr;
+  c2_t<T>* tw_y = nullptr;
+  c2_t<T>* tw_z = nullptr;
+  c2_t<T>* tw_zh = nullptr;
+  PlaneWork<T>* d_plane = nullptr;
+  PencilWork<T>* d_pencil = nullptr;
+};
+
+}  // namespace psb
+
+struct ps_handle {
+  ps_config cfg;
+  int n[3];
+  long long N = 0;
+  int nzh = 0;
+  int nf = 0;
+  int prec = PS_PREC_FP64;
+  int dev = 0;
+  bool fused_plane = true;
+  cudaStream_t st = nullptr;
+  std::string err;
+
+  double* d_w = nullptr;    // nf*N
+  double* d_phi = nullptr;  // nf*N
+  double* d_p = nullptr;
+  double* d_noise = nullptr;
+  double* h_noise = nullptr;  // pinned
+
+  std::vector<std::vector<psb::BlockMap>> blocks;
+  std::vector<double> alpha;  // length ratios
+  std::vector<psb::Sweep> sweeps;
+  std::vector<int> exec;  // sweep indices that are executed (own storage)
+  std::vector<std::pair<int, double>> wfac_keys;
+  std::vector<std::pair<double, double>> ktab_keys;
+  int kmax = 0;
+  std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
+
+  psb::Buffers<float> bf;
+  psb::Buffers<double> bd;
+
+  double* d_qpart = nullptr;
+  double* d_upart = nullptr;
+  psb::DevScalars* d_sc = nullptr;
+  psb::DevScalars* h_sc = nullptr;  // pinned
+  psb::FieldModel fm;
+
+  // Anderson history
+  int am_slots = 0;
+  double* d_hw = nullptr;
+  double* d_hd = nullptr;
+  double* d_gram = nullptr;
+  double* d_gpart = nullptr;
+
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int eager_iters = 0;
+  long long launches_per_iter = 0;
+
+  psb::Mt19937 rng;
+  long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
+  long long iterations = 0;
+
+  // Sweep timing: CUDA events around the propagator sweeps of each iteration.
+  int timing_cap = 0;
+  int timing_count = 0;
+  cudaEvent_t ev_cap_start = nullptr, ev_cap_end = nullptr;  // recorded during capture
+  std::vector<cudaEvent_t> ev_start, ev_end;                 // one pair per sample
+  cudaGraphNode_t node_start = nullptr, node_end = nullptr;  // event-record nodes in the graph
+  bool graph_has_timing = false;
+  std::vector<float> eager_ms;  // samples taken on eager iterations
+  double sweep_bytes = 0.0;  // algorithmic bytes of the sweeps of one iteration
+  long long sweep_steps = 0; // propagator steps (all sweeps) of one iteration
+};
+
+namespace psb {
+
+#define PS_CUDA(h, call)                                                               \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+      return PS_GPU_ERR;                                                               \
+    }                                                                                  \
+  } while (0)
+
+// PsBlockBase::setBlockSteps (psbase/PsBlockBase.cpp:252-326).
+static int set_block_steps(double bs, int force, int* out, std::string& err) {
+  long bsint;
+  const double intpart = (double)((long)bs);
+  const double dx = bs - intpart;
+  if (force) {
+    bsint = (long)floor(bs + 0.5);
+  } else {
+    if ((dx > 0.0001) && (dx < 0.9999)) {
+      char b[160];
+      snprintf(b, sizeof(b), "non-integer # of block steps: blockSteps = %.17g", bs);
+      err = b;
+      return PS_INPUT_ERR;
+    }
+    const long c = (long)ceil(bs), f = (long)floor(bs);
+    if (c == f) bsint = c;
+    else if (fabs(bs - (double)c) < fabs(bs - (double)f)) bsint = c;
+    else bsint = f;
+  }
+  if (bsint < 4) {
+    err = "# of block steps too small (< 4)";
+    return PS_INPUT_ERR;
+  }
+  *out = (int)bsint;
+  return PS_OK;
+}
+
+// Connection end of block `to` that block `from` attaches to
+// (PsBlockCopolymer::buildCntBlockType, pspolymer/PsBlockCopolymer.cpp:157-182).
+static int joined_end(const ps_polymer_config& P, int from, int to) {
+  const ps_block_config& B = P.blocks[to];
+  for (int t = 0; t < B.n_tail; ++t)
+    if (B.tail_joined[t] == from) return TAIL;
+  return HEAD;
+}
+
+// Linear-chain sweeps of one polymer.  Returns false for branched or
+// inconsistent architectures.
+static bool chain_sweeps(const ps_polymer_config& P, std::vector<std::pair<int, int>>& order) {
+  const int nb = P.n_blocks;
+  auto conns = [&](int b, int e) -> std::vector<int> {
+    const ps_block_config& B = P.blocks[b];
+    std::vector<int> v;
+    if (e == HEAD) v.assign(B.head_joined, B.head_joined + B.n_head);
+    else v.assign(B.tail_joined, B.tail_joined + B.n_tail);
+    return v;
+  };
+  for (int b = 0; b < nb; ++b)
+    for (int e = 0; e < 2; ++e) {
+      auto c = conns(b, e);
+      if (c.size() > 1) return false;
+      if (c.size() == 1) {
+        const int to = c[0];
+        if (to < 0 || to >= nb || to == b) return false;
+        const int te = joined_end(P, b, to);
+        auto back = conns(to, te);
+        if (back.size() != 1 || back[0] != b) return false;
+      }
+    }
+  int sb = -1, se = -1;
+  for (int b = 0; b < nb && sb < 0; ++b) {
+    if (P.blocks[b].n_head == 0) { sb = b; se = HEAD; }
+    else if (P.blocks[b].n_tail == 0) { sb = b; se = TAIL; }
+  }
+  if (sb < 0) return false;
+  std::vector<int> seen(nb, 0);
+  int b = sb, e = se;
+  while (true) {
+    if (seen[b]) return false;
+    seen[b] = 1;
+    order.push_back({b, e});
+    const int o = (e == HEAD) ? TAIL : HEAD;
+    auto c = conns(b, o);
+    if (c.empty()) break;
+    const int to = c[0];
+    e = joined_end(P, b, to);
+    b = to;
+  }
+  for (int i = 0; i < nb; ++i)
+    if (!seen[i]) return false;
+  return true;
+}
+
+template <typename T> Buffers<T>& bufs(ps_handle* h);
+template <> Buffers<float>& bufs<float>(ps_handle* h) { return h->bf; }
+template <> Buffers<double>& bufs<double>(ps_handle* h) { return h->bd; }
+
+template <typename T>
+static int alloc_copy(ps_handle* h, T** dst, const std::vector<T>& src) {
+  PS_CUDA(h, cudaMalloc((void**)dst, sizeof(T) * std::max<size_t>(src.size(), 1)));
+  PS_CUDA(h, cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+  return PS_OK;
+}
+
+template <typename T>
+static int make_twiddles(ps_handle* h, c2_t<T>** dst, int L) {
+  std::vector<c2_t<T>> tw(std::max(L, 1));
+  const double twopi = 2.0 * acos(-1.0);
+  for (int m = 0; m < L; ++m) {
+    const double a = twopi * (double)m / (double)L;
+    tw[m].x = (T)cos(a);
+    tw[m].y = (T)(-sin(a));
+  }
+  return alloc_copy(h, dst, tw);
+}
+
+// Separable exp(-ds b^2 k^2): kx carries the 1/N of the unnormalised pair
+// (pspolymer/PsFlexPseudoSpec.cpp:152, :188-206; psbase/PsGridField.cpp:66-104).
+static double kcomp(int i, int n, double dx) {
+  const double twopi = 2.0 * acos(-1.0);
+  const double n2 = (double)n / 2.0;
+  const double nk = n2 - fabs((double)i - n2);
+  double k = twopi * nk / (double)n;
+  return k / dx;
+}
+
+template <typename T>
+static int build_device_tables(ps_handle* h) {
+  Buffers<T>& B = bufs<T>(h);
+  const long long N = h->N;
+  // slices + spectra
+  for (int s : h->exec) {
+    const Sweep& sw = h->sweeps[s];
+    T* sl = nullptr;
+    PS_CUDA(h, cudaMalloc((void**)&sl, sizeof(T) * (size_t)(sw.total + 1) * N));
+    B.slices.push_back(sl);
+    c2_t<T>* sp = nullptr;
+    PS_CUDA(h, cudaMalloc((void**)&sp, sizeof(c2_t<T>) * (size_t)h->n[0] * h->n[1] * h->nzh));
+    B.spec.push_back(sp);
+  }
+  for (size_t i = 0; i < h->wfac_keys.size(); ++i) {
+    T* wf = nullptr;
+    PS_CUDA(h, cudaMalloc((void**)&wf, sizeof(T) * (size_t)N));
+    B.wfac.push_back(wf);
+  }
+  for (auto& kk : h->ktab_keys) {
+    const double ds = kk.first, b = kk.second;
+    std::vector<T> kx(h->n[0]), kyz((size_t)h->n[1] * h->nzh);
+    for (int i = 0; i < h->n[0]; ++i) {
+      const double k = kcomp(i, h->n[0], h->cfg.cell[0]);
+      kx[i] = (T)(exp(-1.0 * ds * (k * k) * b * b) / (double)N);
+    }
+    for (int j = 0; j < h->n[1]; ++j) {
+      const double ky = kcomp(j, h->n[1], h->cfg.cell[1]);
+      for (int kz = 0; kz < h->nzh; ++kz) {
+        const double kzv = kcomp(kz, h->n[2], h->cfg.cell[2]);
+        kyz[(size_t)j * h->nzh + kz] =
+            (T)(exp(-1.0 * ds * (ky * ky) * b * b) * exp(-1.0 * ds * (kzv * kzv) * b * b));
+      }
+    }
+    T* dkx = nullptr;
+    T* dkyz = nullptr;
+    int rc = alloc_copy(h, &dkx, kx);
+    if (rc) return rc;
+    rc = alloc_copy(h, &dkyz, kyz);
+    if (rc) return rc;
+    B.kx.push_back(dkx);
+    B.kyz.push_back(dkyz);
+  }
+  int rc = make_twiddles<T>(h, &B.tw_x, h->n[0]);
+  if (!rc) rc = make_twiddles<T>(h, &B.tw_y, h->n[1]);
+  if (!rc) rc = make_twiddles<T>(h, &B.tw_z, h->n[2]);
+  if (!rc) rc = make_twiddles<T>(h, &B.tw_zh, std::max(h->n[2] / 2, 1));
+  if (rc) return rc;
+
+  // Work tables for every global step.
+  std::vector<PlaneWork<T>> pw;
+  std::vector<PencilWork<T>> xw;
+  h->plane_off.assign(h->kmax + 1, 0);
+  h->plane_cnt.assign(h->kmax + 1, 0);
+  h->pencil_off.assign(h->kmax + 1, 0);
+  h->pencil_cnt.assign(h->kmax + 1, 0);
+  auto seg_of = [&](const Sweep& sw, int step) -> const Seg& {
+    for (const Seg& g : sw.segs)
+      if (step >= g.off && step < g.off + g.steps) return g;
+    return sw.segs.back();
+  };
+  for (int k = 0; k <= h->kmax; ++k) {
+    h->plane_off[k] = (int)pw.size();
+    h->pencil_off[k] = (int)xw.size();
+    for (size_t e = 0; e < h->exec.size(); ++e) {
+      const Sweep& sw = h->sweeps[h->exec[e]];
+      if (k > sw.total) continue;
+      PlaneWork<T> w;
+      memset(&w, 0, sizeof(w));
+      w.mode = (k == 0) ? MODE_FIRST : (k == sw.total ? MODE_LAST : MODE_MID);
+      w.src = nullptr;
+      w.spec = B.spec[e];
+      w.wfac_in = (k > 0) ? B.wfac[seg_of(sw, k - 1).wfac_id] : nullptr;
+      w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
+      w.store = B.slices[e] + (size_t)k * N;
+      pw.push_back(w);
+      if (k < sw.total) {
+        PencilWork<T> x;
+        memset(&x, 0, sizeof(x));
+        x.spec = B.spec[e];
+        x.kx = B.kx[seg_of(sw, k).ktab_id];
+        x.kyz = B.kyz[seg_of(sw, k).ktab_id];
+        xw.push_back(x);
+      }
+    }
+    h->plane_cnt[k] = (int)pw.size() - h->plane_off[k];
+    h->pencil_cnt[k] = (int)xw.size() - h->pencil_off[k];
+  }
+  rc = alloc_copy(h, &B.d_plane, pw);
+  if (!rc) rc = alloc_copy(h, &B.d_pencil, xw);
+  return rc;
+}
+
+// Launch the propagator sweeps of one iteration.
+template <typename T>
+static int launch_sweeps(ps_handle* h, long long* nlaunch) {
+  Buffers<T>& B = bufs<T>(h);
+  const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+  for (int k = 0; k <= h->kmax; ++k) {
+    const PlaneWork<T>* pw = B.d_plane + h->plane_off[k];
+    const int np = h->plane_cnt[k];
+    const PencilWork<T>* xw = B.d_pencil + h->pencil_off[k];
+    const int nxw = h->pencil_cnt[k];
+    if (h->fused_plane) {
+      PS_CUDA(h, launch_plane<T>(pw, np, nx, ny, nz, B.tw_y, B.tw_zh, B.tw_z, h->st));
+      ++*nlaunch;
+      if (nxw > 0) {
+        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz, h->st));
+        ++*nlaunch;
+      }
+    } else {
+      PS_CUDA(h, launch_rows<T>(pw, np, nx * ny, nz, B.tw_zh, B.tw_z, h->st));
+      ++*nlaunch;
+      if (nxw > 0) {
+        if (ny > 1) {
+          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_FWD, ny, nx, h->nzh, B.tw_y, nx, ny, nz, h->st));
+          ++*nlaunch;
+        }
+        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz, h->st));
+        ++*nlaunch;
+        if (ny > 1) {
+          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_INV, ny, nx, h->nzh, B.tw_y, nx, ny, nz, h->st));
+          ++*nlaunch;
+        }
+      }
+    }
+  }
+  return PS_OK;
+}
+
+template <typename T>
+static int launch_iteration(ps_handle* h, long long* nlaunch) {
+  Buffers<T>& B = bufs<T>(h);
+  const long long N = h->N;
+  PS_CUDA(h, launch_zero(h->d_phi, (long long)h->nf * N, h->st));
+  ++*nlaunch;
+  for (size_t i = 0; i < h->wfac_keys.size(); ++i) {
+    const int f = h->wfac_keys[i].first;
+    const double ds = h->wfac_keys[i].second;
+    PS_CUDA(h, launch_wfac<T>(h->d_w + (size_t)f * N, B.wfac[i], -0.5 * ds, N, h->st));
+    ++*nlaunch;
+  }
+  if (h->timing_cap > 0) PS_CUDA(h, cudaEventRecord(h->ev_cap_start, h->st));
+  int rc = launch_sweeps<T>(h, nlaunch);
+  if (rc) return rc;
+  if (h->timing_cap > 0) PS_CUDA(h, cudaEventRecord(h->ev_cap_end, h->st));
+  auto slice = [&](int sweep, int idx) -> const T* {
+    return B.slices[h->sweeps[sweep].storage] + (size_t)idx * N;
+  };
+  for (int ip = 0; ip < h->cfg.n_polymers; ++ip) {
+    const BlockMap& b0 = h->blocks[ip][0];
+    PS_CUDA(h, launch_dot_partials<T>(slice(b0.sweep_head, b0.off_head),
+                                      slice(b0.sweep_tail, b0.off_tail + b0.steps), N, h->d_qpart,
+                                      h->st));
+    PS_CUDA(h, launch_finalize_q(h->d_qpart, (double)N, ip, h->d_sc, h->st));
+    *nlaunch += 2;
+  }
+  for (int ip = 0; ip < h->cfg.n_polymers; ++ip) {
+    const double vf = h->cfg.polymers[ip].volfrac;
+    const double densfac = 1.0 * vf / h->alpha[ip];
+    for (size_t ib = 0; ib < h->blocks[ip].size(); ++ib) {
+      const BlockMap& b = h->blocks[ip][ib];
+      PS_CUDA(h, launch_quadrature<T>(slice(b.sweep_head, b.off_head), slice(b.sweep_tail, b.off_tail),
+                                      b.steps, N, b.ds, densfac, h->d_sc, ip,
+                                      h->d_phi + (size_t)b.field * N, h->st));
+      ++*nlaunch;
+    }
+  }
+  FieldPtrs fp;
+  memset(&fp, 0, sizeof(fp));
+  for (int i = 0; i < h->nf; ++i) {
+    fp.w[i] = h->d_w + (size_t)i * N;
+    fp.phi[i] = h->d_phi + (size_t)i * N;
+  }
+  fp.p = h->d_p;
+  fp.noise = (h->cfg.updater.noise != 0.0) ? h->d_noise : nullptr;
+  if (h->cfg.updater.kind == PS_UPD_ANDERSON) {
+    const int m = h->cfg.updater.anderson_depth;
+    PS_CUDA(h, launch_am_residual(h->fm, fp, h->d_hw, h->d_hd, h->am_slots, h->d_sc, h->d_upart, h->st));
+    PS_CUDA(h, launch_am_gram((long long)h->nf * N, h->d_hd, h->am_slots, m, h->d_sc, h->d_gpart, h->st));
+    PS_CUDA(h, launch_am_solve(h->d_gpart, h->d_gram, h->am_slots, m, h->cfg.updater.anderson_start,
+                               h->cfg.updater.anderson_mix, h->cfg.updater.lambda0, h->d_sc, h->st));
+    PS_CUDA(h, launch_am_mix(h->fm, fp, h->d_hw, h->d_hd, h->am_slots, h->d_sc, h->d_upart, h->st));
+    PS_CUDA(h, launch_update_finalize_am(h->fm, h->d_upart, h->d_sc, h->st));
+    *nlaunch += 5;
+  } else {
+    PS_CUDA(h, launch_sd_update(h->fm, fp, h->d_upart, h->st));
+    PS_CUDA(h, launch_update_finalize(h->fm, h->d_upart, h->d_sc, h->st));
+    *nlaunch += 2;
+  }
+  PS_CUDA(h, launch_pressure_shift(h->d_p, N, h->d_sc, h->st));
+  ++*nlaunch;
+  return PS_OK;
+}
+
+static int run_iteration(ps_handle* h, long long* nlaunch) {
+  return (h->prec == PS_PREC_MIXED) ? launch_iteration<float>(h, nlaunch)
+                                    : launch_iteration<double>(h, nlaunch);
+}
+
+// Gaussian draws the reference makes every iteration even at noise = 0
+// (pseffhamil/PsPolymerUpdater.cpp:263-295); they are owed to the stream and
+// drawn lazily before anything else reads it.
+static void settle_rng(ps_handle* h) {
+  while (h->pending_gauss > 0) {
+    (void)h->rng.gauss();
+    --h->pending_gauss;
+  }
+}
+
+static int prepare_noise(ps_handle* h) {
+  const double s = h->cfg.updater.noise;
+  if (s == 0.0) {
+    h->pending_gauss += (long long)h->nf * h->N;
+    return PS_OK;
+  }
+  settle_rng(h);
+  const long long n = (long long)h->nf * h->N;
+  for (long long i = 0; i < n; ++i) h->h_noise[i] = s * h->rng.gauss();
+  PS_CUDA(h, cudaMemcpyAsync(h->d_noise, h->h_noise, sizeof(double) * (size_t)n,
+                             cudaMemcpyHostToDevice, h->st));
+  return PS_OK;
+}
+
+static void free_all(ps_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  f(h->d_w); f(h->d_phi); f(h->d_p); f(h->d_noise);
+  if (h->h_noise) cudaFreeHost(h->h_noise);
+  for (auto p : h->bf.slices) f(p);
+  for (auto p : h->bf.spec) f(p);
+  for (auto p : h->bf.wfac) f(p);
+  for (auto p : h->bf.kx) f(p);
+  for (auto p : h->bf.kyz) f(p);
+  f(h->bf.tw_x); f(h->bf.tw_y); f(h->bf.tw_z); f(h->bf.tw_zh); f(h->bf.d_plane); f(h->bf.d_pencil);
+  for (auto p : h->bd.slices) f(p);
+  for (auto p : h->bd.spec) f(p);
+  for (auto p : h->bd.wfac) f(p);
+  for (auto p : h->bd.kx) f(p);
+  for (auto p : h->bd.kyz) f(p);
+  f(h->bd.tw_x); f(h->bd.tw_y); f(h->bd.tw_z); f(h->bd.tw_zh); f(h->bd.d_plane); f(h->bd.d_pencil);
+  f(h->d_qpart); f(h->d_upart); f(h->d_sc);
+  if (h->h_sc) cudaFreeHost(h->h_sc);
+  f(h->d_hw); f(h->d_hd); f(h->d_gram); f(h->d_gpart);
+  if (h->ev_cap_start) cudaEventDestroy(h->ev_cap_start);
+  if (h->ev_cap_end) cudaEventDestroy(h->ev_cap_end);
+  for (auto e : h->ev_start) cudaEventDestroy(e);
+  for (auto e : h->ev_end) cudaEventDestroy(e);
+  if (h->st) cudaStreamDestroy(h->st);
+}
+
+static int create_impl(ps_handle* h, const ps_config* cfg) {
+  h->cfg = *cfg;
+  const ps_config& c = *cfg;
+  for (int d = 0; d < 3; ++d) {
+    h->n[d] = c.n[d];
+    if (!extent_supported(c.n[d])) {
+      h->err = "unsupported grid extent " + std::to_string(c.n[d]) +
+               " (supported: 1,4,8,12,16,24,32,48,64,96,128,256)";
+      return PS_INPUT_ERR;
+    }
+    if (!(c.cell[d] > 0.0)) {
+      h->err = "cellSizes must be positive";
+      return PS_ATTRIB_ERR;
+    }
+  }
+  h->N = (long long)c.n[0] * c.n[1] * c.n[2];
+  h->nzh = c.n[2] / 2 + 1;
+  h->nf = c.n_fields;
+  h->prec = c.precision;
+  if (h->prec != PS_PREC_FP64 && h->prec != PS_PREC_MIXED) {
+    h->err = "precision must be PS_PREC_FP64 or PS_PREC_MIXED";
+    return PS_ATTRIB_ERR;
+  }
+  if (h->nf < 2 || h->nf > 3) {
+    h->err = "n_fields must be 2 or 3 (the steepest-descent updater supports 2 or 3)";
+    return PS_ATTRIB_ERR;
+  }
+  if (c.n_polymers < 1 || c.n_polymers > PS_MAX_POLYMERS) {
+    h->err = "n_polymers out of range";
+    return PS_ATTRIB_ERR;
+  }
+  if (c.n_interactions < 0 || c.n_interactions > PS_MAX_INTERACTIONS) {
+    h->err = "n_interactions out of range";
+    return PS_ATTRIB_ERR;
+  }
+  if (c.updater.kind == PS_UPD_ANDERSON &&
+      (c.updater.anderson_depth < 1 || c.updater.anderson_depth > 32)) {
+    h->err = "anderson_depth must be in 1..32";
+    return PS_ATTRIB_ERR;
+  }
+  // Polymers, blocks, steps, density averages (psbase/PsBlockBase.cpp:163-204,
+  // pspolymer/PsPolymerHldr.cpp:67-83, pspolymer/PsBlockCopolymer.cpp:113-127).
+  const double scale_len = (double)c.polymers[0].length;
+  double dens_avg[PS_MAX_FIELDS] = {0, 0, 0, 0};
+  double vtot = 0.0;
+  h->blocks.resize(c.n_polymers);
+  for (int ip = 0; ip < c.n_polymers; ++ip) {
+    const ps_polymer_config& P = c.polymers[ip];
+    if (P.n_blocks < 1 || P.n_blocks > PS_MAX_BLOCKS) {
+      h->err = "polymer " + std::to_string(ip) + ": n_blocks out of range";
+      return PS_ATTRIB_ERR;
+    }
+    if (P.length <= 0) {
+      h->err = "polymer " + std::to_string(ip) + ": length must be positive";
+      return PS_ATTRIB_ERR;
+    }
+    const double alpha = (double)P.length / scale_len;
+    h->alpha.push_back(alpha);
+    vtot += P.volfrac;
+    double ftot = 0.0;
+    for (int ib = 0; ib < P.n_blocks; ++ib) ftot = ftot + P.blocks[ib].lengthfrac;
+    if (fabs(ftot - 1.0) > 0.00001) {
+      h->err = "polymer " + std::to_string(ip) + ": |totalFrac - 1.0| > tolerance";
+      return PS_INPUT_ERR;
+    }
+    for (int ib = 0; ib < P.n_blocks; ++ib) {
+      const ps_block_config& B = P.blocks[ib];
+      if (B.field < 0 || B.field >= h->nf) {
+        h->err = "block field index out of range";
+        return PS_ATTRIB_ERR;
+      }
+      if (!(B.ds > 0.0)) {
+        h->err = "ds not set";
+        return PS_ATTRIB_ERR;
+      }
+      dens_avg[B.field] = dens_avg[B.field] + 1.0 * B.lengthfrac * P.volfrac;
+      BlockMap bm;
+      memset(&bm, 0, sizeof(bm));
+      std::string e2;
+      int rc = set_block_steps(alpha * B.lengthfrac / B.ds, B.force_block_steps, &bm.steps, e2);
+      if (rc) {
+        h->err = "polymer " + std::to_string(ip) + " block " + std::to_string(ib) + ": " + e2;
+        return rc;
+      }
+      bm.field = B.field;
+      bm.ds = B.ds;
+      bm.bseg = (B.bseg_ratio > 0.0) ? B.bseg_ratio : 1.0;
+      h->blocks[ip].push_back(bm);
+    }
+  }
+  if (fabs(vtot - 1.0) > 0.00001) {
+    h->err = "sum of polymer volume fractions != 1";
+    return PS_INPUT_ERR;
+  }
+  // Sweeps
+  for (int ip = 0; ip < c.n_polymers; ++ip) {
+    const ps_polymer_config& P = c.polymers[ip];
+    std::vector<std::pair<int, int>> order;
+    if (!chain_sweeps(P, order)) {
+      h->err = "polymer " + std::to_string(ip) +
+               ": only linear block sequences run on the device path";
+      return PS_INPUT_ERR;
+    }
+    Sweep a, b;
+    a.polymer = b.polymer = ip;
+    for (auto& be : order) {
+      Seg g;
+      g.block = be.first;
+      g.from = be.second;
+      g.off = a.total;
+      g.steps = h->blocks[ip][g.block].steps;
+      g.wfac_id = g.ktab_id = -1;
+      a.segs.push_back(g);
+      a.total += g.steps;
+    }
+    for (int i = (int)order.size() - 1; i >= 0; --i) {
+      Seg g;
+      g.block = order[i].first;
+      g.from = (order[i].second == HEAD) ? TAIL : HEAD;
+      g.off = b.total;
+      g.steps = h->blocks[ip][g.block].steps;
+      g.wfac_id = g.ktab_id = -1;
+      b.segs.push_back(g);
+      b.total += g.steps;
+    }
+    // Mirror-symmetric chains (homopolymers, ABA) give identical sweeps.
+    bool same = (a.segs.size() == b.segs.size());
+    for (size_t i = 0; same && i < a.segs.size(); ++i) {
+      const BlockMap& x = h->blocks[ip][a.segs[i].block];
+      const BlockMap& y = h->blocks[ip][b.segs[i].block];
+      same = (x.field == y.field && x.steps == y.steps && x.ds == y.ds && x.bseg == y.bseg);
+    }
+    const int ia = (int)h->sweeps.size();
+    a.storage = (int)h->exec.size();
+    h->exec.push_back(ia);
+    h->sweeps.push_back(a);
+    if (same) {
+      b.storage = a.storage;
+    } else {
+      b.storage = (int)h->exec.size();
+      h->exec.push_back(ia + 1);
+    }
+    h->sweeps.push_back(b);
+    for (int which = 0; which < 2; ++which) {
+      const Sweep& sw = h->sweeps[ia + which];
+      for (const Seg& g : sw.segs) {
+        BlockMap& bm = h->blocks[ip][g.block];
+        if (g.from == HEAD) { bm.sweep_head = ia + which; bm.off_head = g.off; }
+        else { bm.sweep_tail = ia + which; bm.off_tail = g.off; }
+      }
+    }
+  }
+  // wfac / k-table keys
+  for (Sweep& sw : h->sweeps)
+    for (Seg& g : sw.segs) {
+      const BlockMap& bm = h->blocks[sw.polymer][g.block];
+      std::pair<int, double> wk(bm.field, bm.ds);
+      auto it = std::find(h->wfac_keys.begin(), h->wfac_keys.end(), wk);
+      if (it == h->wfac_keys.end()) {
+        g.wfac_id = (int)h->wfac_keys.size();
+        h->wfac_keys.push_back(wk);
+      } else {
+        g.wfac_id = (int)(it - h->wfac_keys.begin());
+      }
+      std::pair<double, double> kk(bm.ds, bm.bseg);
+      auto it2 = std::find(h->ktab_keys.begin(), h->ktab_keys.end(), kk);
+      if (it2 == h->ktab_keys.end()) {
+        g.ktab_id = (int)h->ktab_keys.size();
+        h->ktab_keys.push_back(kk);
+      } else {
+        g.ktab_id = (int)(it2 - h->ktab_keys.begin());
+      }
+    }
+  h->kmax = 0;
+  for (int s : h->exec) h->kmax = std::max(h->kmax, h->sweeps[s].total);
+  // Field model
+  FieldModel& fm = h->fm;
+  memset(&fm, 0, sizeof(fm));
+  fm.nf = h->nf;
+  fm.n_int = c.n_interactions;
+  for (int it = 0; it < c.n_interactions; ++it) {
+    const ps_interaction_config& I = c.interactions[it];
+    if (I.field_a < 0 || I.field_a >= h->nf || I.field_b < 0 || I.field_b >= h->nf ||
+        I.field_a == I.field_b) {
+      h->err = "interaction scfields out of range";
+      return PS_ATTRIB_ERR;
+    }
+    fm.int_a[it] = I.field_a;
+    fm.int_b[it] = I.field_b;
+    fm.chin[it] = I.chi * scale_len;
+  }
+  for (int i = 0; i < h->nf; ++i) fm.dens_avg[i] = dens_avg[i];
+  fm.lambda0 = c.updater.lambda0;
+  fm.lambda1 = c.updater.lambda1;
+  fm.npol = c.n_polymers;
+  for (int ip = 0; ip < c.n_polymers; ++ip) {
+    fm.vf[ip] = c.polymers[ip].volfrac;
+    fm.alpha[ip] = h->alpha[ip];
+  }
+  fm.N = h->N;
+
+  // Device
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    h->err = "no CUDA device available";
+    return PS_GPU_ERR;
+  }
+  h->dev = c.device;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  const int pb = (h->prec == PS_PREC_MIXED) ? 4 : 8;
+  h->fused_plane = plane_fused_supported(pb, c.n[1], c.n[2]);
+  const size_t nfN = (size_t)h->nf * h->N;
+  PS_CUDA(h, cudaMalloc((void**)&h->d_w, sizeof(double) * nfN));
+  PS_CUDA(h, cudaMalloc((void**)&h->d_phi, sizeof(double) * nfN));
+  PS_CUDA(h, cudaMalloc((void**)&h->d_p, sizeof(double) * (size_t)h->N));
+  PS_CUDA(h, cudaMemset(h->d_w, 0, sizeof(double) * nfN));
+  PS_CUDA(h, cudaMemset(h->d_phi, 0, sizeof(double) * nfN));
+  PS_CUDA(h, cudaMemset(h->d_p, 0, sizeof(double) * (size_t)h->N));
+  if (c.updater.noise != 0.0) {
+    PS_CUDA(h, cudaMalloc((void**)&h->d_noise, sizeof(double) * nfN));
+    PS_CUDA(h, cudaMallocHost((void**)&h->h_noise, sizeof(double) * nfN));
+  }
+  PS_CUDA(h, cudaMalloc((void**)&h->d_qpart, sizeof(double) * kRedBlocks));
+  PS_CUDA(h, cudaMalloc((void**)&h->d_upart, sizeof(double) * kRedBlocks * kUpdQ));
+  PS_CUDA(h, cudaMemset(h->d_upart, 0, sizeof(double) * kRedBlocks * kUpdQ));
+  PS_CUDA(h, cudaMalloc((void**)&h->d_sc, sizeof(DevScalars)));
+  PS_CUDA(h, cudaMemset(h->d_sc, 0, sizeof(DevScalars)));
+  PS_CUDA(h, cudaMallocHost((void**)&h->h_sc, sizeof(DevScalars)));
+  if (c.updater.kind == PS_UPD_ANDERSON) {
+    const int m = c.updater.anderson_depth;
+    h->am_slots = m + 1;
+    PS_CUDA(h, cudaMalloc((void**)&h->d_hw, sizeof(double) * nfN * h->am_slots));
+    PS_CUDA(h, cudaMalloc((void**)&h->d_hd, sizeof(double) * nfN * h->am_slots));
+    PS_CUDA(h, cudaMalloc((void**)&h->d_gram, sizeof(double) * h->am_slots * h->am_slots));
+    PS_CUDA(h, cudaMemset(h->d_gram, 0, sizeof(double) * h->am_slots * h->am_slots));
+    PS_CUDA(h, cudaMalloc((void**)&h->d_gpart, sizeof(double) * kRedBlocks * 33));
+  }
+  int rc = (h->prec == PS_PREC_MIXED) ? build_device_tables<float>(h) : build_device_tables<double>(h);
+  if (rc) return rc;
+  h->rng.seed_((uint32_t)(c.seed & 0xffffffffULL));
+  // Algorithmic bytes of one propagator step: read q(s), read wfac, write q(s+ds).
+  h->sweep_steps = 0;
+  for (int s : h->exec) h->sweep_steps += h->sweeps[s].total;
+  h->sweep_bytes = 3.0 * (double)h->N * (double)pb * (double)h->sweep_steps;
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+static int check_scalars(ps_handle* h) {
+  PS_CUDA(h, cudaMemcpyAsync(h->h_sc, h->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->h_sc->error_flags & 1) {
+    h->err = "PsBlock::calcBigQ() found nan/inf?";
+    return PS_RUN_ERR;
+  }
+  if (h->h_sc->error_flags & 2) {
+    h->err = "non-finite free energy";
+    return PS_RUN_ERR;
+  }
+  return PS_OK;
+}
+
+static int iterate_impl(ps_handle* h, int n) {
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  const bool use_graph = (h->cfg.updater.noise == 0.0);
+  for (int it = 0; it < n; ++it) {
+    int rc = prepare_noise(h);
+    if (rc) return rc;
+    const bool sample = h->timing_cap > 0 && h->timing_count < h->timing_cap;
+    if (!use_graph || h->eager_iters < 1) {
+      long long nl = 0;
+      rc = run_iteration(h, &nl);
+      if (rc) return rc;
+      if (sample) {
+        // eager iteration: the capture events hold this iteration's interval
+        PS_CUDA(h, cudaEventSynchronize(h->ev_cap_end));
+        float ms = 0.f;
+        PS_CUDA(h, cudaEventElapsedTime(&ms, h->ev_cap_start, h->ev_cap_end));
+        h->eager_ms.push_back(ms);
+      }
+      h->launches_per_iter = nl;
+      h->eager_iters++;
+    } else {
+      if (!h->gexec) {
+        long long nl = 0;
+        PS_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        rc = run_iteration(h, &nl);
+        cudaGraph_t g = nullptr;
+        cudaError_t ec = cudaStreamEndCapture(h->st, &g);
+        if (rc) {
+          if (g) cudaGraphDestroy(g);
+          return rc;
+        }
+        if (ec != cudaSuccess) {
+          h->err = std::string("graph capture: ") + cudaGetErrorString(ec);
+          return PS_GPU_ERR;
+        }
+        h->graph = g;
+        PS_CUDA(h, cudaGraphInstantiate(&h->gexec, h->graph, 0));
+        h->launches_per_iter = nl;
+        h->graph_has_timing = false;
+        if (h->timing_cap > 0) {
+          size_t nn = 0;
+          PS_CUDA(h, cudaGraphGetNodes(h->graph, nullptr, &nn));
+          std::vector<cudaGraphNode_t> nodes(nn);
+          PS_CUDA(h, cudaGraphGetNodes(h->graph, nodes.data(), &nn));
+          for (auto nd : nodes) {
+            cudaGraphNodeType ty;
+            PS_CUDA(h, cudaGraphNodeGetType(nd, &ty));
+            if (ty != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev;
+            PS_CUDA(h, cudaGraphEventRecordNodeGetEvent(nd, &ev));
+            if (ev == h->ev_cap_start) h->node_start = nd;
+            if (ev == h->ev_cap_end) h->node_end = nd;
+          }
+          h->graph_has_timing = (h->node_start && h->node_end);
+        }
+      }
+      if (sample && h->graph_has_timing) {
+        PS_CUDA(h, cudaGraphExecEventRecordNodeSetEvent(h->gexec, h->node_start, h->ev_start[h->timing_count]));
+        PS_CUDA(h, cudaGraphExecEventRecordNodeSetEvent(h->gexec, h->node_end, h->ev_end[h->timing_count]));
+        h->timing_count++;
+      }
+      PS_CUDA(h, cudaGraphLaunch(h->gexec, h->st));
+    }
+    h->iterations++;
+  }
+  return check_scalars(h);
+}
+
+}  // namespace psb
+
+using namespace psb;
+
+extern "C" {
+
+const char* ps_version(void) { return "pswift-b200 0.1 (sm_100a)"; }
+
+const char* ps_gpu_last_error(const ps_handle* h) {
+  if (!h) return g_thread_err.c_str();
+  return h->err.c_str();
+}
+
+int ps_gpu_create(const ps_config* cfg, ps_handle** out) {
+  if (!cfg || !out) {
+    g_thread_err = "null argument";
+    return PS_ATTRIB_ERR;
+  }
+  *out = nullptr;
+  ps_handle* h = new ps_handle();
+  int rc = create_impl(h, cfg);
+  if (rc != PS_OK) {
+    g_thread_err = h->err;
+    free_all(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return PS_OK;
+}
+
+int ps_gpu_destroy(ps_handle* h) {
+  if (!h) return PS_OK;
+  cudaSetDevice(h->dev);
+  if (h->st) cudaStreamSynchronize(h->st);
+  free_all(h);
+  delete h;
+  return PS_OK;
+}
+
+int ps_gpu_block_steps(const ps_handle* h, int ip, int ib, int* steps) {
+  if (!h || !steps || ip < 0 || ip >= (int)h->blocks.size() || ib < 0 ||
+      ib >= (int)h->blocks[ip].size())
+    return PS_ATTRIB_ERR;
+  *steps = h->blocks[ip][ib].steps;
+  return PS_OK;
+}
+
+static double* field_ptr(ps_handle* h, int which, int index) {
+  if (which == PS_FIELD_PRES) return h->d_p;
+  if (index < 0 || index >= h->nf) return nullptr;
+  if (which == PS_FIELD_W) return h->d_w + (size_t)index * h->N;
+  if (which == PS_FIELD_PHI) return h->d_phi + (size_t)index * h->N;
+  return nullptr;
+}
+
+int ps_gpu_set_fields(ps_handle* h, int which, int index, const double* data, int on_device) {
+  if (!h || !data) return PS_ATTRIB_ERR;
+  double* dst = field_ptr(h, which, index);
+  if (!dst) {
+    h->err = "bad field selector";
+    return PS_ATTRIB_ERR;
+  }
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaMemcpyAsync(dst, data, sizeof(double) * (size_t)h->N,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->st));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_device) {
+  if (!h || !data) return PS_ATTRIB_ERR;
+  double* src = field_ptr(h, which, index);
+  if (!src) {
+    h->err = "bad field selector";
+    return PS_ATTRIB_ERR;
+  }
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaMemcpyAsync(data, src, sizeof(double) * (size_t)h->N,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->st));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+int ps_gpu_init_random(ps_handle* h) {
+  if (!h) return PS_ATTRIB_ERR;
+  settle_rng(h);
+  std::vector<double> buf((size_t)h->N);
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  for (int i = 0; i < h->nf; ++i) {
+    for (long long r = 0; r < h->N; ++r) {
+      const double u = h->rng.real();
+      buf[(size_t)r] = 1.0 * (u + (-0.5));
+    }
+    PS_CUDA(h, cudaMemcpy(h->d_w + (size_t)i * h->N, buf.data(), sizeof(double) * (size_t)h->N,
+                          cudaMemcpyHostToDevice));
+  }
+  PS_CUDA(h, cudaMemset(h->d_p, 0, sizeof(double) * (size_t)h->N));
+  return PS_OK;
+}
+
+int ps_gpu_iterate(ps_handle* h, int n_iter) {
+  if (!h) return PS_ATTRIB_ERR;
+  if (n_iter < 0) {
+    h->err = "n_iter must be >= 0";
+    return PS_ATTRIB_ERR;
+  }
+  return iterate_impl(h, n_iter);
+}
+
+int ps_gpu_get_scalars(ps_handle* h, ps_scalars* out) {
+  if (!h || !out) return PS_ATTRIB_ERR;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaMemcpyAsync(h->h_sc, h->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  const DevScalars& s = *h->h_sc;
+  memset(out, 0, sizeof(*out));
+  out->free_energy = s.free_energy;
+  out->free_energy_nodis = s.free_energy_nodis;
+  for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip) {
+    out->q[ip] = s.q[ip];
+    out->log_q[ip] = s.log_q[ip];
+  }
+  out->max_incomp = s.max_incomp;
+  out->dh_norm = s.dh_norm;
+  out->pressure_mean = s.pressure_mean;
+  out->iteration = s.iteration;
+  out->error_flags = s.error_flags;
+  return PS_OK;
+}
+
+int ps_gpu_get_propagator(ps_handle* h, int ip, int ib, int end, int n, double* out) {
+  if (!h || !out || ip < 0 || ip >= (int)h->blocks.size() || ib < 0 ||
+      ib >= (int)h->blocks[ip].size())
+    return PS_ATTRIB_ERR;
+  const BlockMap& b = h->blocks[ip][ib];
+  if (n < 0 || n > b.steps) {
+    h->err = "slice index out of range";
+    return PS_ATTRIB_ERR;
+  }
+  const int sweep = (end == PS_FROM_HEAD) ? b.sweep_head : b.sweep_tail;
+  const int off = (end == PS_FROM_HEAD) ? b.off_head : b.off_tail;
+  const int storage = h->sweeps[sweep].storage;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  const size_t N = (size_t)h->N;
+  if (h->prec == PS_PREC_MIXED) {
+    std::vector<float> tmp(N);
+    PS_CUDA(h, cudaMemcpy(tmp.data(), h->bf.slices[storage] + (size_t)(off + n) * N,
+                          sizeof(float) * N, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < N; ++i) out[i] = tmp[i];
+  } else {
+    PS_CUDA(h, cudaMemcpy(out, h->bd.slices[storage] + (size_t)(off + n) * N, sizeof(double) * N,
+                          cudaMemcpyDeviceToHost));
+  }
+  return PS_OK;
+}
+
+int ps_gpu_synchronize(ps_handle* h) {
+  if (!h) return PS_ATTRIB_ERR;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+// Kernel launches one iteration issues (all of them this library's kernels).
+long long ps_gpu_launches_per_iteration(const ps_handle* h) { return h ? h->launches_per_iter : 0; }
+
+void* ps_gpu_stream(const ps_handle* h) { return h ? (void*)h->st : nullptr; }
+
+int ps_gpu_enable_sweep_timing(ps_handle* h, int max_samples) {
+  if (!h || max_samples < 0) return PS_ATTRIB_ERR;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  h->node_start = h->node_end = nullptr;
+  h->graph_has_timing = false;
+  if (!h->ev_cap_start) PS_CUDA(h, cudaEventCreate(&h->ev_cap_start));
+  if (!h->ev_cap_end) PS_CUDA(h, cudaEventCreate(&h->ev_cap_end));
+  while ((int)h->ev_start.size() < max_samples) {
+    cudaEvent_t a, b;
+    PS_CUDA(h, cudaEventCreate(&a));
+    PS_CUDA(h, cudaEventCreate(&b));
+    h->ev_start.push_back(a);
+    h->ev_end.push_back(b);
+  }
+  h->timing_cap = max_samples;
+  h->timing_count = 0;
+  h->eager_ms.clear();
+  return PS_OK;
+}
+
+int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
+                        double* bytes_per_iter, long long* steps_per_iter) {
+  if (!h || !n_out) return PS_ATTRIB_ERR;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  int n = 0;
+  for (float ms : h->eager_ms) {
+    if (ms_out && n < max_out) ms_out[n] = ms;
+    ++n;
+  }
+  for (int i = 0; i < h->timing_count; ++i) {
+    float ms = 0.f;
+    PS_CUDA(h, cudaEventElapsedTime(&ms, h->ev_start[i], h->ev_end[i]));
+    if (ms_out && n < max_out) ms_out[n] = ms;
+    ++n;
+  }
+  *n_out = n;
+  if (bytes_per_iter) *bytes_per_iter = h->sweep_bytes;
+  if (steps_per_iter) *steps_per_iter = h->sweep_steps;
+  h->timing_count = 0;
+  h->eager_ms.clear();
+  return PS_OK;
+}
+
+}  // extern "C"

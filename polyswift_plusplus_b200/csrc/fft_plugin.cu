@@ -1,0 +1,191 @@
+// FFT plugin: PsFFTBase<double,3>::scaledFFTPair on the device
+// (psbase/PsFFTBase.h:105; serial semantics of psfft/PsFFTW.cpp:196-224).
+//
+// res = Re(IFFT(kdata * FFT(data))) with both transforms unnormalised.  The
+// reference computes it as a c2c pair of real data; here it is the same
+// plane / pencil kernels as the propagator (r2c -> pencils -> c2r) with the
+// k multiplier taken from the full real kdata array, symmetrised as
+// (kdata(k) + kdata(-k)) / 2, which is what the real part of the c2c result
+// sees.  Host arrays in and out (one H2D and one D2H copy per call).
+#include <math.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pswift.h"
+#include "kernels.h"
+
+namespace psb {
+static thread_local std::string g_fft_err;
+}
+
+struct ps_fft {
+  int n[3];
+  long long N;
+  int nzh;
+  int dev;
+  bool fused;
+  cudaStream_t st;
+  double* d_data;
+  double* d_res;
+  double* d_k;
+  double2* d_spec;
+  double2 *tw_x, *tw_y, *tw_z, *tw_zh;
+  psb::PlaneWork<double>* d_pw;   // [0] FIRST, [1] LAST
+  psb::PencilWork<double>* d_xw;  // [0]
+};
+
+namespace psb {
+
+static cudaError_t twiddles(double2** dst, int L) {
+  std::vector<double2> tw(L > 0 ? L : 1);
+  const double twopi = 2.0 * acos(-1.0);
+  for (int m = 0; m < L; ++m) {
+    const double a = twopi * (double)m / (double)L;
+    tw[m].x = cos(a);
+    tw[m].y = -sin(a);
+  }
+  cudaError_t e = cudaMalloc((void**)dst, sizeof(double2) * tw.size());
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice);
+}
+
+static void fft_free(ps_fft* f) {
+  auto fr = [](void* p) { if (p) cudaFree(p); };
+  fr(f->d_data); fr(f->d_res); fr(f->d_k); fr(f->d_spec);
+  fr(f->tw_x); fr(f->tw_y); fr(f->tw_z); fr(f->tw_zh); fr(f->d_pw); fr(f->d_xw);
+  if (f->st) cudaStreamDestroy(f->st);
+}
+
+}  // namespace psb
+
+using namespace psb;
+
+#define FFT_CUDA(call)                                                         \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      g_fft_err = std::string(#call) + ": " + cudaGetErrorString(e_);          \
+      return PS_GPU_ERR;                                                       \
+    }                                                                          \
+  } while (0)
+
+static int fft_create_impl(ps_fft* f, const int n[3], int device) {
+  for (int d = 0; d < 3; ++d) {
+    f->n[d] = n[d];
+    if (!extent_supported(n[d])) {
+      g_fft_err = "unsupported FFT extent " + std::to_string(n[d]);
+      return PS_INPUT_ERR;
+    }
+  }
+  f->N = (long long)n[0] * n[1] * n[2];
+  f->nzh = n[2] / 2 + 1;
+  f->dev = device;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    g_fft_err = "no CUDA device available";
+    return PS_GPU_ERR;
+  }
+  FFT_CUDA(cudaSetDevice(device));
+  FFT_CUDA(cudaStreamCreateWithFlags(&f->st, cudaStreamNonBlocking));
+  f->fused = plane_fused_supported(8, n[1], n[2]);
+  const size_t N = (size_t)f->N;
+  FFT_CUDA(cudaMalloc((void**)&f->d_data, sizeof(double) * N));
+  FFT_CUDA(cudaMalloc((void**)&f->d_res, sizeof(double) * N));
+  FFT_CUDA(cudaMalloc((void**)&f->d_k, sizeof(double) * N));
+  FFT_CUDA(cudaMalloc((void**)&f->d_spec, sizeof(double2) * (size_t)n[0] * n[1] * f->nzh));
+  FFT_CUDA(twiddles(&f->tw_x, n[0]));
+  FFT_CUDA(twiddles(&f->tw_y, n[1]));
+  FFT_CUDA(twiddles(&f->tw_z, n[2]));
+  FFT_CUDA(twiddles(&f->tw_zh, n[2] / 2 > 0 ? n[2] / 2 : 1));
+  PlaneWork<double> pw[2];
+  memset(pw, 0, sizeof(pw));
+  pw[0].mode = MODE_FIRST;
+  pw[0].src = f->d_data;
+  pw[0].spec = f->d_spec;
+  pw[1].mode = MODE_LAST;
+  pw[1].spec = f->d_spec;
+  pw[1].store = f->d_res;
+  PencilWork<double> xw;
+  memset(&xw, 0, sizeof(xw));
+  xw.spec = f->d_spec;
+  xw.kfull = f->d_k;
+  FFT_CUDA(cudaMalloc((void**)&f->d_pw, sizeof(pw)));
+  FFT_CUDA(cudaMemcpy(f->d_pw, pw, sizeof(pw), cudaMemcpyHostToDevice));
+  FFT_CUDA(cudaMalloc((void**)&f->d_xw, sizeof(xw)));
+  FFT_CUDA(cudaMemcpy(f->d_xw, &xw, sizeof(xw), cudaMemcpyHostToDevice));
+  return PS_OK;
+}
+
+extern "C" {
+
+int ps_fft_create(const int n[3], int precision, int device, ps_fft** out) {
+  if (!n || !out) {
+    g_fft_err = "null argument";
+    return PS_ATTRIB_ERR;
+  }
+  *out = nullptr;
+  if (precision != PS_PREC_FP64) {
+    g_fft_err = "the scaledFFTPair plugin computes in FP64 only";
+    return PS_ATTRIB_ERR;
+  }
+  ps_fft* f = new ps_fft;
+  memset(f, 0, sizeof(*f));
+  int rc = fft_create_impl(f, n, device);
+  if (rc != PS_OK) {
+    fft_free(f);
+    delete f;
+    return rc;
+  }
+  *out = f;
+  return PS_OK;
+}
+
+int ps_fft_destroy(ps_fft* f) {
+  if (!f) return PS_OK;
+  cudaSetDevice(f->dev);
+  if (f->st) cudaStreamSynchronize(f->st);
+  fft_free(f);
+  delete f;
+  return PS_OK;
+}
+
+int ps_fft_size(const ps_fft* f, size_t* n_total) {
+  if (!f || !n_total) return PS_ATTRIB_ERR;
+  *n_total = (size_t)f->N;
+  return PS_OK;
+}
+
+int ps_fft_scaled_pair(ps_fft* f, const double* data, const double* kdata, double* res) {
+  if (!f || !data || !kdata || !res) {
+    g_fft_err = "null argument";
+    return PS_ATTRIB_ERR;
+  }
+  const size_t N = (size_t)f->N;
+  const int nx = f->n[0], ny = f->n[1], nz = f->n[2];
+  FFT_CUDA(cudaSetDevice(f->dev));
+  FFT_CUDA(cudaMemcpyAsync(f->d_data, data, sizeof(double) * N, cudaMemcpyHostToDevice, f->st));
+  FFT_CUDA(cudaMemcpyAsync(f->d_k, kdata, sizeof(double) * N, cudaMemcpyHostToDevice, f->st));
+  if (f->fused) {
+    FFT_CUDA(launch_plane<double>(f->d_pw, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, f->st));
+    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, f->st));
+    FFT_CUDA(launch_plane<double>(f->d_pw + 1, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, f->st));
+  } else {
+    FFT_CUDA(launch_rows<double>(f->d_pw, 1, nx * ny, nz, f->tw_zh, f->tw_z, f->st));
+    if (ny > 1)
+      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_FWD, ny, nx, f->nzh, f->tw_y, nx, ny, nz, f->st));
+    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, f->st));
+    if (ny > 1)
+      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_INV, ny, nx, f->nzh, f->tw_y, nx, ny, nz, f->st));
+    FFT_CUDA(launch_rows<double>(f->d_pw + 1, 1, nx * ny, nz, f->tw_zh, f->tw_z, f->st));
+  }
+  FFT_CUDA(cudaMemcpyAsync(res, f->d_res, sizeof(double) * N, cudaMemcpyDeviceToHost, f->st));
+  FFT_CUDA(cudaStreamSynchronize(f->st));
+  return PS_OK;
+}
+
+const char* ps_fft_last_error(void) { return g_fft_err.c_str(); }
+
+}  // extern "C"

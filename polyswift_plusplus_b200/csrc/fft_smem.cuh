@@ -1,0 +1,180 @@
+// Shared-memory Stockham FFT building blocks (radix 2, 3, 4, 8) for sm_100a.
+//
+// A CTA transforms a batch of B pencils of length L that sit in shared memory,
+// element (b, i) at buf[b*bs + i*is].  Every pass keeps a single buffer: each
+// thread pulls all of its butterfly inputs into registers, the CTA
+// synchronises, then the butterflies are written back in Stockham order.  The
+// output is in natural order.  Twiddles come from a table tw[m] =
+// exp(-2 pi i m / L) computed on the host in FP64.
+#pragma once
+
+#include "common.cuh"
+
+namespace psb {
+
+// ---------------------------------------------------------------------------
+// In-register DFTs of radix R (natural-order output).
+// ---------------------------------------------------------------------------
+template <int R, bool INV, typename C> struct Dft;
+
+template <bool INV, typename C> struct Dft<1, INV, C> {
+  static __device__ __forceinline__ void run(C*) {}
+};
+
+template <bool INV, typename C> struct Dft<2, INV, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0];
+    v[0] = cadd(a, v[1]);
+    v[1] = csub(a, v[1]);
+  }
+};
+
+template <bool INV, typename C> struct Dft<3, INV, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    using S = decltype(v[0].x);
+    const S h = S(0.86602540378443864676);  // sqrt(3)/2
+    C s = cadd(v[1], v[2]);
+    C d = csub(v[1], v[2]);
+    C y0 = cadd(v[0], s);
+    C m = {v[0].x - S(0.5) * s.x, v[0].y - S(0.5) * s.y};
+    C t = mul_mi<INV>(d);
+    t = {h * t.x, h * t.y};
+    v[0] = y0;
+    v[1] = cadd(m, t);
+    v[2] = csub(m, t);
+  }
+};
+
+template <bool INV, typename C> struct Dft<4, INV, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    C s0 = cadd(v[0], v[2]);
+    C d0 = csub(v[0], v[2]);
+    C s1 = cadd(v[1], v[3]);
+    C d1 = mul_mi<INV>(csub(v[1], v[3]));
+    v[0] = cadd(s0, s1);
+    v[2] = csub(s0, s1);
+    v[1] = cadd(d0, d1);
+    v[3] = csub(d0, d1);
+  }
+};
+
+template <bool INV, typename C> struct Dft<8, INV, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    using S = decltype(v[0].x);
+    const S c = S(0.70710678118654752440);  // sqrt(2)/2
+    C a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      a[r] = cadd(v[r], v[r + 4]);
+      b[r] = csub(v[r], v[r + 4]);
+    }
+    // b[r] *= w8^r (conjugated for the inverse)
+    {
+      C x = b[1];
+      if (INV) b[1] = {c * (x.x - x.y), c * (x.x + x.y)};
+      else     b[1] = {c * (x.x + x.y), c * (x.y - x.x)};
+      b[2] = mul_mi<INV>(b[2]);
+      x = b[3];
+      if (INV) b[3] = {-c * (x.x + x.y), c * (x.x - x.y)};
+      else     b[3] = {c * (x.y - x.x), -c * (x.x + x.y)};
+    }
+    Dft<4, INV, C>::run(a);
+    Dft<4, INV, C>::run(b);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      v[2 * m] = a[m];
+      v[2 * m + 1] = b[m];
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Radix plans.
+// ---------------------------------------------------------------------------
+template <int... Rs> struct RadixList {};
+
+template <int L> struct Plan;  // RadixList of the passes, product = L
+template <> struct Plan<1> { using type = RadixList<>; };
+template <> struct Plan<2> { using type = RadixList<2>; };
+template <> struct Plan<3> { using type = RadixList<3>; };
+template <> struct Plan<4> { using type = RadixList<4>; };
+template <> struct Plan<6> { using type = RadixList<2, 3>; };
+template <> struct Plan<8> { using type = RadixList<8>; };
+template <> struct Plan<12> { using type = RadixList<4, 3>; };
+template <> struct Plan<16> { using type = RadixList<4, 4>; };
+template <> struct Plan<24> { using type = RadixList<8, 3>; };
+template <> struct Plan<32> { using type = RadixList<8, 4>; };
+template <> struct Plan<48> { using type = RadixList<4, 4, 3>; };
+template <> struct Plan<64> { using type = RadixList<8, 8>; };
+template <> struct Plan<96> { using type = RadixList<8, 4, 3>; };
+template <> struct Plan<128> { using type = RadixList<8, 4, 4>; };
+template <> struct Plan<192> { using type = RadixList<8, 8, 3>; };
+template <> struct Plan<256> { using type = RadixList<8, 8, 4>; };
+
+// One Stockham pass: radix R, NS = product of the radices already applied.
+// Thread t handles butterflies g = t + u*T.  BFAST selects the butterfly order:
+// batch-fastest (columns, is > 1) or index-fastest (rows, is == 1).
+template <int L, int R, int NS, int B, int T, bool INV, bool BFAST, typename C>
+__device__ __forceinline__ void stockham_pass(C* buf, int bs, int is, const C* tw) {
+  constexpr int M = L / R;       // butterflies per pencil
+  constexpr int NB = B * M;      // butterflies in the batch
+  constexpr int U = (NB + T - 1) / T;
+  constexpr int TS = L / (NS * R);
+  C v[U][R];
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int g = t + u * T;
+    if ((NB % T) == 0 || g < NB) {
+      const int b = BFAST ? (g % B) : (g / M);
+      const int j = BFAST ? (g / B) : (g % M);
+      const C* base = buf + b * bs;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[u][r] = base[(j + r * M) * is];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int g = t + u * T;
+    if ((NB % T) == 0 || g < NB) {
+      const int b = BFAST ? (g % B) : (g / M);
+      const int j = BFAST ? (g / B) : (g % M);
+      const int k = j % NS;
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C w = tw[r * k * TS];
+          v[u][r] = INV ? cmulc(v[u][r], w) : cmul(v[u][r], w);
+        }
+      }
+      Dft<R, INV, C>::run(v[u]);
+      C* base = buf + b * bs;
+      const int d = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[(d + r * NS) * is] = v[u][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int L, int NS, typename RL> struct Passes;
+template <int L, int NS> struct Passes<L, NS, RadixList<>> {
+  template <int B, int T, bool INV, bool BFAST, typename C>
+  static __device__ __forceinline__ void run(C*, int, int, const C*) {}
+};
+template <int L, int NS, int R, int... Rest> struct Passes<L, NS, RadixList<R, Rest...>> {
+  template <int B, int T, bool INV, bool BFAST, typename C>
+  static __device__ __forceinline__ void run(C* buf, int bs, int is, const C* tw) {
+    stockham_pass<L, R, NS, B, T, INV, BFAST>(buf, bs, is, tw);
+    Passes<L, NS * R, RadixList<Rest...>>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
+  }
+};
+
+// Batched FFT of B pencils of length L in shared memory.
+template <int L, int B, int T, bool INV, bool BFAST, typename C>
+__device__ __forceinline__ void smem_fft(C* buf, int bs, int is, const C* tw) {
+  Passes<L, 1, typename Plan<L>::type>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
+}
+
+}  // namespace psb

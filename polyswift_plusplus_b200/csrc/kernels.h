@@ -1,0 +1,55 @@
+// Host-side launch interface of the sm_100a SCFT kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "common.cuh"
+
+namespace psb {
+
+// One propagator step of one sweep, real-space side (see prop_kernels.cu).
+enum { MODE_FIRST = 0, MODE_MID = 1, MODE_LAST = 2 };
+
+template <typename T> struct PlaneWork {
+  const T* src;       // MODE_FIRST: initial q (nullptr = ones)
+  c2_t<T>* spec;      // half spectrum [nx][ny][nz/2+1]
+  const T* wfac_in;   // wfac of the step being finished (nullptr = 1)
+  const T* wfac_out;  // wfac of the step being started (nullptr = 1)
+  T* store;           // slice receiving q (FIRST: the initial q; MID/LAST: q(s+ds))
+  int mode;
+  int pad;
+};
+
+// Pencil pass along a strided axis of the half spectrum.
+enum { PENCIL_FWD = 0, PENCIL_INV = 1, PENCIL_KINV = 2, PENCIL_KFULL = 3 };
+
+template <typename T> struct PencilWork {
+  c2_t<T>* spec;
+  const T* kx;        // PENCIL_KINV: factor along the pencil axis (1/N folded in)
+  const T* kyz;       // PENCIL_KINV: factor per (y, kz) column
+  const double* kfull;// PENCIL_KFULL: full real k array [nx][ny][nz] (plugin path)
+};
+
+bool extent_supported(int n);
+// The fused y-z plane kernel exists for this plane and fits in shared memory.
+bool plane_fused_supported(int prec_bytes, int ny, int nz);
+
+// Twiddle tables: tw_L[m] = exp(-2 pi i m / L); tw_zh has length nz/2, tw_z length nz.
+template <typename T>
+cudaError_t launch_plane(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,
+                         const c2_t<T>* tw_y, const c2_t<T>* tw_zh, const c2_t<T>* tw_z,
+                         cudaStream_t st);
+
+// Row (z only) pass over nrows = nx*ny flattened rows.
+template <typename T>
+cudaError_t launch_rows(const PlaneWork<T>* d_works, int nworks, int nrows, int nz,
+                        const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st);
+
+// Pencils of length L along an axis of stride `inner` (elements), `outer`
+// independent groups of L*inner elements; dims used only by PENCIL_KFULL.
+template <typename T>
+cudaError_t launch_pencil(const PencilWork<T>* d_works, int nworks, int mode, int L, int outer,
+                          int inner, const c2_t<T>* tw, int nx, int ny, int nz, cudaStream_t st);
+
+}  // namespace psb

@@ -1,0 +1,190 @@
+"""Python mirror of the reference's domain / plugin interfaces over the C-ABI.
+
+``ScftSolver`` follows the PsDomain build cycle (pstrol/PsDomain.cpp:64-372):
+construction = setAttrib + buildData + buildSolvers (``ps_gpu_create``), then
+``initialize()`` (the reference's "random" monomerDens initialisation) or
+``restore(w, p)`` (dump/restart of (dens, conj) fields), then ``update(t)``
+iterations, and scalars equal to what the reference's free-energy history and
+``getLogBigQ`` report.  ``B200FFT`` is the ``PsFFTBase::scaledFFTPair`` plugin.
+All computation runs on the GPU through the native library; nothing here falls
+back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+from .config import ScftConfig
+
+
+class ScftSolver:
+    def __init__(self, cfg: ScftConfig):
+        self.cfg = cfg
+        self._lib = A.load_library()
+        self._pc = cfg.to_ps_config()
+        h = C.c_void_p()
+        A.check(self._lib.ps_gpu_create(C.byref(self._pc), C.byref(h)), None)
+        self._h = h
+        self.N = cfg.n_total
+        self.nf = len(cfg.fields)
+        self.t = 0
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ps_gpu_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        A.check(rc, self._h)
+
+    # -- build cycle ------------------------------------------------------
+    def block_steps(self, polymer: int, block: int) -> int:
+        v = C.c_int()
+        self._check(self._lib.ps_gpu_block_steps(self._h, polymer, block, C.byref(v)))
+        return v.value
+
+    def initialize(self) -> None:
+        """PsMonomerDens::initialize "random": w_i = U[0,1) - 0.5, p = 0."""
+        self._check(self._lib.ps_gpu_init_random(self._h))
+
+    def restore(self, w, p=None) -> None:
+        """Set the conjugate fields (nf x N, or a list) and optionally the pressure."""
+        w = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in w]
+        if len(w) != self.nf:
+            raise ValueError(f"expected {self.nf} fields")
+        for i, x in enumerate(w):
+            self.set_field(A.PS_FIELD_W, i, x)
+        if p is not None:
+            self.set_field(A.PS_FIELD_PRES, 0, p)
+        else:
+            self.set_field(A.PS_FIELD_PRES, 0, np.zeros(self.N))
+
+    def set_field(self, which: int, index: int, data) -> None:
+        if hasattr(data, "data_ptr"):  # torch tensor: on the handle's device, or (pinned) host
+            t = data
+            if t.dtype != __import__("torch").float64 or not t.is_contiguous():
+                raise ValueError("tensors must be contiguous float64")
+            if t.numel() != self.N:
+                raise ValueError("wrong field size")
+            self._check(self._lib.ps_gpu_set_fields(self._h, which, index, C.c_void_p(t.data_ptr()),
+                                                    1 if t.is_cuda else 0))
+            return
+        x = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+        if x.size != self.N:
+            raise ValueError("wrong field size")
+        self._check(self._lib.ps_gpu_set_fields(self._h, which, index, x.ctypes.data_as(C.c_void_p), 0))
+
+    def get_field(self, which: int, index: int = 0, out=None):
+        if out is not None and hasattr(out, "data_ptr"):
+            self._check(self._lib.ps_gpu_get_fields(self._h, which, index, C.c_void_p(out.data_ptr()), 1))
+            return out
+        x = np.empty(self.N, dtype=np.float64) if out is None else out
+        self._check(self._lib.ps_gpu_get_fields(self._h, which, index, x.ctypes.data_as(C.c_void_p), 0))
+        return x
+
+    def w(self, i: int) -> np.ndarray:
+        return self.get_field(A.PS_FIELD_W, i)
+
+    def phi(self, i: int) -> np.ndarray:
+        return self.get_field(A.PS_FIELD_PHI, i)
+
+    def pressure(self) -> np.ndarray:
+        return self.get_field(A.PS_FIELD_PRES, 0)
+
+    # -- iterations -------------------------------------------------------
+    def update(self, n: int = 1) -> None:
+        """Run n SCFT iterations (PsDomain::update order)."""
+        self._check(self._lib.ps_gpu_iterate(self._h, int(n)))
+        self.t += n
+
+    def scalars(self) -> dict:
+        s = A.ps_scalars()
+        self._check(self._lib.ps_gpu_get_scalars(self._h, C.byref(s)))
+        return s.as_dict(len(self.cfg.polymers))
+
+    def propagator(self, polymer: int, block: int, end: int, n: int) -> np.ndarray:
+        x = np.empty(self.N, dtype=np.float64)
+        self._check(self._lib.ps_gpu_get_propagator(self._h, polymer, block, end, n,
+                                                    x.ctypes.data_as(C.c_void_p)))
+        return x
+
+    def synchronize(self) -> None:
+        self._check(self._lib.ps_gpu_synchronize(self._h))
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(self._lib.ps_gpu_launches_per_iteration(self._h))
+
+    @property
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t (e.g. for torch.cuda.ExternalStream)."""
+        return int(self._lib.ps_gpu_stream(self._h) or 0)
+
+    def enable_sweep_timing(self, max_samples: int) -> None:
+        self._check(self._lib.ps_gpu_enable_sweep_timing(self._h, int(max_samples)))
+
+    def sweep_timing(self, max_out: int = 4096):
+        """(per-iteration sweep durations in ms, algorithmic bytes per iteration's
+        sweeps, propagator steps per iteration); clears the samples."""
+        buf = (C.c_double * max_out)()
+        n = C.c_int()
+        b = C.c_double()
+        s = C.c_longlong()
+        self._check(self._lib.ps_gpu_sweep_timing(self._h, buf, max_out, C.byref(n), C.byref(b),
+                                                  C.byref(s)))
+        return [buf[i] for i in range(min(n.value, max_out))], b.value, s.value
+
+
+class B200FFT:
+    """PsFFTBase<double,3>::scaledFFTPair plugin (host arrays in and out)."""
+
+    def __init__(self, n, device: int = 0):
+        self._lib = A.load_library()
+        arr = (C.c_int * 3)(*[int(v) for v in n])
+        h = C.c_void_p()
+        A.check(self._lib.ps_fft_create(arr, A.PS_PREC_FP64, device, C.byref(h)), fft=True)
+        self._h = h
+        self.n = tuple(int(v) for v in n)
+        self.N = self.n[0] * self.n[1] * self.n[2]
+
+    def getFFTSize(self) -> int:
+        v = C.c_size_t()
+        A.check(self._lib.ps_fft_size(self._h, C.byref(v)), fft=True)
+        return int(v.value)
+
+    def scaledFFTPair(self, data, kdata) -> np.ndarray:
+        d = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+        k = np.ascontiguousarray(kdata, dtype=np.float64).reshape(-1)
+        if d.size != self.N or k.size != self.N:
+            raise ValueError("data/kdata size must equal getFFTSize()")
+        res = np.empty(self.N, dtype=np.float64)
+        A.check(self._lib.ps_fft_scaled_pair(self._h, d.ctypes.data_as(C.c_void_p),
+                                             k.ctypes.data_as(C.c_void_p),
+                                             res.ctypes.data_as(C.c_void_p)), fft=True)
+        return res
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ps_fft_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

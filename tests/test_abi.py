@@ -1,0 +1,139 @@
+"""The C-ABI library loads and exports every entry point include/pswift.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from polyswift_plusplus_b200 import _abi as A
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(ps_\w+)\s*\(", text, flags=re.M):
+            names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("ps_gpu_create", "ps_gpu_iterate", "ps_gpu_get_scalars", "ps_fft_scaled_pair"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(native_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(A.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, f"declared but not exported: {missing}"
+    for n in declared_functions():
+        assert hasattr(native_lib, n)
+        assert n in A.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_version_string(native_lib):
+    assert b"sm_100a" in native_lib.ps_version()
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """Every ctypes field offset and struct size equals gcc's offsetof/sizeof."""
+    structs = [A.ps_block_config, A.ps_polymer_config, A.ps_interaction_config,
+               A.ps_updater_config, A.ps_config, A.ps_scalars]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pswift.h"', 'int main(void){']
+    for s in structs:
+        n = s.__name__
+        lines.append(f'printf("{n} size %zu\\n", sizeof({n}));')
+        for f in s._fields_:
+            lines.append(f'printf("{n} {f[0]} %zu\\n", offsetof({n}, {f[0]}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        a, b, c = line.split()
+        got[(a, b)] = int(c)
+    for s in structs:
+        n = s.__name__
+        assert got[(n, "size")] == C.sizeof(s), n
+        for f in s._fields_:
+            assert got[(n, f[0])] == getattr(s, f[0]).offset, (n, f[0])
+
+
+def test_config_parser_reads_reference_style_input():
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+$ NX = 16
+$ DX = 0.25
+nsteps = 20
+randomSeed = 38383
+setupPS(NX, NX, NX, DX, DX, DX, "'off'")
+<EffHamil mainHamil>
+  kind = canonicalMF
+  updaterSequence = [wAwB]
+  <Updater wAwB>
+    kind = steepestDescent
+    relaxlambdas = [0.40 0.20]
+    noise = 0.0
+    updatefields = [totA totB]
+    interactions = [AB]
+  </Updater>
+  <Interaction AB>
+    kind = flory
+    chi = 0.12
+    scfields = [totA totB]
+  </Interaction>
+</EffHamil>
+<PhysField totA>
+  kind = monomerDens
+  type = fieldD3R
+</PhysField>
+<PhysField totB>
+  kind = monomerDens
+  type = fieldD3R
+</PhysField>
+<PhysField defaultPressure>
+  kind = constraint
+  type = fieldD3R
+</PhysField>
+<Polymer diblock1>
+  kind = blockCopolymer
+  volfrac = 1.0
+  length = 100
+  <Block blockA>
+    kind = flexPseudoSpec
+    scfield = totA
+    ds = 0.05
+    lengthfrac = 0.5
+    headjoined = [freeEnd]
+    tailjoined = [blockB]
+  </Block>
+  <Block blockB>
+    kind = flexPseudoSpec
+    scfield = totB
+    ds = 0.05
+    lengthfrac = 0.5
+    headjoined = [blockA]
+    tailjoined = [freeEnd]
+  </Block>
+</Polymer>
+<History freeE1>
+  kind = freeEnergy
+  updaterName = wAwB
+</History>
+"""
+    cfg = config_from_text(text)
+    assert cfg.n == (16, 16, 16) and cfg.cell == (0.25, 0.25, 0.25)
+    assert cfg.fields == ["totA", "totB"] and cfg.seed == 38383 and cfg.nsteps == 20
+    assert cfg.updater.relaxlambdas == (0.40, 0.20)
+    pc = cfg.to_ps_config()
+    assert pc.polymers[0].blocks[1].n_head == 1 and pc.polymers[0].blocks[1].head_joined[0] == 0
+    assert pc.interactions[0].chi == pytest.approx(0.12)

@@ -1,0 +1,244 @@
+"""GPU parity: the sm_100a path through the C-ABI against the FP64 oracle.
+
+Tolerances: FP64 device path 1e-10 relative (fields: 1e-10 of the field's max
+magnitude); mixed path |dF/F| < 1e-6.
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from polyswift_plusplus_b200 import _abi as A
+from polyswift_plusplus_b200 import workloads as W
+from polyswift_plusplus_b200.config import Block, Interaction, Polymer, ScftConfig, Updater
+from polyswift_plusplus_b200.scft import B200FFT, ScftSolver
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL64 = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def run_both(cfg, w, iters, p=None):
+    g = ScftSolver(cfg)
+    g.restore(w, p)
+    o = O.Oracle(cfg)
+    o.restore(w, p)
+    hist_o = o.update(iters)
+    hist_g = []
+    for _ in range(iters):
+        g.update(1)
+        hist_g.append(g.scalars())
+    return g, o, hist_g, hist_o
+
+
+def assert_parity(cfg, g, o, hist_g, hist_o, tol=TOL64):
+    for hg, ho in zip(hist_g, hist_o):
+        assert abs(hg["free_energy"] - ho["free_energy"]) <= tol * max(abs(ho["free_energy"]), 1e-2)
+        for ip in range(len(cfg.polymers)):
+            assert hg["q"][ip] == pytest.approx(ho["q"][ip], rel=tol)
+        assert abs(hg["max_incomp"] - ho["max_incomp"]) <= tol * max(ho["max_incomp"], 1e-3)
+    for i in range(len(cfg.fields)):
+        assert rel(g.w(i), o.w(i)) < tol
+        assert rel(g.phi(i), o.phi(i)) < tol
+    assert rel(g.pressure(), o.pressure()) < tol * 10
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (12, 12, 12), (32, 32, 32),
+                                   (24, 48, 48), (16, 64, 1), (8, 4, 256), (4, 16, 32),
+                                   (64, 64, 64)])
+def test_fft_plugin_matches_oracle(gpu, oracle_lib, shape):
+    rng = np.random.default_rng(3)
+    d = rng.standard_normal(shape)
+    k = rng.standard_normal(shape)  # non-symmetric kdata: exercises the c2c real-part semantics
+    f = B200FFT(shape)
+    assert f.getFFTSize() == d.size
+    got = f.scaledFFTPair(d, k).reshape(shape)
+    ref = O.scaled_fft_pair(d, k)
+    assert rel(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_fp64_diblock_parity(gpu, oracle_lib, n):
+    cfg, w = W.diblock32(n=n)
+    g, o, hg, ho = run_both(cfg, w, 12 if n == 32 else 25)
+    assert_parity(cfg, g, o, hg, ho)
+    assert g.launches_per_iteration > 0
+
+
+def test_fp64_propagator_slices(gpu, oracle_lib):
+    cfg, w = W.diblock32(n=16)
+    g, o, _, _ = run_both(cfg, w, 2)
+    for ib, steps in ((0, 30), (1, 70)):
+        for end in (A.PS_FROM_HEAD, A.PS_FROM_TAIL):
+            for n in (0, 1, steps // 2, steps):
+                assert rel(g.propagator(0, ib, end, n), o.propagator(0, ib, end, n)) < TOL64
+
+
+@pytest.mark.parametrize("name", ["diblock8", "triblock8", "blend8"])
+def test_gpu_matches_golden(gpu, name):
+    import sys
+    sys.path.insert(0, str(GOLD))
+    from make_golden import small_configs
+    cfg, _ = small_configs()[name]
+    gd = np.load(GOLD / f"scft_{name}.npz")
+    g = ScftSolver(cfg)
+    g.restore(list(gd["w0"]))
+    fe = []
+    for _ in range(len(gd["free_energy"])):
+        g.update(1)
+        fe.append(g.scalars()["free_energy"])
+    assert np.allclose(fe, gd["free_energy"], rtol=TOL64, atol=1e-12)
+    for i in range(len(cfg.fields)):
+        assert rel(g.w(i), gd["w"][i]) < TOL64
+        assert rel(g.phi(i), gd["phi"][i]) < TOL64
+
+
+def test_fp64_triblock_three_fields(gpu, oracle_lib):
+    ds = 0.02
+    tri = Polymer("abc", 1.0, 100, [Block("a", "A", ds, 0.3, ["freeEnd"], ["b"]),
+                                    Block("b", "B", ds, 0.4, ["a"], ["c"]),
+                                    Block("c", "C", ds, 0.3, ["b"], ["freeEnd"])])
+    cfg = ScftConfig(n=(16, 16, 16), cell=(0.25,) * 3, fields=["A", "B", "C"], polymers=[tri],
+                     interactions=[Interaction("AB", 0.3, ["A", "B"]),
+                                   Interaction("BC", 0.3, ["B", "C"]),
+                                   Interaction("AC", 0.45, ["A", "C"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)), seed=91)
+    w = W.random_fields(cfg, 0.3)
+    g, o, hg, ho = run_both(cfg, w, 10)
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_fp64_blend_with_homopolymer(gpu, oracle_lib):
+    cfg = W.blend(16, 18.0, 0.35, 0.15, precision="fp64", seed=12, anderson=False)
+    w = W.random_fields(cfg, 0.3)
+    g, o, hg, ho = run_both(cfg, w, 10)
+    assert_parity(cfg, g, o, hg, ho)
+    # homopolymer: forward and backward propagators coincide
+    assert rel(g.propagator(1, 0, A.PS_FROM_HEAD, 17), o.propagator(1, 0, A.PS_FROM_TAIL, 17)) < TOL64
+
+
+def test_fp64_anderson_parity(gpu, oracle_lib):
+    cfg, w = W.diblock32(n=16)
+    cfg.updater = Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=5,
+                          anderson_mix=0.1, anderson_start=4)
+    g, o, hg, ho = run_both(cfg, w, 20)
+    assert_parity(cfg, g, o, hg, ho, tol=1e-9)
+
+
+def test_fp64_split_plane_path(gpu, oracle_lib):
+    """(ny, nz) planes without a fused kernel run as row + y-pencil passes."""
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = (8, 4, 256)
+    cfg.cell = (0.5, 0.5, 0.03125)
+    w = W.random_fields(cfg, 0.5)
+    g, o, hg, ho = run_both(cfg, w, 4)
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_fp64_two_dimensional_grid(gpu, oracle_lib):
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = (64, 64, 1)
+    cfg.cell = (0.1, 0.1, 0.1)
+    w = W.random_fields(cfg, 0.5)
+    g, o, hg, ho = run_both(cfg, w, 6)
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_reference_random_init_and_noise(gpu, oracle_lib):
+    cfg, _ = W.diblock32(n=16)
+    cfg.updater.noise = 0.002
+    g = ScftSolver(cfg)
+    g.initialize()
+    o = O.Oracle(cfg)
+    o.initialize()
+    for i in range(2):
+        assert np.array_equal(g.w(i), o.w(i))
+    ho = o.update(3)
+    g.update(3)
+    hg = g.scalars()
+    assert hg["free_energy"] == pytest.approx(ho[-1]["free_energy"], rel=TOL64)
+    for i in range(2):
+        assert rel(g.w(i), o.w(i)) < TOL64
+
+
+def test_mixed_precision_close_to_fp64(gpu, oracle_lib):
+    cfg, w = W.diblock32(n=32, precision="mixed")
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(20)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(20)
+    s = g.scalars()
+    assert abs(s["free_energy"] - ho[-1]["free_energy"]) / abs(ho[-1]["free_energy"]) < 1e-6
+    assert max(rel(g.phi(i), o.phi(i)) for i in range(2)) < 1e-5
+
+
+def test_kat_uniform_field_gpu(gpu):
+    cfg, _ = W.diblock32(n=16)
+    g = ScftSolver(cfg)
+    c = 0.7
+    g.restore([np.full(cfg.n_total, c)] * 2)
+    g.update(1)
+    s = g.scalars()
+    assert s["q"][0] == pytest.approx(math.exp(-c), rel=1e-13)
+    for n in (0, 10, 30):
+        assert np.allclose(g.propagator(0, 0, A.PS_FROM_HEAD, n), math.exp(-c * 0.01 * n), rtol=1e-13)
+    g2 = ScftSolver(cfg)
+    g2.restore([np.zeros(cfg.n_total)] * 2)
+    g2.update(1)
+    assert np.allclose(g2.phi(0), 0.33333 * 0.01 * 90, rtol=1e-13)
+
+
+def test_kat_q_independent_of_s_gpu(gpu):
+    cfg, w = W.diblock32(n=16)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(1)
+    Q = g.scalars()["q"][0]
+    for ib, steps in ((0, 30), (1, 70)):
+        for n in (0, 9, steps):
+            qs = g.propagator(0, ib, A.PS_FROM_HEAD, n)
+            qt = g.propagator(0, ib, A.PS_FROM_TAIL, steps - n)
+            assert np.mean(qs * qt) == pytest.approx(Q, rel=1e-12)
+
+
+def test_graph_replay_is_deterministic(gpu):
+    cfg, w = W.diblock32(n=16)
+    a, b = ScftSolver(cfg), ScftSolver(cfg)
+    a.restore(w)
+    b.restore(w)
+    a.update(6)
+    for _ in range(6):
+        b.update(1)
+    assert a.scalars()["free_energy"] == b.scalars()["free_energy"]
+    assert np.array_equal(a.w(0), b.w(0))
+
+
+def test_errors_are_status_codes(gpu):
+    cfg, w = W.diblock32(n=8)
+    g = ScftSolver(cfg)
+    bad = w[0].copy()
+    bad[5] = np.nan
+    g.restore([bad, w[1]])
+    with pytest.raises(A.PsError) as e:
+        g.update(1)
+    assert e.value.code == A.PS_RUN_ERR
+    cfg2, _ = W.diblock32(n=8)
+    cfg2.n = (10, 10, 10)
+    with pytest.raises(A.PsError) as e:
+        ScftSolver(cfg2)
+    assert e.value.code == A.PS_INPUT_ERR
+    cfg3, _ = W.diblock32(n=8)
+    cfg3.polymers[0].blocks[0].ds = 0.013
+    cfg3.polymers[0].blocks[1].ds = 0.013
+    with pytest.raises(A.PsError) as e:
+        ScftSolver(cfg3)
+    assert e.value.code == A.PS_INPUT_ERR

@@ -1,0 +1,169 @@
+"""CPU tests of the oracle: pinned against numpy, golden fixtures and known answers."""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle.np_scft import NpScft, block_steps
+from polyswift_plusplus_b200 import _abi as A
+from polyswift_plusplus_b200 import workloads as W
+from polyswift_plusplus_b200.config import Block, Interaction, Polymer, ScftConfig, Updater
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def test_mt19937_matches_numpy_and_golden(oracle_lib):
+    d = np.load(GOLD / "mt19937_seed38383.npz")
+    assert np.array_equal(O.mt_u32(38383, 1000), d["u32"])
+    assert np.array_equal(O.mt_reals(38383, 2000), d["reals"])
+    assert np.array_equal(O.mt_gauss(38383, 1000), d["gauss"])
+    # the published MT19937 known answer for init_genrand(5489)
+    assert O.mt_u32(5489, 3).tolist() == [3499211612, 581869302, 3890346734]
+    # the product's seeded-field generator draws the same stream
+    assert np.array_equal(W.mt_reals(38383, 2000), d["reals"])
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (12, 16, 4), (24, 48, 32), (5, 7, 3), (64, 64, 1)])
+def test_fft_matches_numpy(oracle_lib, shape):
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ref = np.fft.fftn(x)
+    scale = np.abs(ref).max()
+    assert np.abs(O.fft3d(x, -1) - ref).max() / scale < 1e-13
+    assert np.abs(O.fft3d(x, +1) - np.fft.ifftn(x) * x.size).max() / scale < 1e-13
+
+
+def test_scaled_fft_pair_matches_numpy(oracle_lib):
+    rng = np.random.default_rng(2)
+    d = rng.standard_normal((8, 12, 16))
+    k = rng.standard_normal((8, 12, 16))  # arbitrary, non-symmetric kdata
+    ref = np.fft.ifftn(np.fft.fftn(d) * k).real * d.size
+    got = O.scaled_fft_pair(d, k)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("name", ["diblock8", "triblock8", "blend8"])
+def test_oracle_matches_golden(oracle_lib, name):
+    import sys
+    sys.path.insert(0, str(GOLD))
+    from make_golden import small_configs
+    cfg, _ = small_configs()[name]
+    g = np.load(GOLD / f"scft_{name}.npz")
+    o = O.Oracle(cfg)
+    o.restore(list(g["w0"]))
+    hist = o.update(len(g["free_energy"]))
+    fe = np.array([h["free_energy"] for h in hist])
+    assert np.allclose(fe, g["free_energy"], rtol=1e-12, atol=1e-13)
+    q = np.array([h["q"] for h in hist])
+    assert np.allclose(q, g["q"], rtol=1e-12)
+    for i in range(len(cfg.fields)):
+        assert np.allclose(o.w(i), g["w"][i], rtol=1e-12, atol=1e-12)
+        assert np.allclose(o.phi(i), g["phi"][i], rtol=1e-12, atol=1e-12)
+    assert np.allclose(o.pressure(), g["p"], rtol=1e-12, atol=1e-12)
+
+
+def test_oracle_matches_numpy_restatement_16(oracle_lib):
+    cfg, w = W.diblock32(n=16)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    n = NpScft(cfg)
+    n.restore(w)
+    hist = o.update(6)
+    for h in hist:
+        r = n.iterate()
+        assert abs(h["free_energy"] - r["free_energy"]) < 1e-12
+        assert abs(h["q"][0] - r["q"][0]) < 1e-12 * r["q"][0]
+
+
+def test_kat1_zero_field(oracle_lib):
+    """w = 0: q = 1 everywhere, Q = 1, phi_A = f * 0.99999 (the 0.33333 Simpson factor)."""
+    cfg, _ = W.diblock32(n=8)
+    o = O.Oracle(cfg)
+    o.restore([np.zeros(cfg.n_total)] * 2)
+    h = o.update(1)[0]
+    assert h["q"][0] == pytest.approx(1.0, abs=1e-14)
+    # A has 30 steps (31 points, pure Simpson): 0.33333*ds*90 = 0.299997
+    assert np.allclose(o.phi(0), 0.33333 * 0.01 * 90, rtol=1e-13)
+    # B has 70 steps
+    assert np.allclose(o.phi(1), 0.33333 * 0.01 * 210, rtol=1e-13)
+
+
+def test_kat2_uniform_field(oracle_lib):
+    """w_A = w_B = c: q(s) = exp(-c s) exactly, Q = exp(-c)."""
+    cfg, _ = W.diblock32(n=8)
+    c = 0.7
+    o = O.Oracle(cfg)
+    o.restore([np.full(cfg.n_total, c)] * 2)
+    h = o.update(1)[0]
+    assert h["q"][0] == pytest.approx(math.exp(-c), rel=1e-13)
+    for n in (0, 7, 30):
+        q = o.propagator(0, 0, A.PS_FROM_HEAD, n)
+        assert np.allclose(q, math.exp(-c * 0.01 * n), rtol=1e-13)
+
+
+def test_kat3_single_mode_decay(oracle_lib):
+    """w = 0, q0 = cos(k x): each step multiplies the mode by exp(-ds k^2)."""
+    cfg, _ = W.diblock32(n=16)
+    L = cfg.box[0]
+    x = (np.arange(16) * cfg.cell[0])[:, None, None] * np.ones((16, 16, 16))
+    k = 2 * math.pi * 3 / L
+    q0 = np.cos(k * x).reshape(-1)
+    res = O.scaled_fft_pair(q0.reshape(16, 16, 16), np.exp(-0.01 * k * k) * np.ones((16, 16, 16)))
+    # a uniform kdata multiplies every mode equally; the full k2 operator decays cos(kx)
+    o = O.Oracle(cfg)
+    k2 = o.k2(0, 0).reshape(16, 16, 16)
+    step = O.scaled_fft_pair(q0.reshape(16, 16, 16), k2).reshape(-1) / cfg.n_total
+    assert np.allclose(step, math.exp(-0.01 * k * k) * q0, atol=1e-14)
+    assert np.allclose(res.reshape(-1) / cfg.n_total, math.exp(-0.01 * k * k) * q0, atol=1e-14)
+
+
+def test_kat4_q_independent_of_s(oracle_lib):
+    """<q(r,s) q+(r,s)> is the same at every contour point."""
+    cfg, w = W.diblock32(n=8)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    h = o.update(1)[0]
+    Q = h["q"][0]
+    for ib, steps in ((0, 30), (1, 70)):
+        for n in (0, 5, steps):
+            qs = o.propagator(0, ib, A.PS_FROM_HEAD, n)
+            qt = o.propagator(0, ib, A.PS_FROM_TAIL, steps - n)
+            assert np.mean(qs * qt) == pytest.approx(Q, rel=1e-12)
+
+
+def test_block_steps_rounding():
+    """psbase/PsBlockBase.cpp:252-326 (and the device path agrees)."""
+    assert block_steps(70.00000001, False) == 70
+    assert block_steps(69.99999, False) == 70
+    with pytest.raises(ValueError):
+        block_steps(51.2, False)
+    assert block_steps(51.2, True) == 51
+    assert block_steps(76.8, True) == 77
+    with pytest.raises(ValueError):
+        block_steps(3.0, False)
+
+
+def test_oracle_rejects_bad_input(oracle_lib):
+    cfg, _ = W.diblock32(n=8)
+    cfg.polymers[0].blocks[0].lengthfrac = 0.305  # non-integer steps and sum f != 1
+    with pytest.raises(A.PsError) as e:
+        O.Oracle(cfg)
+    assert e.value.code == A.PS_INPUT_ERR
+
+
+def test_anderson_oracle_converges_faster(oracle_lib):
+    cfg, w = W.diblock32(n=16)
+    o_sd = O.Oracle(cfg)
+    o_sd.restore(w)
+    h_sd = o_sd.update(40)
+    cfg.updater = Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=5,
+                          anderson_mix=0.1, anderson_start=5)
+    o_am = O.Oracle(cfg)
+    o_am.restore(w)
+    h_am = o_am.update(40)
+    # the first anderson_start steps are plain steepest descent: identical
+    for a, b in zip(h_sd[:5], h_am[:5]):
+        assert a["free_energy"] == b["free_energy"]
+    assert h_am[-1]["dh_norm"] < h_sd[-1]["dh_norm"]
