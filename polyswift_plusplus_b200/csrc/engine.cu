@@ -402,10 +402,14 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
     PS_CUDA(h, launch_wfac<T>(h->d_w + (size_t)f * N, B.wfac[i], -0.5 * ds, N, h->st));
     ++*nlaunch;
   }
-  if (h->timing_cap > 0) PS_CUDA(h, cudaEventRecord(h->ev_cap_start, h->st));
+  // cudaEventRecordExternal: inside stream capture this becomes an event-record
+  // node of the graph (a plain record would only order the capture).
+  if (h->timing_cap > 0)
+    PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_start, h->st, cudaEventRecordExternal));
   int rc = launch_sweeps<T>(h, nlaunch);
   if (rc) return rc;
-  if (h->timing_cap > 0) PS_CUDA(h, cudaEventRecord(h->ev_cap_end, h->st));
+  if (h->timing_cap > 0)
+    PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_end, h->st, cudaEventRecordExternal));
   auto slice = [&](int sweep, int idx) -> const T* {
     return B.slices[h->sweeps[sweep].storage] + (size_t)idx * N;
   };

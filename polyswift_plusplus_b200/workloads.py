@@ -8,7 +8,9 @@ point in row-major order, plus the deterministic seeds described per workload.
 
 * ``diblock32``   32^3, box 4.0 Rg, f_A 0.30, chiN 20, Ns 100, steepest descent
                   lambda = (0.1, 0.05); w = U(-0.1, 0.1) +/- cos(2 pi x / L).
-* ``diblock128``  128^3, box 8.0 Rg, f_A 0.35, chiN 25, Ns 200, Anderson depth 10;
+* ``diblock128``  128^3, box 8.0 Rg, f_A 0.35, chiN 25, Ns 200, Anderson depth 10
+                  (mixing 0.5 after 100 steepest-descent steps, which let the melt order
+                  first; started earlier the history pulls it to the disordered saddle);
                   w = U(-0.05, 0.05) +/- hexagonal seed (three cosines with integer
                   wave vectors (2,0), (-1,2), (-1,-2) x 2 pi / L in the x-y plane:
                   the periodic box's nearest match to 120 degrees).
@@ -87,7 +89,7 @@ def hex_seed(cfg: ScftConfig) -> np.ndarray:
 
 def diblock128(precision="mixed", n=128, anderson=True) -> tuple[ScftConfig, list[np.ndarray]]:
     upd = (Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=10,
-                   anderson_mix=0.1, anderson_start=10) if anderson
+                   anderson_mix=0.5, anderson_start=100) if anderson
            else Updater(kind="steepestDescent", relaxlambdas=(0.1, 0.05)))
     cfg = diblock_config(n, 8.0 * n / 128, 0.35, 25.0, 200, upd, precision)
     s = hex_seed(cfg)
@@ -119,7 +121,7 @@ def triblock256(precision="mixed", n=256) -> tuple[ScftConfig, list[np.ndarray]]
                                    Interaction("BC", 30.0 / length, ["B", "C"]),
                                    Interaction("AC", 45.0 / length, ["A", "C"])],
                      updater=Updater(kind="andersonMixing", relaxlambdas=(0.05, 0.025),
-                                     anderson_depth=20, anderson_mix=0.05, anderson_start=20),
+                                     anderson_depth=20, anderson_mix=0.5, anderson_start=200),
                      seed=38383, precision=precision)
     return cfg, random_fields(cfg, 0.05)
 
@@ -134,7 +136,7 @@ def blend(n: int, chin: float, f_a: float, phi_h: float, precision="mixed", seed
         polymers.append(Polymer(name="homoA", volfrac=phi_h, length=length // 2, blocks=[
             Block("homoA_A", "A", ds, 1.0, ["freeEnd"], ["freeEnd"])]))
     upd = (Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=10,
-                   anderson_mix=0.1, anderson_start=10) if anderson
+                   anderson_mix=0.5, anderson_start=100) if anderson
            else Updater(kind="steepestDescent", relaxlambdas=(0.1, 0.05)))
     box = 4.0 * n / 32
     return ScftConfig(n=(n, n, n), cell=(box / n,) * 3, fields=["A", "B"], polymers=polymers,
