@@ -335,6 +335,7 @@ static int build_device_tables(ps_handle* h) {
       w.wfac_in = (k > 0) ? B.wfac[seg_of(sw, k - 1).wfac_id] : nullptr;
       w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
       w.store = B.slices[e] + (size_t)k * N;
+      w.status = &h->d_sc->error_flags;
       pw.push_back(w);
       if (k < sw.total) {
         PencilWork<T> x;
@@ -776,6 +777,10 @@ static int check_scalars(ps_handle* h) {
   if (h->h_sc->error_flags & 2) {
     h->err = "non-finite free energy";
     return PS_RUN_ERR;
+  }
+  if (h->h_sc->error_flags & 4) {
+    h->err = "a bulk shared-memory copy did not complete within the wait limit";
+    return PS_GPU_ERR;
   }
   return PS_OK;
 }

@@ -88,6 +88,58 @@ template <bool INV, typename C> struct Dft<8, INV, C> {
   }
 };
 
+// 16-point DFT as 4 x 4: radix-4 over n1 for each n2, twiddle w16^(n2 k1),
+// radix-4 over n2; output index k1 + 4 k2.
+template <bool INV, typename C> struct Dft<16, INV, C> {
+  template <int M>
+  static __device__ __forceinline__ C tw16(C x) {
+    using S = decltype(x.x);
+    constexpr int m = M % 16;
+    if constexpr (m == 0) {
+      return x;
+    } else if constexpr (m == 4) {
+      return mul_mi<INV>(x);
+    } else {
+      // w = (cos(pi m / 8), -sin(pi m / 8)), conjugated for the inverse
+      const S c1 = S(0.92387953251128675613), s1 = S(0.38268343236508977173);
+      const S c2 = S(0.70710678118654752440);
+      S wr, wi;
+      if constexpr (m == 1) { wr = c1; wi = -s1; }
+      else if constexpr (m == 2) { wr = c2; wi = -c2; }
+      else if constexpr (m == 3) { wr = s1; wi = -c1; }
+      else if constexpr (m == 6) { wr = -c2; wi = -c2; }
+      else { wr = -c1; wi = s1; }  // m == 9
+      if (INV) wi = -wi;
+      return C{x.x * wr - x.y * wi, x.x * wi + x.y * wr};
+    }
+  }
+  static __device__ __forceinline__ void run(C* v) {
+    C a[4][4];  // a[n2][k1]
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+      for (int n1 = 0; n1 < 4; ++n1) a[n2][n1] = v[4 * n1 + n2];
+      Dft<4, INV, C>::run(a[n2]);
+    }
+    a[1][1] = tw16<1>(a[1][1]);
+    a[1][2] = tw16<2>(a[1][2]);
+    a[1][3] = tw16<3>(a[1][3]);
+    a[2][1] = tw16<2>(a[2][1]);
+    a[2][2] = tw16<4>(a[2][2]);
+    a[2][3] = tw16<6>(a[2][3]);
+    a[3][1] = tw16<3>(a[3][1]);
+    a[3][2] = tw16<6>(a[3][2]);
+    a[3][3] = tw16<9>(a[3][3]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      C b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      Dft<4, INV, C>::run(b);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Radix plans.
 // ---------------------------------------------------------------------------
@@ -171,10 +223,16 @@ template <int L, int NS, int R, int... Rest> struct Passes<L, NS, RadixList<R, R
   }
 };
 
-// Batched FFT of B pencils of length L in shared memory.
-template <int L, int B, int T, bool INV, bool BFAST, typename C>
+// Batched FFT of B pencils of length L in shared memory (radix plan RL).
+template <int L, int B, int T, bool INV, bool BFAST, typename C, typename RL = typename Plan<L>::type>
 __device__ __forceinline__ void smem_fft(C* buf, int bs, int is, const C* tw) {
-  Passes<L, 1, typename Plan<L>::type>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
+  Passes<L, 1, RL>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
 }
+
+// Fewer, wider passes for the pencil kernel (more values per thread).
+template <int L> struct WidePlan { using type = typename Plan<L>::type; };
+template <> struct WidePlan<64> { using type = RadixList<16, 4>; };
+template <> struct WidePlan<128> { using type = RadixList<16, 8>; };
+template <> struct WidePlan<256> { using type = RadixList<16, 16>; };
 
 }  // namespace psb

@@ -17,6 +17,7 @@ template <typename T> struct PlaneWork {
   const T* wfac_in;   // wfac of the step being finished (nullptr = 1)
   const T* wfac_out;  // wfac of the step being started (nullptr = 1)
   T* store;           // slice receiving q (FIRST: the initial q; MID/LAST: q(s+ds))
+  int* status;        // error word: bit 2 set when a bulk copy did not land in time
   int mode;
   int pad;
 };

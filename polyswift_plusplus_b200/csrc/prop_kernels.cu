@@ -4,7 +4,8 @@
 //     q(s+ds) = wfac * Re(IFFT(k2 * FFT(wfac * q(s)))) / N
 // is split into two passes over a half spectrum S[x][y][kz] (kz <= nz/2) that
 // stays resident in L2 between passes:
-//   plane pass  (one CTA per x-plane, whole y-z plane in shared memory):
+//   plane pass  (one CTA per x-plane, whole y-z plane in shared memory, loaded
+//       and stored with one bulk TMA copy each):
 //       inverse y FFT -> inverse z c2r -> q = a*wfac_in -> store q(s+ds)
 //       -> a = q*wfac_out -> forward z r2c -> forward y FFT
 //     i.e. the end of step s and the start of step s+1 fused in one launch;
@@ -18,12 +19,33 @@
 
 #include "fft_smem.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace psb {
 
 template <typename T>
 __device__ __forceinline__ T ld_or_one(const T* p, size_t i) {
   return p ? __ldg(p + i) : T(1);
+}
+
+// 16-byte vector of T: 4 floats or 2 doubles.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <> struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
+template <typename V, typename T>
+__device__ __forceinline__ T vget(const V& v, int i) {
+  return reinterpret_cast<const T*>(&v)[i];
+}
+template <typename V, typename T>
+__device__ __forceinline__ void vset(V& v, int i, T x) {
+  reinterpret_cast<T*>(&v)[i] = x;
 }
 
 // Forward post-processing of one row: slots hold C = FFT_h(a_even + i a_odd),
@@ -83,9 +105,88 @@ __device__ __forceinline__ void c2r_pre(C* buf, const C* twn, int rows) {
   }
 }
 
+// Real-space part of a step on the tile held in shared memory (row stride RS
+// reals): MID: q = a*wfac_in, store q, a = q*wfac_out; LAST: q = a*wfac_in,
+// store q; FIRST: a = src (or 1), store a, a = a*wfac_out.
+template <typename T, int ROWS, int NZ, int TH>
+__device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_t roff, int rows) {
+  constexpr int RS = 2 * (NZ / 2 + 1);
+  using VT = Vec16<T>;
+  using V = typename VT::type;
+  constexpr int VN = VT::n;
+  if constexpr (NZ % VN == 0 && (ROWS * NZ / VN) % TH == 0) {
+    // vectorised, in chunks of UC vectors per thread whose global loads are all
+    // issued before any of them is used
+    constexpr int G = ROWS * NZ / VN;
+    constexpr int U = G / TH;
+    constexpr int UC = (U % 4 == 0) ? 4 : ((U % 3 == 0) ? 3 : ((U % 2 == 0) ? 2 : 1));
+    constexpr int ZV = NZ / VN;
+    static_assert(U % UC == 0, "chunking");
+    const bool same = (w.wfac_in == w.wfac_out);
+    const bool need_in = (w.mode != MODE_FIRST) && w.wfac_in;
+    const bool need_out = (w.mode != MODE_LAST) && w.wfac_out && !(w.mode == MODE_MID && same);
+    const bool need_src = (w.mode == MODE_FIRST) && w.src;
+#pragma unroll 1
+    for (int u0 = 0; u0 < U; u0 += UC) {
+      V a[UC], b[UC];
+#pragma unroll
+      for (int c = 0; c < UC; ++c) {
+        const int g = threadIdx.x + (u0 + c) * TH;
+        const int r = g / ZV;
+        const size_t gi = roff + (size_t)r * NZ + (size_t)(g - r * ZV) * VN;
+        if (r < rows) {
+          if (need_in) a[c] = __ldg(reinterpret_cast<const V*>(w.wfac_in + gi));
+          else if (need_src) a[c] = *reinterpret_cast<const V*>(w.src + gi);
+          if (need_out) b[c] = __ldg(reinterpret_cast<const V*>(w.wfac_out + gi));
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < UC; ++c) {
+        const int g = threadIdx.x + (u0 + c) * TH;
+        const int r = g / ZV;
+        const int z = (g - r * ZV) * VN;
+        if (r >= rows) continue;
+        const size_t gi = roff + (size_t)r * NZ + z;
+        T* sp = rbuf + r * RS + z;
+        V q;
+#pragma unroll
+        for (int i = 0; i < VN; ++i) {
+          T v;
+          if (w.mode == MODE_FIRST) v = need_src ? vget<V, T>(a[c], i) : T(1);
+          else v = sp[i] * (need_in ? vget<V, T>(a[c], i) : T(1));
+          vset(q, i, v);
+        }
+        if (w.store) *reinterpret_cast<V*>(w.store + gi) = q;
+        if (w.mode != MODE_LAST) {
+#pragma unroll
+          for (int i = 0; i < VN; ++i) {
+            T f = T(1);
+            if (need_out) f = vget<V, T>(b[c], i);
+            else if (w.mode == MODE_MID && same && need_in) f = vget<V, T>(a[c], i);
+            sp[i] = vget<V, T>(q, i) * f;
+          }
+        }
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < ROWS * NZ; e += TH) {
+      const int r = e / NZ;
+      const int z = e - r * NZ;
+      if (r >= rows) continue;
+      const size_t g = roff + (size_t)e;
+      T q;
+      if (w.mode == MODE_FIRST) q = w.src ? w.src[g] : T(1);
+      else q = rbuf[r * RS + z] * ld_or_one(w.wfac_in, g);
+      if (w.store) w.store[g] = q;
+      if (w.mode != MODE_LAST) rbuf[r * RS + z] = q * ld_or_one(w.wfac_out, g);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
-// Plane / row pass.  DO_Y: tile = one whole x-plane (ROWS = ny) and the y FFT
-// is done here; otherwise tile = ROWS consecutive (x,y) rows, z only.
+// Plane / row pass.  DO_Y: tile = one whole x-plane (ROWS = ny), moved in and
+// out with bulk TMA copies, and the y FFT is done here; otherwise tile = ROWS
+// consecutive (x,y) rows, z only.
 // ---------------------------------------------------------------------------
 template <typename T, int ROWS, int NZ, int TH, bool DO_Y>
 __global__ void __launch_bounds__(TH)
@@ -96,12 +197,14 @@ __global__ void __launch_bounds__(TH)
   constexpr int NZH = NZ / 2 + 1;
   constexpr int H = (NZ > 1) ? NZ / 2 : 1;
   constexpr int SPEC = ROWS * NZH;
-  constexpr int RS = 2 * NZH;  // real row stride inside the buffer
+  constexpr uint32_t SPEC_BYTES = (uint32_t)(SPEC * sizeof(C));
+  constexpr bool BULK = DO_Y && (SPEC_BYTES % 16 == 0);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s_tw_zh = reinterpret_cast<C*>(smem_raw);
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* s_tw_zh = buf + SPEC;
   C* s_tw_z = s_tw_zh + H;
   C* s_tw_y = s_tw_z + NZ;
-  C* buf = s_tw_y + (DO_Y ? ROWS : 0);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(s_tw_y + (DO_Y ? ROWS : 0));
   T* rbuf = reinterpret_cast<T*>(buf);
 
   const PlaneWork<T> w = works[blockIdx.y];
@@ -110,7 +213,14 @@ __global__ void __launch_bounds__(TH)
   const int rows = min(ROWS, nrows_total - row0);
   const size_t roff = (size_t)row0 * NZ;
   const size_t soff = (size_t)row0 * NZH;
+  const bool load_spec = (w.mode != MODE_FIRST);
 
+  if (BULK && load_spec && tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_arrive_expect_tx(bar, SPEC_BYTES);
+    bulk_g2s(buf, w.spec + soff, SPEC_BYTES, bar);
+  }
   if constexpr (NZ > 1) {
     for (int i = tid; i < H; i += TH) s_tw_zh[i] = tw_zh[i];
     for (int i = tid; i < NZ; i += TH) s_tw_z[i] = tw_z[i];
@@ -119,86 +229,113 @@ __global__ void __launch_bounds__(TH)
     for (int i = tid; i < ROWS; i += TH) s_tw_y[i] = tw_y[i];
   }
 
-  if (w.mode != MODE_FIRST) {
-    for (int i = tid; i < SPEC; i += TH) {
-      const int r = i / NZH;
-      buf[i] = (r < rows) ? w.spec[soff + i] : C{T(0), T(0)};
+  if (load_spec) {
+    if constexpr (BULK) {
+      __syncthreads();  // the mbarrier is initialised before anyone polls it
+      // every thread waits (bounded); the CTA then agrees on the outcome
+      const int ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0);
+      if (!ok) {
+        // the copy did not land in time: flag it, give the copy in flight one
+        // more bounded wait, and leave without touching the buffer
+        if (tid == 0) {
+          if (w.status) atomicOr(w.status, 4);
+          mbar_wait_bounded(bar, 0);
+        }
+        return;
+      }
+    } else {
+      for (int i = tid; i < SPEC; i += TH) {
+        const int r = i / NZH;
+        buf[i] = (r < rows) ? w.spec[soff + i] : C{T(0), T(0)};
+      }
     }
     __syncthreads();
     if constexpr (DO_Y) smem_fft<ROWS, NZH, TH, true, true>(buf, 1, NZH, s_tw_y);
     if constexpr (NZ > 1) {
       c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
       __syncthreads();
-      smem_fft<H, ROWS, TH, true, false>(buf, NZH, 1, s_tw_zh);
-    }
-    const bool mid = (w.mode == MODE_MID);
-    for (int e = tid; e < ROWS * NZ; e += TH) {
-      const int r = e / NZ;
-      const int z = e - r * NZ;
-      if (r >= rows) continue;
-      const size_t g = roff + (size_t)e;
-      const T a = rbuf[r * RS + z];
-      const T q = a * ld_or_one(w.wfac_in, g);
-      w.store[g] = q;
-      if (mid) rbuf[r * RS + z] = q * ld_or_one(w.wfac_out, g);
-    }
-    if (!mid) return;  // uniform over the CTA
-  } else {
-    for (int e = tid; e < ROWS * NZ; e += TH) {
-      const int r = e / NZ;
-      const int z = e - r * NZ;
-      T a = T(0);
-      if (r < rows) {
-        const size_t g = roff + (size_t)e;
-        a = w.src ? w.src[g] : T(1);
-        if (w.store) w.store[g] = a;
-        a = a * ld_or_one(w.wfac_out, g);
-      }
-      rbuf[r * RS + z] = a;
+      smem_fft<H, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
     }
   }
+  real_space<T, ROWS, NZ, TH>(w, rbuf, roff, rows);
+  if (w.mode == MODE_LAST) return;  // uniform over the CTA
   if constexpr (NZ == 1) {
     // one real per row: make it a complex number with zero imaginary part
     for (int r = tid; r < ROWS; r += TH) buf[r].y = T(0);
   }
   __syncthreads();
   if constexpr (NZ > 1) {
-    smem_fft<H, ROWS, TH, false, false>(buf, NZH, 1, s_tw_zh);
+    smem_fft<H, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
     r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
     __syncthreads();
   }
   if constexpr (DO_Y) smem_fft<ROWS, NZH, TH, false, true>(buf, 1, NZH, s_tw_y);
-  for (int i = tid; i < SPEC; i += TH) {
-    if (i / NZH < rows) w.spec[soff + i] = buf[i];
+  if constexpr (BULK) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      bulk_s2g(w.spec + soff, buf, SPEC_BYTES);
+      bulk_commit();
+      bulk_wait_read_all();
+    }
+  } else {
+    for (int i = tid; i < SPEC; i += TH) {
+      if (i / NZH < rows) w.spec[soff + i] = buf[i];
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Pencil pass along a strided axis.  Tile = TK adjacent columns of `inner`.
+// Pencil pass along a strided axis.  Tile = TK adjacent columns of `inner`,
+// loaded with 16-byte vector loads all issued before use.
 // ---------------------------------------------------------------------------
 template <typename T, int L, int TK, int TH, int MODE>
 __global__ void __launch_bounds__(TH)
     pencil_kernel(const PencilWork<T>* __restrict__ works, int inner, int tiles,
                   const c2_t<T>* __restrict__ tw, int nx, int ny, int nz) {
   using C = c2_t<T>;
-  constexpr int TKP = TK;  // row stride in shared memory
+  using V = typename Vec16<T>::type;
+  constexpr int CPV = 16 / sizeof(C);  // complex values per 16-byte vector
+  constexpr int VPR = TK / CPV;        // vectors per tile row
+  constexpr int NV = L * VPR;          // vectors per tile
+  constexpr int UV = (NV + TH - 1) / TH;
+  using RL = typename WidePlan<L>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s_tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = s_tw + L;
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* s_tw = buf + L * TK;
   const PencilWork<T> w = works[blockIdx.y];
   const int tid = threadIdx.x;
   const int o = blockIdx.x / tiles;
   const int c0 = (blockIdx.x - o * tiles) * TK;
   C* base = w.spec + (size_t)o * L * inner;
-  for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
-  for (int e = tid; e < L * TK; e += TH) {
-    const int i = e / TK;
-    const int cc = e - i * TK;
-    const int c = c0 + cc;
-    buf[i * TKP + cc] = (c < inner) ? base[(size_t)i * inner + c] : C{T(0), T(0)};
+  const bool full = (c0 + TK <= inner) && (inner % CPV == 0);
+  if (full) {
+    V v[UV];
+#pragma unroll
+    for (int u = 0; u < UV; ++u) {
+      const int e = tid + u * TH;
+      if (NV % TH == 0 || e < NV) {
+        const int i = e / VPR;
+        const int cv = e - i * VPR;
+        v[u] = *reinterpret_cast<const V*>(base + (size_t)i * inner + c0 + cv * CPV);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UV; ++u) {
+      const int e = tid + u * TH;
+      if (NV % TH == 0 || e < NV) reinterpret_cast<V*>(buf)[e] = v[u];
+    }
+  } else {
+    for (int e = tid; e < L * TK; e += TH) {
+      const int i = e / TK;
+      const int cc = e - i * TK;
+      const int c = c0 + cc;
+      buf[e] = (c < inner) ? base[(size_t)i * inner + c] : C{T(0), T(0)};
+    }
   }
+  for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
   __syncthreads();
-  if (MODE != PENCIL_INV) smem_fft<L, TK, TH, false, true>(buf, 1, TKP, s_tw);
+  if (MODE != PENCIL_INV) smem_fft<L, TK, TH, false, true, C, RL>(buf, 1, TK, s_tw);
   if (MODE == PENCIL_KINV) {
     for (int e = tid; e < L * TK; e += TH) {
       const int i = e / TK;
@@ -206,8 +343,8 @@ __global__ void __launch_bounds__(TH)
       const int c = c0 + cc;
       if (c < inner) {
         const T f = __ldg(w.kx + i) * __ldg(w.kyz + c);
-        C v = buf[i * TKP + cc];
-        buf[i * TKP + cc] = {v.x * f, v.y * f};
+        const C v = buf[e];
+        buf[e] = {v.x * f, v.y * f};
       }
     }
     __syncthreads();
@@ -226,18 +363,30 @@ __global__ void __launch_bounds__(TH)
         const double k1 = w.kfull[((size_t)i * ny + y) * nz + kz];
         const double k2 = w.kfull[((size_t)xm * ny + ym) * nz + zm];
         const T f = T(0.5 * (k1 + k2));
-        C v = buf[i * TKP + cc];
-        buf[i * TKP + cc] = {v.x * f, v.y * f};
+        const C v = buf[e];
+        buf[e] = {v.x * f, v.y * f};
       }
     }
     __syncthreads();
   }
-  if (MODE != PENCIL_FWD) smem_fft<L, TK, TH, true, true>(buf, 1, TKP, s_tw);
-  for (int e = tid; e < L * TK; e += TH) {
-    const int i = e / TK;
-    const int cc = e - i * TK;
-    const int c = c0 + cc;
-    if (c < inner) base[(size_t)i * inner + c] = buf[i * TKP + cc];
+  if (MODE != PENCIL_FWD) smem_fft<L, TK, TH, true, true, C, RL>(buf, 1, TK, s_tw);
+  if (full) {
+#pragma unroll
+    for (int u = 0; u < UV; ++u) {
+      const int e = tid + u * TH;
+      if (NV % TH == 0 || e < NV) {
+        const int i = e / VPR;
+        const int cv = e - i * VPR;
+        *reinterpret_cast<V*>(base + (size_t)i * inner + c0 + cv * CPV) = reinterpret_cast<const V*>(buf)[e];
+      }
+    }
+  } else {
+    for (int e = tid; e < L * TK; e += TH) {
+      const int i = e / TK;
+      const int cc = e - i * TK;
+      const int c = c0 + cc;
+      if (c < inner) base[(size_t)i * inner + c] = buf[e];
+    }
   }
 }
 
@@ -272,7 +421,8 @@ static cudaError_t launch_plane_t(const PlaneWork<T>* d_works, int nworks, int n
   using C = c2_t<T>;
   constexpr int NZH = NZ / 2 + 1;
   constexpr int H = (NZ > 1) ? NZ / 2 : 1;
-  const size_t smem = sizeof(C) * ((size_t)H + NZ + (DO_Y ? ROWS : 0) + (size_t)ROWS * NZH);
+  const size_t smem =
+      sizeof(C) * ((size_t)ROWS * NZH + H + NZ + (DO_Y ? ROWS : 0)) + sizeof(uint64_t);
   auto kern = plane_kernel<T, ROWS, NZ, TH, DO_Y>;
   static unsigned attr_mask = 0;
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
@@ -333,14 +483,14 @@ cudaError_t launch_rows_impl(const PlaneWork<T>* d_works, int nworks, int nrows,
   PSB_ROW_CASE(T, 4, 64, 128)
   PSB_ROW_CASE(T, 8, 32, 128)
   PSB_ROW_CASE(T, 12, 32, 128)
-  PSB_ROW_CASE(T, 16, 16, 128)
-  PSB_ROW_CASE(T, 24, 16, 128)
-  PSB_ROW_CASE(T, 32, 16, 256)
-  PSB_ROW_CASE(T, 48, 8, 128)
-  PSB_ROW_CASE(T, 64, 8, 256)
-  PSB_ROW_CASE(T, 96, 8, 256)
-  PSB_ROW_CASE(T, 128, 8, 256)
-  PSB_ROW_CASE(T, 256, 4, 256)
+  PSB_ROW_CASE(T, 16, 32, 128)
+  PSB_ROW_CASE(T, 24, 32, 128)
+  PSB_ROW_CASE(T, 32, 32, 256)
+  PSB_ROW_CASE(T, 48, 32, 256)
+  PSB_ROW_CASE(T, 64, 32, 256)
+  PSB_ROW_CASE(T, 96, 16, 256)
+  PSB_ROW_CASE(T, 128, 16, 256)
+  PSB_ROW_CASE(T, 256, 8, 256)
   return cudaErrorInvalidValue;
 }
 
@@ -348,7 +498,7 @@ template <typename T, int L, int TK, int TH, int MODE>
 static cudaError_t launch_pencil_t(const PencilWork<T>* d_works, int nworks, int outer, int inner,
                                    const c2_t<T>* tw, int nx, int ny, int nz, cudaStream_t st) {
   using C = c2_t<T>;
-  const size_t smem = sizeof(C) * ((size_t)L + (size_t)L * TK);
+  const size_t smem = sizeof(C) * ((size_t)L * TK + (size_t)L);
   auto kern = pencil_kernel<T, L, TK, TH, MODE>;
   static unsigned attr_mask = 0;
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
@@ -376,8 +526,9 @@ static cudaError_t launch_pencil_modes(const PencilWork<T>* d_works, int nworks,
   return cudaErrorInvalidValue;
 }
 
-template <typename T> struct PencilTK { static constexpr int v = 16; };
-template <> struct PencilTK<double> { static constexpr int v = 8; };
+// Tile widths: 256-byte rows (32 float2 or 16 double2 columns).
+template <typename T> struct PencilTK { static constexpr int v = 32; };
+template <> struct PencilTK<double> { static constexpr int v = 16; };
 
 #define PSB_PENCIL_CASE(T, L, TH)                                                          \
   if (len == L)                                                                             \
@@ -391,13 +542,13 @@ cudaError_t launch_pencil_impl(const PencilWork<T>* d_works, int nworks, int mod
   PSB_PENCIL_CASE(T, 1, 64)
   PSB_PENCIL_CASE(T, 4, 64)
   PSB_PENCIL_CASE(T, 8, 64)
-  PSB_PENCIL_CASE(T, 12, 64)
-  PSB_PENCIL_CASE(T, 16, 64)
-  PSB_PENCIL_CASE(T, 24, 64)
+  PSB_PENCIL_CASE(T, 12, 128)
+  PSB_PENCIL_CASE(T, 16, 128)
+  PSB_PENCIL_CASE(T, 24, 128)
   PSB_PENCIL_CASE(T, 32, 128)
-  PSB_PENCIL_CASE(T, 48, 128)
-  PSB_PENCIL_CASE(T, 64, 128)
-  PSB_PENCIL_CASE(T, 96, 128)
+  PSB_PENCIL_CASE(T, 48, 256)
+  PSB_PENCIL_CASE(T, 64, 256)
+  PSB_PENCIL_CASE(T, 96, 256)
   PSB_PENCIL_CASE(T, 128, 256)
   PSB_PENCIL_CASE(T, 256, 256)
   return cudaErrorInvalidValue;
