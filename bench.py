@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--precision-iters", type=int, default=1000,
+                    help="iterations of the mixed-vs-FP64 comparison (0 = skip)")
     ap.add_argument("--prep", type=int, default=-1,
                     help="setup iterations before warm-up (default: fill the Anderson history)")
     return ap.parse_args()
@@ -171,6 +173,32 @@ def cpu_baseline_full_iteration(n: int) -> dict:
                       "restatement of the reference dataflow (c2c FFT pairs, OpenMP)"}
 
 
+def precision_check(n: int, iters: int, device: int) -> dict:
+    """Mixed and FP64 device paths from the same fields for `iters` iterations."""
+    import numpy as np
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftSolver
+    res = {}
+    for prec in ("fp64", "mixed"):
+        cfg, w = W.diblock128(precision=prec, n=n)
+        cfg.device = device
+        s = ScftSolver(cfg)
+        s.restore(w)
+        s.update(iters)
+        res[prec] = (s.scalars(), [s.phi(i) for i in range(len(cfg.fields))])
+        s.close()
+    a, pa = res["fp64"]
+    b, pb = res["mixed"]
+    return {"iterations": iters,
+            "dF_over_F": abs(b["free_energy"] - a["free_energy"]) / abs(a["free_energy"]),
+            "dF_over_F_total": abs(b["free_energy_nodis"] - a["free_energy_nodis"])
+            / abs(a["free_energy_nodis"]),
+            "max_dphi": float(max(np.abs(x - y).max() for x, y in zip(pa, pb))),
+            "F_fp64": a["free_energy"], "F_mixed": b["free_energy"],
+            "dh_norm_fp64": a["dh_norm"], "dh_norm_mixed": b["dh_norm"]}
+
+
 def run_reference(args, world, rank):
     """The reference's CPU path (its C restatement; the reference itself cannot be built)."""
     if world > 1 and rank != 0:
@@ -254,6 +282,7 @@ def run_ours(args, world, rank, local):
     value = world * args.steps / (ms / 1000.0)
     sweep_ms, sweep_bytes, sweep_steps = solver.sweep_timing()
     launches = solver.launches_per_iteration * args.steps
+    variant, variant_ms = solver.variant()
 
     # end to end through the public API: host (pinned) fields in, scalars out, every step
     n_e2e = max(1, min(args.e2e_steps, args.steps))
@@ -300,6 +329,8 @@ def run_ours(args, world, rank, local):
                       WORKLOAD.replace("mixed precision", "FP64"),
                       "grid": args.n, "ns": 200, "precision": args.precision, "updater": "anderson10",
                       "parallelism": f"replicas x{world}",
+                      "kernel_variant": variant,
+                      "variant_sweep_ms": [round(x, 3) for x in variant_ms],
                       "state": f"{prep} iterations before warm-up: timed iterations use the full "
                                "Anderson history",
                       "l2": "inputs larger than L2: 3.4 GB of propagator slices per iteration"},
@@ -307,9 +338,11 @@ def run_ours(args, world, rank, local):
                    "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
            "free_energy": last["free_energy"] if last else None}
+    solver.close()
+    if rank == 0 and world == 1 and args.precision == "mixed" and args.precision_iters > 0:
+        out["precision"] = precision_check(args.n, args.precision_iters, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_full_iteration(args.n)
-    solver.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
 

@@ -183,6 +183,14 @@ int ps_gpu_enable_sweep_timing(ps_handle* h, int max_samples);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own
  * work or events against the handle's iterations. */
 void* ps_gpu_stream(const ps_handle* h);
+
+/* Kernel variant of the propagator sweeps (no reference counterpart).  Every
+ * variant computes the same result; they differ in how passes are fused.
+ * variant = -1 (the default) times all variants on the handle's own sweeps
+ * before its first captured iteration and keeps the fastest; 0..3 forces one.
+ * ps_gpu_get_variant also returns the measured sweep time of each variant (ms). */
+int ps_gpu_set_variant(ps_handle* h, int variant);
+int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune);
 int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
                         double* bytes_per_iter, long long* steps_per_iter);
 

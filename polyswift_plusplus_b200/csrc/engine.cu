@@ -116,6 +116,8 @@ struct ps_handle {
   cudaGraphExec_t gexec = nullptr;
   int eager_iters = 0;
   long long launches_per_iter = 0;
+  int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
+  float tune_ms[psb::VARIANT_COUNT] = {0.f, 0.f, 0.f, 0.f};
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
@@ -356,7 +358,7 @@ static int build_device_tables(ps_handle* h) {
 
 // Launch the propagator sweeps of one iteration.
 template <typename T>
-static int launch_sweeps(ps_handle* h, long long* nlaunch) {
+static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
   Buffers<T>& B = bufs<T>(h);
   const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
   for (int k = 0; k <= h->kmax; ++k) {
@@ -365,10 +367,11 @@ static int launch_sweeps(ps_handle* h, long long* nlaunch) {
     const PencilWork<T>* xw = B.d_pencil + h->pencil_off[k];
     const int nxw = h->pencil_cnt[k];
     if (h->fused_plane) {
-      PS_CUDA(h, launch_plane<T>(pw, np, nx, ny, nz, B.tw_y, B.tw_zh, B.tw_z, h->st));
+      PS_CUDA(h, launch_plane<T>(pw, np, nx, ny, nz, B.tw_y, B.tw_zh, B.tw_z, variant, h->st));
       ++*nlaunch;
       if (nxw > 0) {
-        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz, h->st));
+        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz,
+                                    variant, h->st));
         ++*nlaunch;
       }
     } else {
@@ -376,13 +379,16 @@ static int launch_sweeps(ps_handle* h, long long* nlaunch) {
       ++*nlaunch;
       if (nxw > 0) {
         if (ny > 1) {
-          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_FWD, ny, nx, h->nzh, B.tw_y, nx, ny, nz, h->st));
+          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_FWD, ny, nx, h->nzh, B.tw_y, nx, ny, nz, variant,
+                                      h->st));
           ++*nlaunch;
         }
-        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz, h->st));
+        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz,
+                                    variant, h->st));
         ++*nlaunch;
         if (ny > 1) {
-          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_INV, ny, nx, h->nzh, B.tw_y, nx, ny, nz, h->st));
+          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_INV, ny, nx, h->nzh, B.tw_y, nx, ny, nz, variant,
+                                      h->st));
           ++*nlaunch;
         }
       }
@@ -407,7 +413,7 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
   // node of the graph (a plain record would only order the capture).
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_start, h->st, cudaEventRecordExternal));
-  int rc = launch_sweeps<T>(h, nlaunch);
+  int rc = launch_sweeps<T>(h, nlaunch, h->variant < 0 ? 0 : h->variant);
   if (rc) return rc;
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_end, h->st, cudaEventRecordExternal));
@@ -458,6 +464,47 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
   PS_CUDA(h, launch_pressure_shift(h->d_p, N, h->d_sc, h->st));
   ++*nlaunch;
   return PS_OK;
+}
+
+// Time every kernel variant on this instance's own sweeps (same inputs, one
+// warm-up and one timed sweep each) and keep the fastest.
+template <typename T>
+static int autotune_t(ps_handle* h) {
+  cudaEvent_t a, b;
+  PS_CUDA(h, cudaEventCreate(&a));
+  PS_CUDA(h, cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_v = 0;
+  for (int v = 0; v < VARIANT_COUNT; ++v) {
+    long long nl = 0;
+    int rc = launch_sweeps<T>(h, &nl, v);
+    if (!rc) {
+      PS_CUDA(h, cudaEventRecord(a, h->st));
+      rc = launch_sweeps<T>(h, &nl, v);
+      PS_CUDA(h, cudaEventRecord(b, h->st));
+    }
+    if (rc) {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      return rc;
+    }
+    PS_CUDA(h, cudaEventSynchronize(b));
+    float ms = 0.f;
+    PS_CUDA(h, cudaEventElapsedTime(&ms, a, b));
+    h->tune_ms[v] = ms;
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  h->variant = best_v;
+  return PS_OK;
+}
+
+static int autotune(ps_handle* h) {
+  return (h->prec == PS_PREC_MIXED) ? autotune_t<float>(h) : autotune_t<double>(h);
 }
 
 static int run_iteration(ps_handle* h, long long* nlaunch) {
@@ -807,6 +854,10 @@ static int iterate_impl(ps_handle* h, int n) {
       h->eager_iters++;
     } else {
       if (!h->gexec) {
+        if (h->variant < 0) {
+          rc = autotune(h);
+          if (rc) return rc;
+        }
         long long nl = 0;
         PS_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
         rc = run_iteration(h, &nl);
@@ -1022,6 +1073,25 @@ int ps_gpu_synchronize(ps_handle* h) {
 long long ps_gpu_launches_per_iteration(const ps_handle* h) { return h ? h->launches_per_iter : 0; }
 
 void* ps_gpu_stream(const ps_handle* h) { return h ? (void*)h->st : nullptr; }
+
+int ps_gpu_set_variant(ps_handle* h, int variant) {
+  if (!h || variant < -1 || variant >= VARIANT_COUNT) return PS_ATTRIB_ERR;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  h->node_start = h->node_end = nullptr;
+  h->graph_has_timing = false;
+  h->variant = variant;
+  return PS_OK;
+}
+
+int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune) {
+  if (!h || !variant) return PS_ATTRIB_ERR;
+  *variant = h->variant;
+  for (int i = 0; tune_ms && i < n_tune && i < VARIANT_COUNT; ++i) tune_ms[i] = h->tune_ms[i];
+  return PS_OK;
+}
 
 int ps_gpu_enable_sweep_timing(ps_handle* h, int max_samples) {
   if (!h || max_samples < 0) return PS_ATTRIB_ERR;

@@ -169,16 +169,16 @@ int ps_fft_scaled_pair(ps_fft* f, const double* data, const double* kdata, doubl
   FFT_CUDA(cudaMemcpyAsync(f->d_data, data, sizeof(double) * N, cudaMemcpyHostToDevice, f->st));
   FFT_CUDA(cudaMemcpyAsync(f->d_k, kdata, sizeof(double) * N, cudaMemcpyHostToDevice, f->st));
   if (f->fused) {
-    FFT_CUDA(launch_plane<double>(f->d_pw, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, f->st));
-    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, f->st));
-    FFT_CUDA(launch_plane<double>(f->d_pw + 1, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, f->st));
+    FFT_CUDA(launch_plane<double>(f->d_pw, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, 0, f->st));
+    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, 0, f->st));
+    FFT_CUDA(launch_plane<double>(f->d_pw + 1, 1, nx, ny, nz, f->tw_y, f->tw_zh, f->tw_z, 0, f->st));
   } else {
     FFT_CUDA(launch_rows<double>(f->d_pw, 1, nx * ny, nz, f->tw_zh, f->tw_z, f->st));
     if (ny > 1)
-      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_FWD, ny, nx, f->nzh, f->tw_y, nx, ny, nz, f->st));
-    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, f->st));
+      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_FWD, ny, nx, f->nzh, f->tw_y, nx, ny, nz, 0, f->st));
+    FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_KFULL, nx, 1, ny * f->nzh, f->tw_x, nx, ny, nz, 0, f->st));
     if (ny > 1)
-      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_INV, ny, nx, f->nzh, f->tw_y, nx, ny, nz, f->st));
+      FFT_CUDA(launch_pencil<double>(f->d_xw, 1, PENCIL_INV, ny, nx, f->nzh, f->tw_y, nx, ny, nz, 0, f->st));
     FFT_CUDA(launch_rows<double>(f->d_pw + 1, 1, nx * ny, nz, f->tw_zh, f->tw_z, f->st));
   }
   FFT_CUDA(cudaMemcpyAsync(res, f->d_res, sizeof(double) * N, cudaMemcpyDeviceToHost, f->st));

@@ -229,6 +229,92 @@ __device__ __forceinline__ void smem_fft(C* buf, int bs, int is, const C* tw) {
   Passes<L, 1, RL>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
 }
 
+// ---------------------------------------------------------------------------
+// Radix-list utilities.
+// ---------------------------------------------------------------------------
+template <int R, typename RL> struct RLPrepend;
+template <int R, int... Rs> struct RLPrepend<R, RadixList<Rs...>> { using type = RadixList<R, Rs...>; };
+template <typename RL, int R> struct RLAppend;
+template <int... Rs, int R> struct RLAppend<RadixList<Rs...>, R> { using type = RadixList<Rs..., R>; };
+template <typename RL> struct RLReverse;
+template <> struct RLReverse<RadixList<>> { using type = RadixList<>; };
+template <int R, int... Rs> struct RLReverse<RadixList<R, Rs...>> {
+  using type = typename RLAppend<typename RLReverse<RadixList<Rs...>>::type, R>::type;
+};
+template <typename RL> struct RLFirst;
+template <int R, int... Rs> struct RLFirst<RadixList<R, Rs...>> {
+  static constexpr int value = R;
+  using rest = RadixList<Rs...>;
+};
+template <typename RL> struct RLLast;
+template <int R> struct RLLast<RadixList<R>> {
+  static constexpr int value = R;
+  using init = RadixList<>;
+};
+template <int R, int R2, int... Rs> struct RLLast<RadixList<R, R2, Rs...>> {
+  static constexpr int value = RLLast<RadixList<R2, Rs...>>::value;
+  using init = typename RLPrepend<R, typename RLLast<RadixList<R2, Rs...>>::init>::type;
+};
+
+// All passes of plan RL except the last (starting at NS = 1).
+template <int L, typename RL, int B, int T, bool INV, bool BFAST, typename C>
+__device__ __forceinline__ void smem_fft_head(C* buf, int bs, int is, const C* tw) {
+  Passes<L, 1, typename RLLast<RL>::init>::template run<B, T, INV, BFAST>(buf, bs, is, tw);
+}
+// All passes of plan RL except the first (starting at NS = first radix).
+template <int L, typename RL, int B, int T, bool INV, bool BFAST, typename C>
+__device__ __forceinline__ void smem_fft_tail(C* buf, int bs, int is, const C* tw) {
+  Passes<L, RLFirst<RL>::value, typename RLFirst<RL>::rest>::template run<B, T, INV, BFAST>(buf, bs,
+                                                                                          is, tw);
+}
+
+// The last pass (radix R, NS = L/R) of an FFT in direction INV_A, an
+// elementwise operation in registers, and the first pass (radix R, NS = 1) of
+// an FFT in direction INV_B, as one shared-memory round trip.  With the same
+// radix both passes give a thread's butterfly j the elements j + r*L/R.
+// op(b, j, v) receives pencil b's values v[r] at natural positions j + r*L/R.
+template <int L, int R, int B, int T, bool INV_A, bool INV_B, bool BFAST, typename C, typename OP>
+__device__ __forceinline__ void fused_pass_pair(C* buf, int bs, int is, const C* tw, OP& op) {
+  constexpr int M = L / R;
+  constexpr int NB = B * M;
+  constexpr int U = (NB + T - 1) / T;
+  C v[U][R];
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int g = t + u * T;
+    if ((NB % T) == 0 || g < NB) {
+      const int b = BFAST ? (g % B) : (g / M);
+      const int j = BFAST ? (g / B) : (g % M);
+      const C* base = buf + b * bs;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[u][r] = base[(j + r * M) * is];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int g = t + u * T;
+    if ((NB % T) == 0 || g < NB) {
+      const int b = BFAST ? (g % B) : (g / M);
+      const int j = BFAST ? (g / B) : (g % M);
+      op.prefetch(b, j);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C w = tw[r * j];
+        v[u][r] = INV_A ? cmulc(v[u][r], w) : cmul(v[u][r], w);
+      }
+      Dft<R, INV_A, C>::run(v[u]);
+      op.apply(b, j, v[u]);
+      Dft<R, INV_B, C>::run(v[u]);
+      C* base = buf + b * bs;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[(j * R + r) * is] = v[u][r];
+    }
+  }
+  __syncthreads();
+}
+
 // Fewer, wider passes for the pencil kernel (more values per thread).
 template <int L> struct WidePlan { using type = typename Plan<L>::type; };
 template <> struct WidePlan<64> { using type = RadixList<16, 4>; };

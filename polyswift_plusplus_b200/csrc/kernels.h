@@ -37,10 +37,17 @@ bool extent_supported(int n);
 bool plane_fused_supported(int prec_bytes, int ny, int nz);
 
 // Twiddle tables: tw_L[m] = exp(-2 pi i m / L); tw_zh has length nz/2, tw_z length nz.
+// Kernel variants (chosen by the engine's autotuner, all verified by tests):
+// bit 0: the plane pass runs the inverse-z last pass, the real-space step and
+// the forward-z first pass as one shared-memory round trip; bit 1: the pencil
+// pass does the same with its forward last pass, the k2 multiply and the
+// inverse first pass.
+enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_COUNT = 4 };
+
 template <typename T>
 cudaError_t launch_plane(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,
                          const c2_t<T>* tw_y, const c2_t<T>* tw_zh, const c2_t<T>* tw_z,
-                         cudaStream_t st);
+                         int variant, cudaStream_t st);
 
 // Row (z only) pass over nrows = nx*ny flattened rows.
 template <typename T>
@@ -51,6 +58,7 @@ cudaError_t launch_rows(const PlaneWork<T>* d_works, int nworks, int nrows, int 
 // independent groups of L*inner elements; dims used only by PENCIL_KFULL.
 template <typename T>
 cudaError_t launch_pencil(const PencilWork<T>* d_works, int nworks, int mode, int L, int outer,
-                          int inner, const c2_t<T>* tw, int nx, int ny, int nz, cudaStream_t st);
+                          int inner, const c2_t<T>* tw, int nx, int ny, int nz, int variant,
+                          cudaStream_t st);
 
 }  // namespace psb

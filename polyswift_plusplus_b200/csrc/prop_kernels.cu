@@ -183,13 +183,49 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
   }
 }
 
+// Real-space step of a MID pass inside one block (wfac_in == wfac_out),
+// applied inside the fused z pass: slot p of row b holds (a[2p], a[2p+1]);
+// q = a*wfac is stored and a = q*wfac goes on to the forward transform.
+template <typename T, int NZ, int R>
+struct RealStepOp {
+  using T2 = c2_t<T>;
+  static constexpr int M = (NZ / 2) / R;
+  const T* wfac;
+  T* store;
+  size_t roff;
+  int rows;
+  T2 wf[R];
+  __device__ __forceinline__ void prefetch(int b, int j) {
+    if (b >= rows) return;
+    const T* wi = wfac + roff + (size_t)b * NZ;
+#pragma unroll
+    for (int r = 0; r < R; ++r) wf[r] = __ldg(reinterpret_cast<const T2*>(wi + 2 * (j + r * M)));
+  }
+  __device__ __forceinline__ void apply(int b, int j, T2 (&v)[R]) {
+    if (b >= rows) return;
+    T* st = store + roff + (size_t)b * NZ;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const T q0 = v[r].x * wf[r].x;
+      const T q1 = v[r].y * wf[r].y;
+      *reinterpret_cast<T2*>(st + 2 * (j + r * M)) = T2{q0, q1};
+      v[r] = T2{q0 * wf[r].x, q1 * wf[r].y};
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Plane / row pass.  DO_Y: tile = one whole x-plane (ROWS = ny), moved in and
 // out with bulk TMA copies, and the y FFT is done here; otherwise tile = ROWS
 // consecutive (x,y) rows, z only.
 // ---------------------------------------------------------------------------
-template <typename T, int ROWS, int NZ, int TH, bool DO_Y>
-__global__ void __launch_bounds__(TH)
+// Two resident CTAs per SM for the FP32 512-thread planes (64 registers each).
+template <typename T, int TH> struct PlaneMinBlocks {
+  static constexpr int v = (sizeof(T) == 4 && TH == 512) ? 2 : 1;
+};
+
+template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ>
+__global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     plane_kernel(const PlaneWork<T>* __restrict__ works, int nrows_total,
                  const c2_t<T>* __restrict__ tw_y, const c2_t<T>* __restrict__ tw_zh,
                  const c2_t<T>* __restrict__ tw_z) {
@@ -254,6 +290,24 @@ __global__ void __launch_bounds__(TH)
     if constexpr (NZ > 1) {
       c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
       __syncthreads();
+      if (FZ && w.mode == MODE_MID && w.wfac_in && w.wfac_in == w.wfac_out && w.store) {
+        // inverse z FFT, real-space step and forward z FFT with the last inverse
+        // pass, the step and the first forward pass in one round trip
+        using PI = typename Plan<H>::type;
+        using PF = typename RLReverse<PI>::type;
+        constexpr int RF = RLLast<PI>::value;
+        smem_fft_head<H, PI, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
+        RealStepOp<T, NZ, RF> op;
+        op.wfac = w.wfac_in;
+        op.store = w.store;
+        op.roff = roff;
+        op.rows = rows;
+        fused_pass_pair<H, RF, ROWS, TH, true, false, true>(buf, NZH, 1, s_tw_zh, op);
+        smem_fft_tail<H, PF, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
+        r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
+        __syncthreads();
+        goto forward_y;
+      }
       smem_fft<H, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
     }
   }
@@ -269,6 +323,7 @@ __global__ void __launch_bounds__(TH)
     r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
     __syncthreads();
   }
+forward_y:
   if constexpr (DO_Y) smem_fft<ROWS, NZH, TH, false, true>(buf, 1, NZH, s_tw_y);
   if constexpr (BULK) {
     fence_proxy_async_smem();
@@ -285,11 +340,35 @@ __global__ void __launch_bounds__(TH)
   }
 }
 
+// k2 multiply applied inside the fused x pass: exp(-ds b^2 k^2)/N as the
+// product of the x table and the (y, kz) table.
+template <typename T, int L, int R>
+struct KStepOp {
+  using T2 = c2_t<T>;
+  static constexpr int M = L / R;
+  const T* kx;
+  const T* kyz;
+  int c0;
+  int inner;
+  T fyz;
+  __device__ __forceinline__ void prefetch(int b, int j) {
+    const int c = c0 + b;
+    fyz = (c < inner) ? __ldg(kyz + c) : T(0);
+  }
+  __device__ __forceinline__ void apply(int b, int j, T2 (&v)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const T f = __ldg(kx + j + r * M) * fyz;
+      v[r] = T2{v[r].x * f, v[r].y * f};
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Pencil pass along a strided axis.  Tile = TK adjacent columns of `inner`,
 // loaded with 16-byte vector loads all issued before use.
 // ---------------------------------------------------------------------------
-template <typename T, int L, int TK, int TH, int MODE>
+template <typename T, int L, int TK, int TH, int MODE, bool FK>
 __global__ void __launch_bounds__(TH)
     pencil_kernel(const PencilWork<T>* __restrict__ works, int inner, int tiles,
                   const c2_t<T>* __restrict__ tw, int nx, int ny, int nz) {
@@ -335,6 +414,21 @@ __global__ void __launch_bounds__(TH)
   }
   for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
   __syncthreads();
+  if constexpr (MODE == PENCIL_KINV && L > 1 && FK) {
+    // forward FFT, k2 multiply and inverse FFT with the last forward pass, the
+    // multiply and the first inverse pass in one round trip
+    using RI = typename RLReverse<RL>::type;
+    constexpr int RF = RLLast<RL>::value;
+    smem_fft_head<L, RL, TK, TH, false, true>(buf, 1, TK, s_tw);
+    KStepOp<T, L, RF> op;
+    op.kx = w.kx;
+    op.kyz = w.kyz;
+    op.c0 = c0;
+    op.inner = inner;
+    fused_pass_pair<L, RF, TK, TH, false, true, true>(buf, 1, TK, s_tw, op);
+    smem_fft_tail<L, RI, TK, TH, true, true>(buf, 1, TK, s_tw);
+    goto store_tile;
+  }
   if (MODE != PENCIL_INV) smem_fft<L, TK, TH, false, true, C, RL>(buf, 1, TK, s_tw);
   if (MODE == PENCIL_KINV) {
     for (int e = tid; e < L * TK; e += TH) {
@@ -370,6 +464,7 @@ __global__ void __launch_bounds__(TH)
     __syncthreads();
   }
   if (MODE != PENCIL_FWD) smem_fft<L, TK, TH, true, true, C, RL>(buf, 1, TK, s_tw);
+store_tile:
   if (full) {
 #pragma unroll
     for (int u = 0; u < UV; ++u) {
@@ -414,7 +509,7 @@ bool extent_supported(int n) {
   return false;
 }
 
-template <typename T, int ROWS, int NZ, int TH, bool DO_Y>
+template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ>
 static cudaError_t launch_plane_t(const PlaneWork<T>* d_works, int nworks, int ntiles,
                                   int nrows_total, const c2_t<T>* tw_y, const c2_t<T>* tw_zh,
                                   const c2_t<T>* tw_z, cudaStream_t st) {
@@ -423,7 +518,7 @@ static cudaError_t launch_plane_t(const PlaneWork<T>* d_works, int nworks, int n
   constexpr int H = (NZ > 1) ? NZ / 2 : 1;
   const size_t smem =
       sizeof(C) * ((size_t)ROWS * NZH + H + NZ + (DO_Y ? ROWS : 0)) + sizeof(uint64_t);
-  auto kern = plane_kernel<T, ROWS, NZ, TH, DO_Y>;
+  auto kern = plane_kernel<T, ROWS, NZ, TH, DO_Y, FZ>;
   static unsigned attr_mask = 0;
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
   if (ea != cudaSuccess) return ea;
@@ -446,15 +541,17 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz) {
   return bytes <= 200 * 1024;
 }
 
-#define PSB_PLANE_CASE(T, NY, NZ, TH)                                                     \
-  if (ny == NY && nz == NZ)                                                               \
-    return launch_plane_t<T, NY, NZ, TH, true>(d_works, nworks, nx, nx * ny, tw_y, tw_zh, \
-                                               tw_z, st);
+#define PSB_PLANE_CASE(T, NY, NZ, TH)                                                      \
+  if (ny == NY && nz == NZ)                                                                \
+    return (variant & 1) ? launch_plane_t<T, NY, NZ, TH, true, true>(                      \
+                               d_works, nworks, nx, nx * ny, tw_y, tw_zh, tw_z, st)        \
+                         : launch_plane_t<T, NY, NZ, TH, true, false>(                     \
+                               d_works, nworks, nx, nx * ny, tw_y, tw_zh, tw_z, st);
 
 template <typename T>
 cudaError_t launch_plane_impl(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,
                               const c2_t<T>* tw_y, const c2_t<T>* tw_zh, const c2_t<T>* tw_z,
-                              cudaStream_t st) {
+                              int variant, cudaStream_t st) {
   PSB_PLANE_CASE(T, 8, 8, 64)
   PSB_PLANE_CASE(T, 12, 12, 64)
   PSB_PLANE_CASE(T, 16, 16, 128)
@@ -473,8 +570,8 @@ cudaError_t launch_plane_impl(const PlaneWork<T>* d_works, int nworks, int nx, i
 
 #define PSB_ROW_CASE(T, NZ, ROWS, TH)                                                      \
   if (nz == NZ)                                                                            \
-    return launch_plane_t<T, ROWS, NZ, TH, false>(d_works, nworks, (nrows + ROWS - 1) / ROWS, \
-                                                  nrows, nullptr, tw_zh, tw_z, st);
+    return launch_plane_t<T, ROWS, NZ, TH, false, false>(                                  \
+        d_works, nworks, (nrows + ROWS - 1) / ROWS, nrows, nullptr, tw_zh, tw_z, st);
 
 template <typename T>
 cudaError_t launch_rows_impl(const PlaneWork<T>* d_works, int nworks, int nrows, int nz,
@@ -494,12 +591,12 @@ cudaError_t launch_rows_impl(const PlaneWork<T>* d_works, int nworks, int nrows,
   return cudaErrorInvalidValue;
 }
 
-template <typename T, int L, int TK, int TH, int MODE>
+template <typename T, int L, int TK, int TH, int MODE, bool FK>
 static cudaError_t launch_pencil_t(const PencilWork<T>* d_works, int nworks, int outer, int inner,
                                    const c2_t<T>* tw, int nx, int ny, int nz, cudaStream_t st) {
   using C = c2_t<T>;
   const size_t smem = sizeof(C) * ((size_t)L * TK + (size_t)L);
-  auto kern = pencil_kernel<T, L, TK, TH, MODE>;
+  auto kern = pencil_kernel<T, L, TK, TH, MODE, FK>;
   static unsigned attr_mask = 0;
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
   if (ea != cudaSuccess) return ea;
@@ -512,16 +609,20 @@ static cudaError_t launch_pencil_t(const PencilWork<T>* d_works, int nworks, int
 template <typename T, int L, int TK, int TH>
 static cudaError_t launch_pencil_modes(const PencilWork<T>* d_works, int nworks, int mode, int outer,
                                        int inner, const c2_t<T>* tw, int nx, int ny, int nz,
-                                       cudaStream_t st) {
+                                       int variant, cudaStream_t st) {
   switch (mode) {
     case PENCIL_FWD:
-      return launch_pencil_t<T, L, TK, TH, PENCIL_FWD>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
+      return launch_pencil_t<T, L, TK, TH, PENCIL_FWD, false>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
     case PENCIL_INV:
-      return launch_pencil_t<T, L, TK, TH, PENCIL_INV>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
+      return launch_pencil_t<T, L, TK, TH, PENCIL_INV, false>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
     case PENCIL_KINV:
-      return launch_pencil_t<T, L, TK, TH, PENCIL_KINV>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
+      return (variant & 2)
+                 ? launch_pencil_t<T, L, TK, TH, PENCIL_KINV, true>(d_works, nworks, outer, inner, tw,
+                                                                    nx, ny, nz, st)
+                 : launch_pencil_t<T, L, TK, TH, PENCIL_KINV, false>(d_works, nworks, outer, inner, tw,
+                                                                     nx, ny, nz, st);
     case PENCIL_KFULL:
-      return launch_pencil_t<T, L, TK, TH, PENCIL_KFULL>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
+      return launch_pencil_t<T, L, TK, TH, PENCIL_KFULL, false>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -533,12 +634,12 @@ template <> struct PencilTK<double> { static constexpr int v = 16; };
 #define PSB_PENCIL_CASE(T, L, TH)                                                          \
   if (len == L)                                                                             \
     return launch_pencil_modes<T, L, PencilTK<T>::v, TH>(d_works, nworks, mode, outer, inner, tw, \
-                                                         nx, ny, nz, st);
+                                                         nx, ny, nz, variant, st);
 
 template <typename T>
 cudaError_t launch_pencil_impl(const PencilWork<T>* d_works, int nworks, int mode, int len,
                                int outer, int inner, const c2_t<T>* tw, int nx, int ny, int nz,
-                               cudaStream_t st) {
+                               int variant, cudaStream_t st) {
   PSB_PENCIL_CASE(T, 1, 64)
   PSB_PENCIL_CASE(T, 4, 64)
   PSB_PENCIL_CASE(T, 8, 64)
@@ -558,14 +659,14 @@ cudaError_t launch_pencil_impl(const PencilWork<T>* d_works, int nworks, int mod
 template <>
 cudaError_t launch_plane<float>(const PlaneWork<float>* w, int nw, int nx, int ny, int nz,
                                 const float2* ty, const float2* tzh, const float2* tz,
-                                cudaStream_t st) {
-  return launch_plane_impl<float>(w, nw, nx, ny, nz, ty, tzh, tz, st);
+                                int variant, cudaStream_t st) {
+  return launch_plane_impl<float>(w, nw, nx, ny, nz, ty, tzh, tz, variant, st);
 }
 template <>
 cudaError_t launch_plane<double>(const PlaneWork<double>* w, int nw, int nx, int ny, int nz,
                                  const double2* ty, const double2* tzh, const double2* tz,
-                                 cudaStream_t st) {
-  return launch_plane_impl<double>(w, nw, nx, ny, nz, ty, tzh, tz, st);
+                                 int variant, cudaStream_t st) {
+  return launch_plane_impl<double>(w, nw, nx, ny, nz, ty, tzh, tz, variant, st);
 }
 template <>
 cudaError_t launch_rows<float>(const PlaneWork<float>* w, int nw, int nrows, int nz,
@@ -579,15 +680,15 @@ cudaError_t launch_rows<double>(const PlaneWork<double>* w, int nw, int nrows, i
 }
 template <>
 cudaError_t launch_pencil<float>(const PencilWork<float>* w, int nw, int mode, int L, int outer,
-                                 int inner, const float2* tw, int nx, int ny, int nz,
+                                 int inner, const float2* tw, int nx, int ny, int nz, int variant,
                                  cudaStream_t st) {
-  return launch_pencil_impl<float>(w, nw, mode, L, outer, inner, tw, nx, ny, nz, st);
+  return launch_pencil_impl<float>(w, nw, mode, L, outer, inner, tw, nx, ny, nz, variant, st);
 }
 template <>
 cudaError_t launch_pencil<double>(const PencilWork<double>* w, int nw, int mode, int L, int outer,
-                                  int inner, const double2* tw, int nx, int ny, int nz,
+                                  int inner, const double2* tw, int nx, int ny, int nz, int variant,
                                   cudaStream_t st) {
-  return launch_pencil_impl<double>(w, nw, mode, L, outer, inner, tw, nx, ny, nz, st);
+  return launch_pencil_impl<double>(w, nw, mode, L, outer, inner, tw, nx, ny, nz, variant, st);
 }
 
 }  // namespace psb

@@ -72,6 +72,34 @@ def test_fp64_diblock_parity(gpu, oracle_lib, n):
     assert g.launches_per_iteration > 0
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("n", [16, 32])
+def test_every_kernel_variant_matches_oracle(gpu, oracle_lib, variant, n):
+    cfg, w = W.diblock32(n=n)
+    g = ScftSolver(cfg)
+    g.set_variant(variant)
+    g.restore(w)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(4)
+    hg = []
+    for _ in range(4):
+        g.update(1)
+        hg.append(g.scalars())
+    assert g.variant()[0] == variant
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_autotune_picks_a_measured_variant(gpu):
+    cfg, w = W.diblock32(n=32, precision="mixed")
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(3)
+    v, ms = g.variant()
+    assert 0 <= v < 4 and all(t > 0 for t in ms)
+    assert ms[v] == min(ms)
+
+
 def test_fp64_propagator_slices(gpu, oracle_lib):
     cfg, w = W.diblock32(n=16)
     g, o, _, _ = run_both(cfg, w, 2)
@@ -200,10 +228,14 @@ def test_reference_random_init_and_noise(gpu, oracle_lib):
 
 
 def test_mixed_precision_close_to_fp64_at_convergence(gpu):
-    """|dF/F| < 1e-6 between the mixed (FP32 sweeps) and FP64 paths at a converged
-    state.  At the saddle point F is stationary in w and phi, so the FP32 error
-    of phi enters F only at second order; far from convergence it enters at
-    first order (about 6e-5 after 20 iterations of this case)."""
+    """Mixed (FP32 sweeps) against FP64 at a converged state of a 32^3, Ns = 100
+    diblock.  F is stationary in w and phi at the saddle point, but -ln Q enters
+    F at first order, and Q from FP32 FFT sweeps carries the round-off of 2 Ns
+    transforms: about 1e-6 relative, varying from iteration to iteration (a
+    single-precision numpy/pocketfft sweep of the same fields gives 6e-7 over
+    100 steps).  That puts a floor of about 5e-6 (absolute) on F: about 1.5e-5
+    relative to the disorder-subtracted F of -0.33 here and about 1.5e-6
+    relative to the total F (without the disorder subtraction, 3.87 here)."""
     out = {}
     for prec in ("fp64", "mixed"):
         cfg, w = W.diblock32(n=32, precision=prec)
@@ -217,9 +249,13 @@ def test_mixed_precision_close_to_fp64_at_convergence(gpu):
     s32, phi32 = out["mixed"]
     assert s64["dh_norm"] < 1e-6
     dfe = abs(s32["free_energy"] - s64["free_energy"]) / abs(s64["free_energy"])
+    dfe_tot = (abs(s32["free_energy_nodis"] - s64["free_energy_nodis"])
+               / abs(s64["free_energy_nodis"]))
     dphi = max(np.abs(a - b).max() for a, b in zip(phi32, phi64))
-    print(f"mixed vs fp64 at convergence: |dF/F| = {dfe:.3e}, max|dphi| = {dphi:.3e}")
-    assert dfe < 1e-6
+    print(f"mixed vs fp64 at convergence: |dF/F| = {dfe:.3e} (total F: {dfe_tot:.3e}), "
+          f"max|dphi| = {dphi:.3e}")
+    assert dfe < 1e-4
+    assert dfe_tot < 1e-5
     # the lamellae may translate by a fraction of a cell under FP32 noise (a zero
     # mode of the saddle point), so max|dphi| is reported and only sanity-bounded
     assert dphi < 1e-2
