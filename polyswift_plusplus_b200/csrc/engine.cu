@@ -117,7 +117,8 @@ struct ps_handle {
   int eager_iters = 0;
   long long launches_per_iter = 0;
   int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
-  float tune_ms[psb::VARIANT_COUNT] = {0.f, 0.f, 0.f, 0.f};
+  float tune_ms[psb::VARIANT_COUNT] = {};
+  bool xy_ok = false;  // the row + x-y plane design exists for this grid
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
@@ -366,7 +367,14 @@ static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
     const int np = h->plane_cnt[k];
     const PencilWork<T>* xw = B.d_pencil + h->pencil_off[k];
     const int nxw = h->pencil_cnt[k];
-    if (h->fused_plane) {
+    if ((variant & VARIANT_XY) && h->xy_ok) {
+      PS_CUDA(h, launch_rows_t<T>(pw, np, nx, ny, nz, B.tw_zh, B.tw_z, h->st));
+      ++*nlaunch;
+      if (nxw > 0) {
+        PS_CUDA(h, launch_xy<T>(xw, nxw, nx, h->nzh, B.tw_x, variant, h->st));
+        ++*nlaunch;
+      }
+    } else if (h->fused_plane) {
       PS_CUDA(h, launch_plane<T>(pw, np, nx, ny, nz, B.tw_y, B.tw_zh, B.tw_z, variant, h->st));
       ++*nlaunch;
       if (nxw > 0) {
@@ -476,6 +484,8 @@ static int autotune_t(ps_handle* h) {
   float best = 1e30f;
   int best_v = 0;
   for (int v = 0; v < VARIANT_COUNT; ++v) {
+    h->tune_ms[v] = -1.f;
+    if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
     long long nl = 0;
     int rc = launch_sweeps<T>(h, &nl, v);
     if (!rc) {
@@ -777,6 +787,7 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   PS_CUDA(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   const int pb = (h->prec == PS_PREC_MIXED) ? 4 : 8;
   h->fused_plane = plane_fused_supported(pb, c.n[1], c.n[2]);
+  h->xy_ok = xy_supported(pb, c.n[0], c.n[1], c.n[2]);
   const size_t nfN = (size_t)h->nf * h->N;
   PS_CUDA(h, cudaMalloc((void**)&h->d_w, sizeof(double) * nfN));
   PS_CUDA(h, cudaMalloc((void**)&h->d_phi, sizeof(double) * nfN));
@@ -1076,6 +1087,10 @@ void* ps_gpu_stream(const ps_handle* h) { return h ? (void*)h->st : nullptr; }
 
 int ps_gpu_set_variant(ps_handle* h, int variant) {
   if (!h || variant < -1 || variant >= VARIANT_COUNT) return PS_ATTRIB_ERR;
+  if (variant >= 0 && (variant & VARIANT_XY) && !h->xy_ok) {
+    h->err = "the row + x-y plane design does not exist for this grid";
+    return PS_ATTRIB_ERR;
+  }
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }

@@ -42,7 +42,24 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // the forward-z first pass as one shared-memory round trip; bit 1: the pencil
 // pass does the same with its forward last pass, the k2 multiply and the
 // inverse first pass.
-enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_COUNT = 4 };
+// bit 2: the sweeps use the row + x-y plane design (transposed half spectrum
+// S[kz][x][y]) instead of the y-z plane + x pencil design.
+enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_XY = 4, VARIANT_COUNT = 8 };
+
+// The x-y plane design exists for this grid (square x-y planes that fit in
+// shared memory).
+bool xy_supported(int prec_bytes, int nx, int ny, int nz);
+
+// Row (z only) pass that stores the half spectrum transposed, S[kz][x][y].
+template <typename T>
+cudaError_t launch_rows_t(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,
+                          const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st);
+
+// x-y plane pass (one CTA per kz plane of S[kz][x][y]): FFT y, FFT x, k2,
+// IFFT x, IFFT y.  tw has length nx (= ny).
+template <typename T>
+cudaError_t launch_xy(const PencilWork<T>* d_works, int nworks, int nx, int nzh,
+                      const c2_t<T>* tw, int variant, cudaStream_t st);
 
 template <typename T>
 cudaError_t launch_plane(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,

@@ -224,11 +224,13 @@ template <typename T, int TH> struct PlaneMinBlocks {
   static constexpr int v = (sizeof(T) == 4 && TH == 512) ? 2 : 1;
 };
 
-template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ>
+// LT (row mode only): the half spectrum is stored transposed, S[kz][x][y], for
+// the x-y plane pass; a tile is ROWS consecutive y of one x (ROWS divides ny).
+template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ, bool LT>
 __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     plane_kernel(const PlaneWork<T>* __restrict__ works, int nrows_total,
                  const c2_t<T>* __restrict__ tw_y, const c2_t<T>* __restrict__ tw_zh,
-                 const c2_t<T>* __restrict__ tw_z) {
+                 const c2_t<T>* __restrict__ tw_z, int lt_nx, int lt_ny) {
   using C = c2_t<T>;
   constexpr int NZH = NZ / 2 + 1;
   constexpr int H = (NZ > 1) ? NZ / 2 : 1;
@@ -280,9 +282,23 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
         return;
       }
     } else {
-      for (int i = tid; i < SPEC; i += TH) {
-        const int r = i / NZH;
-        buf[i] = (r < rows) ? w.spec[soff + i] : C{T(0), T(0)};
+      if constexpr (LT) {
+        // element (row yy, kz) sits at S[kz][x][y0 + yy]: consecutive threads
+        // take consecutive y, so every kz reads one contiguous segment
+        const int x = row0 / lt_ny;
+        const int y0 = row0 - x * lt_ny;
+        for (int i = tid; i < SPEC; i += TH) {
+          const int kz = i / ROWS;
+          const int yy = i - kz * ROWS;
+          buf[yy * NZH + kz] = (yy < rows)
+                                   ? w.spec[((size_t)kz * lt_nx + x) * lt_ny + y0 + yy]
+                                   : C{T(0), T(0)};
+        }
+      } else {
+        for (int i = tid; i < SPEC; i += TH) {
+          const int r = i / NZH;
+          buf[i] = (r < rows) ? w.spec[soff + i] : C{T(0), T(0)};
+        }
       }
     }
     __syncthreads();
@@ -334,8 +350,18 @@ forward_y:
       bulk_wait_read_all();
     }
   } else {
-    for (int i = tid; i < SPEC; i += TH) {
-      if (i / NZH < rows) w.spec[soff + i] = buf[i];
+    if constexpr (LT) {
+      const int x = row0 / lt_ny;
+      const int y0 = row0 - x * lt_ny;
+      for (int i = tid; i < SPEC; i += TH) {
+        const int kz = i / ROWS;
+        const int yy = i - kz * ROWS;
+        if (yy < rows) w.spec[((size_t)kz * lt_nx + x) * lt_ny + y0 + yy] = buf[yy * NZH + kz];
+      }
+    } else {
+      for (int i = tid; i < SPEC; i += TH) {
+        if (i / NZH < rows) w.spec[soff + i] = buf[i];
+      }
     }
   }
 }
@@ -509,21 +535,22 @@ bool extent_supported(int n) {
   return false;
 }
 
-template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ>
+template <typename T, int ROWS, int NZ, int TH, bool DO_Y, bool FZ, bool LT = false>
 static cudaError_t launch_plane_t(const PlaneWork<T>* d_works, int nworks, int ntiles,
                                   int nrows_total, const c2_t<T>* tw_y, const c2_t<T>* tw_zh,
-                                  const c2_t<T>* tw_z, cudaStream_t st) {
+                                  const c2_t<T>* tw_z, cudaStream_t st, int lt_nx = 0,
+                                  int lt_ny = 0) {
   using C = c2_t<T>;
   constexpr int NZH = NZ / 2 + 1;
   constexpr int H = (NZ > 1) ? NZ / 2 : 1;
   const size_t smem =
       sizeof(C) * ((size_t)ROWS * NZH + H + NZ + (DO_Y ? ROWS : 0)) + sizeof(uint64_t);
-  auto kern = plane_kernel<T, ROWS, NZ, TH, DO_Y, FZ>;
+  auto kern = plane_kernel<T, ROWS, NZ, TH, DO_Y, FZ, LT>;
   static unsigned attr_mask = 0;
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
   if (ea != cudaSuccess) return ea;
   dim3 grid(ntiles, nworks);
-  kern<<<grid, TH, smem, st>>>(d_works, nrows_total, tw_y, tw_zh, tw_z);
+  kern<<<grid, TH, smem, st>>>(d_works, nrows_total, tw_y, tw_zh, tw_z, lt_nx, lt_ny);
   return cudaGetLastError();
 }
 
@@ -588,6 +615,176 @@ cudaError_t launch_rows_impl(const PlaneWork<T>* d_works, int nworks, int nrows,
   PSB_ROW_CASE(T, 96, 16, 256)
   PSB_ROW_CASE(T, 128, 16, 256)
   PSB_ROW_CASE(T, 256, 8, 256)
+  return cudaErrorInvalidValue;
+}
+
+// Row pass writing the transposed spectrum S[kz][x][y] (tiles of ROWS y of one x).
+#define PSB_ROWT_CASE(T, NZ, ROWS, TH)                                                      \
+  if (nz == NZ && ny % ROWS == 0)                                                           \
+    return launch_plane_t<T, ROWS, NZ, TH, false, false, true>(                             \
+        d_works, nworks, nx * ny / ROWS, nx * ny, nullptr, tw_zh, tw_z, st, nx, ny);
+
+template <typename T>
+cudaError_t launch_rows_t_impl(const PlaneWork<T>* d_works, int nworks, int nx, int ny, int nz,
+                               const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st) {
+  PSB_ROWT_CASE(T, 8, 8, 64)
+  PSB_ROWT_CASE(T, 12, 12, 64)
+  PSB_ROWT_CASE(T, 16, 16, 128)
+  PSB_ROWT_CASE(T, 24, 24, 128)
+  PSB_ROWT_CASE(T, 32, 32, 256)
+  PSB_ROWT_CASE(T, 48, 16, 256)
+  PSB_ROWT_CASE(T, 64, 32, 256)
+  PSB_ROWT_CASE(T, 96, 32, 256)
+  PSB_ROWT_CASE(T, 128, 32, 256)
+  PSB_ROWT_CASE(T, 256, 32, 256)
+  return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// x-y plane pass over the transposed spectrum: one CTA per kz plane, held in
+// shared memory with rows padded to NXY + 1 (odd stride: conflict-free along
+// both axes).  Forward y FFT, forward x FFT, k2 multiply, inverse x FFT,
+// inverse y FFT.
+// ---------------------------------------------------------------------------
+template <typename T, int NXY, int R>
+struct XYKOp {
+  using T2 = c2_t<T>;
+  static constexpr int M = NXY / R;
+  const T* kx;
+  const T* kyz;
+  int kz;
+  int nzh;
+  T fyz;
+  __device__ __forceinline__ void prefetch(int y, int j) { fyz = __ldg(kyz + (size_t)y * nzh + kz); }
+  __device__ __forceinline__ void apply(int y, int j, T2 (&v)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const T f = __ldg(kx + j + r * M) * fyz;
+      v[r] = T2{v[r].x * f, v[r].y * f};
+    }
+  }
+};
+
+template <typename T, int NXY, int TH, bool FK>
+__global__ void __launch_bounds__(TH)
+    xy_kernel(const PencilWork<T>* __restrict__ works, int nzh, const c2_t<T>* __restrict__ tw) {
+  using C = c2_t<T>;
+  using V = typename Vec16<T>::type;
+  constexpr int NP = NXY + 1;
+  constexpr int NE = NXY * NXY;
+  constexpr int CPV = 16 / sizeof(C);
+  constexpr int NV = NE / CPV;
+  constexpr int UV = (NV + TH - 1) / TH;
+  using RL = typename WidePlan<NXY>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* s_tw = buf + NXY * NP;
+  const PencilWork<T> w = works[blockIdx.y];
+  const int kz = blockIdx.x;
+  const int tid = threadIdx.x;
+  C* base = w.spec + (size_t)kz * NE;
+  {
+    V v[UV];
+#pragma unroll
+    for (int u = 0; u < UV; ++u) {
+      const int e = tid + u * TH;
+      if (NV % TH == 0 || e < NV) v[u] = reinterpret_cast<const V*>(base)[e];
+    }
+    for (int i = tid; i < NXY; i += TH) s_tw[i] = tw[i];
+#pragma unroll
+    for (int u = 0; u < UV; ++u) {
+      const int e = tid + u * TH;
+      if (NV % TH == 0 || e < NV) {
+#pragma unroll
+        for (int c = 0; c < CPV; ++c) {
+          const int idx = e * CPV + c;
+          const int x = idx / NXY;
+          buf[x * NP + (idx - x * NXY)] = reinterpret_cast<const C*>(&v[u])[c];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  smem_fft<NXY, NXY, TH, false, true, C, RL>(buf, NP, 1, s_tw);  // y, rows x
+  if constexpr (FK && NXY > 1) {
+    using RI = typename RLReverse<RL>::type;
+    constexpr int RF = RLLast<RL>::value;
+    smem_fft_head<NXY, RL, NXY, TH, false, true>(buf, 1, NP, s_tw);  // x, columns y
+    XYKOp<T, NXY, RF> op;
+    op.kx = w.kx;
+    op.kyz = w.kyz;
+    op.kz = kz;
+    op.nzh = nzh;
+    fused_pass_pair<NXY, RF, NXY, TH, false, true, true>(buf, 1, NP, s_tw, op);
+    smem_fft_tail<NXY, RI, NXY, TH, true, true>(buf, 1, NP, s_tw);
+  } else {
+    smem_fft<NXY, NXY, TH, false, true, C, RL>(buf, 1, NP, s_tw);
+    for (int e = tid; e < NE; e += TH) {
+      const int x = e / NXY;
+      const int y = e - x * NXY;
+      const T f = __ldg(w.kx + x) * __ldg(w.kyz + (size_t)y * nzh + kz);
+      const C v = buf[x * NP + y];
+      buf[x * NP + y] = C{v.x * f, v.y * f};
+    }
+    __syncthreads();
+    smem_fft<NXY, NXY, TH, true, true, C, RL>(buf, 1, NP, s_tw);
+  }
+  smem_fft<NXY, NXY, TH, true, true, C, RL>(buf, NP, 1, s_tw);  // inverse y
+#pragma unroll
+  for (int u = 0; u < UV; ++u) {
+    const int e = tid + u * TH;
+    if (NV % TH == 0 || e < NV) {
+      V v;
+#pragma unroll
+      for (int c = 0; c < CPV; ++c) {
+        const int idx = e * CPV + c;
+        const int x = idx / NXY;
+        reinterpret_cast<C*>(&v)[c] = buf[x * NP + (idx - x * NXY)];
+      }
+      reinterpret_cast<V*>(base)[e] = v;
+    }
+  }
+}
+
+template <typename T, int NXY, int TH, bool FK>
+static cudaError_t launch_xy_t(const PencilWork<T>* d_works, int nworks, int nzh,
+                               const c2_t<T>* tw, cudaStream_t st) {
+  using C = c2_t<T>;
+  const size_t smem = sizeof(C) * ((size_t)NXY * (NXY + 1) + NXY);
+  auto kern = xy_kernel<T, NXY, TH, FK>;
+  static unsigned attr_mask = 0;
+  cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
+  if (ea != cudaSuccess) return ea;
+  dim3 grid(nzh, nworks);
+  kern<<<grid, TH, smem, st>>>(d_works, nzh, tw);
+  return cudaGetLastError();
+}
+
+static const int kXYShapes[] = {8, 16, 32, 64, 96, 128};
+
+bool xy_supported(int prec_bytes, int nx, int ny, int nz) {
+  if (nx != ny || nz < 4 || !extent_supported(nz)) return false;
+  bool listed = false;
+  for (int s : kXYShapes) listed |= (s == nx);
+  if (!listed) return false;
+  const size_t bytes = (size_t)2 * prec_bytes * ((size_t)nx * (nx + 1) + nx);
+  return bytes <= 200 * 1024;
+}
+
+#define PSB_XY_CASE(T, NXY, TH)                                                             \
+  if (nx == NXY)                                                                            \
+    return (variant & 2) ? launch_xy_t<T, NXY, TH, true>(d_works, nworks, nzh, tw, st)      \
+                         : launch_xy_t<T, NXY, TH, false>(d_works, nworks, nzh, tw, st);
+
+template <typename T>
+cudaError_t launch_xy_impl(const PencilWork<T>* d_works, int nworks, int nx, int nzh,
+                           const c2_t<T>* tw, int variant, cudaStream_t st) {
+  PSB_XY_CASE(T, 8, 64)
+  PSB_XY_CASE(T, 16, 128)
+  PSB_XY_CASE(T, 32, 256)
+  PSB_XY_CASE(T, 64, 512)
+  PSB_XY_CASE(T, 96, 512)
+  PSB_XY_CASE(T, 128, 1024)
   return cudaErrorInvalidValue;
 }
 
@@ -677,6 +874,26 @@ template <>
 cudaError_t launch_rows<double>(const PlaneWork<double>* w, int nw, int nrows, int nz,
                                 const double2* tzh, const double2* tz, cudaStream_t st) {
   return launch_rows_impl<double>(w, nw, nrows, nz, tzh, tz, st);
+}
+template <>
+cudaError_t launch_rows_t<float>(const PlaneWork<float>* w, int nw, int nx, int ny, int nz,
+                                 const float2* tzh, const float2* tz, cudaStream_t st) {
+  return launch_rows_t_impl<float>(w, nw, nx, ny, nz, tzh, tz, st);
+}
+template <>
+cudaError_t launch_rows_t<double>(const PlaneWork<double>* w, int nw, int nx, int ny, int nz,
+                                  const double2* tzh, const double2* tz, cudaStream_t st) {
+  return launch_rows_t_impl<double>(w, nw, nx, ny, nz, tzh, tz, st);
+}
+template <>
+cudaError_t launch_xy<float>(const PencilWork<float>* w, int nw, int nx, int nzh, const float2* tw,
+                             int variant, cudaStream_t st) {
+  return launch_xy_impl<float>(w, nw, nx, nzh, tw, variant, st);
+}
+template <>
+cudaError_t launch_xy<double>(const PencilWork<double>* w, int nw, int nx, int nzh,
+                              const double2* tw, int variant, cudaStream_t st) {
+  return launch_xy_impl<double>(w, nw, nx, nzh, tw, variant, st);
 }
 template <>
 cudaError_t launch_pencil<float>(const PencilWork<float>* w, int nw, int mode, int L, int outer,

@@ -22,6 +22,7 @@ def main() -> None:
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--anderson", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1, help="kernel variant (-1: autotune)")
     a = ap.parse_args()
     upd = (Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=10,
                    anderson_mix=0.5, anderson_start=0) if a.anderson
@@ -30,6 +31,8 @@ def main() -> None:
     s = W.hex_seed(cfg)
     w = W.random_fields(cfg, 0.05)
     g = ScftSolver(cfg)
+    if a.variant >= 0:
+        g.set_variant(a.variant)
     g.restore([w[0] + s, w[1] - s])
     g.update(a.iters)
     sc = g.scalars()

@@ -72,7 +72,7 @@ def test_fp64_diblock_parity(gpu, oracle_lib, n):
     assert g.launches_per_iteration > 0
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", list(range(8)))
 @pytest.mark.parametrize("n", [16, 32])
 def test_every_kernel_variant_matches_oracle(gpu, oracle_lib, variant, n):
     cfg, w = W.diblock32(n=n)
@@ -96,8 +96,30 @@ def test_autotune_picks_a_measured_variant(gpu):
     g.restore(w)
     g.update(3)
     v, ms = g.variant()
-    assert 0 <= v < 4 and all(t > 0 for t in ms)
-    assert ms[v] == min(ms)
+    timed = [t for t in ms if t > 0]
+    assert 0 <= v < 8 and len(timed) >= 4
+    assert ms[v] == min(timed)
+
+
+def test_xy_design_mixed_and_blend(gpu, oracle_lib):
+    """The row + x-y plane design on a blend (3 sweeps, one aliased) in both precisions."""
+    for prec, tol in (("fp64", TOL64), ("mixed", None)):
+        cfg = W.blend(16, 18.0, 0.35, 0.15, precision=prec, seed=12, anderson=False)
+        w = W.random_fields(cfg, 0.3)
+        g = ScftSolver(cfg)
+        g.set_variant(6)
+        g.restore(w)
+        o = O.Oracle(cfg)
+        o.restore(w)
+        ho = o.update(5)
+        hg = []
+        for _ in range(5):
+            g.update(1)
+            hg.append(g.scalars())
+        if tol:
+            assert_parity(cfg, g, o, hg, ho)
+        else:
+            assert abs(hg[-1]["free_energy"] - ho[-1]["free_energy"]) < 1e-5
 
 
 def test_fp64_propagator_slices(gpu, oracle_lib):
@@ -291,8 +313,13 @@ def test_kat_q_independent_of_s_gpu(gpu):
 
 
 def test_graph_replay_is_deterministic(gpu):
+    """Same variant, same inputs: bitwise the same results, whether the
+    iterations come from one graph replay loop or one call each.  (Variants
+    differ from each other in rounding, so the autotuned choice is pinned.)"""
     cfg, w = W.diblock32(n=16)
     a, b = ScftSolver(cfg), ScftSolver(cfg)
+    a.set_variant(2)
+    b.set_variant(2)
     a.restore(w)
     b.restore(w)
     a.update(6)
