@@ -205,6 +205,28 @@ int ps_fft_scaled_pair(ps_fft* f, const double* data, const double* kdata, doubl
 /* Message for the last FFT-plugin error of the calling thread. */
 const char* ps_fft_last_error(void);
 
+/* --- scaledFFTPair without any allocation ---------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need the transform: a host whose device memory is all owned by
+ * another allocator (a framework's caching allocator or a pool that reserved
+ * the GPU at start-up), or a solver loop that must not allocate once running.
+ * Same result as ps_fft_scaled_pair, but data, kdata and res are the caller's
+ * DEVICE arrays (n[0]*n[1]*n[2] doubles on the current device; data and res
+ * 16-byte aligned) and the call is asynchronous on `stream` (a cudaStream_t;
+ * NULL is the default stream).  The working storage is one fixed device array
+ * of ps_fft_noalloc_scratch_bytes() bytes (4 MiB) per device, held until the
+ * process exits: grids whose half spectrum nx*ny*(nz/2+1)*16 bytes plus
+ * tables exceed it return PS_INPUT_ERR (64^3 fits, 96^3 does not).  All calls on a device
+ * share that storage, so calls that overlap on the GPU (other streams or
+ * threads) race.  The first call on each device resolves the storage's
+ * address; make it before any stream capture.  Errors: PS_ATTRIB_ERR (null or
+ * misaligned pointer), PS_INPUT_ERR (extent or size), PS_GPU_ERR (CUDA). */
+int ps_fft_scaled_pair_noalloc(const int n[3], const double* data, const double* kdata,
+                               double* res, void* stream);
+size_t ps_fft_noalloc_scratch_bytes(void);
+/* Message for the last error of ps_fft_scaled_pair_noalloc on the calling thread. */
+const char* ps_fft_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

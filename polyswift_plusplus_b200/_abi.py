@@ -113,6 +113,9 @@ SIGNATURES = {
     "ps_fft_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "ps_fft_scaled_pair": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ps_fft_last_error": (C.c_char_p, []),
+    "ps_fft_scaled_pair_noalloc": (C.c_int, [C.POINTER(C.c_int), _vp, _vp, _vp, _vp]),
+    "ps_fft_noalloc_scratch_bytes": (C.c_size_t, []),
+    "ps_fft_noalloc_last_error": (C.c_char_p, []),
 }
 
 _lib = None
