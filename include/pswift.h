@@ -194,6 +194,35 @@ int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_t
 int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
                         double* bytes_per_iter, long long* steps_per_iter);
 
+/* --- Batched instances (no reference counterpart: the reference runs one
+ * PsDomain per process, polyswift/polyswift/polyswift.cxx:544-588) ----------
+ * ps_gpu_batch_create builds `count` independent instances on one device
+ * (each exactly as ps_gpu_create would, noise must be 0) and groups them into
+ * size classes of equal grid and precision.  ps_gpu_batch_iterate runs n_iter
+ * iterations of every instance: each class's propagator sweeps are merged into
+ * one launch per contour step, the per-instance field updates run as parallel
+ * branches, and the whole iteration is one captured CUDA graph after the
+ * first.  Each instance's result equals ps_gpu_iterate on it alone with the
+ * same kernel variant.  ps_gpu_batch_instance returns the instance's handle
+ * for ps_gpu_set_fields / get_fields / get_scalars / get_propagator (owned by
+ * the batch: do not destroy it; do not iterate it while the batch runs).
+ * ps_gpu_batch_set_variant forces one kernel variant for every class (-1:
+ * autotune each class on its merged sweeps). */
+typedef struct ps_batch ps_batch;
+int ps_gpu_batch_create(const ps_config* cfgs, int count, ps_batch** out);
+int ps_gpu_batch_destroy(ps_batch* b);
+int ps_gpu_batch_size(const ps_batch* b);
+ps_handle* ps_gpu_batch_instance(ps_batch* b, int index);
+int ps_gpu_batch_iterate(ps_batch* b, int n_iter);
+int ps_gpu_batch_set_variant(ps_batch* b, int variant);
+/* Size classes: class_of[i] for each instance, variants[c] for each class. */
+int ps_gpu_batch_classes(const ps_batch* b, int* n_classes, int* class_of, int max_inst,
+                         int* variants, int max_classes);
+long long ps_gpu_batch_launches_per_iteration(const ps_batch* b);
+void* ps_gpu_batch_stream(const ps_batch* b);
+/* Message for the last error of a batch (or of the calling thread when b is NULL). */
+const char* ps_gpu_batch_last_error(const ps_batch* b);
+
 /* --- FFT plugin: PsFFTBase<T,3>::scaledFFTPair with host pointers ---------
  * res = Re(IFFT(kdata * FFT(data))), both transforms unnormalised, as the
  * reference's FFTW c2c pair.  Inputs and outputs are host arrays of n[0]*n[1]*n[2]

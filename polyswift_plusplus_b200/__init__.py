@@ -7,7 +7,7 @@ C-ABI of ``include/pswift.h``; this package is the Python side of that ABI.
 from . import _abi
 from .config import (Block, Interaction, Polymer, ScftConfig, Updater, config_from_file,
                      config_from_text)
-from .scft import B200FFT, ScftSolver
+from .scft import B200FFT, ScftBatch, ScftSolver
 
 __all__ = ["Block", "Interaction", "Polymer", "ScftConfig", "Updater", "config_from_file",
-           "config_from_text", "ScftSolver", "B200FFT", "_abi"]
+           "config_from_text", "ScftSolver", "ScftBatch", "B200FFT", "_abi"]

@@ -108,6 +108,17 @@ SIGNATURES = {
     "ps_gpu_get_variant": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]),
     "ps_gpu_sweep_timing": (C.c_int, [_vp, _dbl_p, C.c_int, C.POINTER(C.c_int), _dbl_p,
                                       C.POINTER(C.c_longlong)]),
+    "ps_gpu_batch_create": (C.c_int, [C.POINTER(ps_config), C.c_int, C.POINTER(_vp)]),
+    "ps_gpu_batch_destroy": (C.c_int, [_vp]),
+    "ps_gpu_batch_size": (C.c_int, [_vp]),
+    "ps_gpu_batch_instance": (_vp, [_vp, C.c_int]),
+    "ps_gpu_batch_iterate": (C.c_int, [_vp, C.c_int]),
+    "ps_gpu_batch_set_variant": (C.c_int, [_vp, C.c_int]),
+    "ps_gpu_batch_classes": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
+                                       C.POINTER(C.c_int), C.c_int]),
+    "ps_gpu_batch_launches_per_iteration": (C.c_longlong, [_vp]),
+    "ps_gpu_batch_stream": (_vp, [_vp]),
+    "ps_gpu_batch_last_error": (C.c_char_p, [_vp]),
     "ps_fft_create": (C.c_int, [C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(_vp)]),
     "ps_fft_destroy": (C.c_int, [_vp]),
     "ps_fft_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
@@ -147,12 +158,14 @@ def load_library(path: Path | None = None) -> C.CDLL:
     return lib
 
 
-def check(rc: int, handle=None, fft: bool = False) -> None:
+def check(rc: int, handle=None, fft: bool = False, batch=None) -> None:
     if rc == PS_OK:
         return
     lib = load_library()
     if fft:
         msg = lib.ps_fft_last_error()
+    elif batch is not None:
+        msg = lib.ps_gpu_batch_last_error(batch)
     else:
         msg = lib.ps_gpu_last_error(handle)
     raise PsError(rc, (msg or b"").decode(errors="replace"))

@@ -18,134 +18,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/pswift.h"
-#include "field_kernels.cuh"
-#include "kernels.h"
-#include "mt19937.h"
+#include "engine_state.h"
 
 namespace psb {
 
 static thread_local std::string g_thread_err;
-
-enum { HEAD = 0, TAIL = 1 };
-
-struct Seg {
-  int block;
-  int from;   // HEAD: this sweep produces the block's qs; TAIL: its qts
-  int off;    // slice offset of the segment inside the sweep
-  int steps;
-  int wfac_id;
-  int ktab_id;
-};
-
-struct Sweep {
-  int polymer;
-  std::vector<Seg> segs;
-  int total = 0;
-  int storage = -1;  // index of the executed sweep holding its slices
-};
-
-struct BlockMap {
-  int steps;
-  int field;
-  double ds, bseg;
-  int sweep_head, off_head;  // qs[n]  = slices(sweep_head)[off_head + n]
-  int sweep_tail, off_tail;  // qts[n] = slices(sweep_tail)[off_tail + n]
-};
-
-template <typename T> struct Buffers {
-  std::vector<T*> slices;        // per executed sweep: (total+1)*N
-  std::vector<c2_t<T>*> spec;    // per executed sweep
-  std::vector<T*> wfac;          // per (field, ds) key
-  std::vector<T*> kx, kyz;       // per (ds, bseg) key
-  c2_t<T>* tw_x = nullptr;
-  c2_t<T>* tw_y = nullptr;
-  c2_t<T>* tw_z = nullptr;
-  c2_t<T>* tw_zh = nullptr;
-  PlaneWork<T>* d_plane = nullptr;
-  PencilWork<T>* d_pencil = nullptr;
-};
-
-}  // namespace psb
-
-struct ps_handle {
-  ps_config cfg;
-  int n[3];
-  long long N = 0;
-  int nzh = 0;
-  int nf = 0;
-  int prec = PS_PREC_FP64;
-  int dev = 0;
-  bool fused_plane = true;
-  cudaStream_t st = nullptr;
-  std::string err;
-
-  double* d_w = nullptr;    // nf*N
-  double* d_phi = nullptr;  // nf*N
-  double* d_p = nullptr;
-  double* d_noise = nullptr;
-  double* h_noise = nullptr;  // pinned
-
-  std::vector<std::vector<psb::BlockMap>> blocks;
-  std::vector<double> alpha;  // length ratios
-  std::vector<psb::Sweep> sweeps;
-  std::vector<int> exec;  // sweep indices that are executed (own storage)
-  std::vector<std::pair<int, double>> wfac_keys;
-  std::vector<std::pair<double, double>> ktab_keys;
-  int kmax = 0;
-  std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
-
-  psb::Buffers<float> bf;
-  psb::Buffers<double> bd;
-
-  double* d_qpart = nullptr;
-  double* d_upart = nullptr;
-  psb::DevScalars* d_sc = nullptr;
-  psb::DevScalars* h_sc = nullptr;  // pinned
-  psb::FieldModel fm;
-
-  // Anderson history
-  int am_slots = 0;
-  double* d_hw = nullptr;
-  double* d_hd = nullptr;
-  double* d_gram = nullptr;
-  double* d_gpart = nullptr;
-
-  // graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  int eager_iters = 0;
-  long long launches_per_iter = 0;
-  int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
-  float tune_ms[psb::VARIANT_COUNT] = {};
-  bool xy_ok = false;  // the row + x-y plane design exists for this grid
-
-  psb::Mt19937 rng;
-  long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
-  long long iterations = 0;
-
-  // Sweep timing: CUDA events around the propagator sweeps of each iteration.
-  int timing_cap = 0;
-  int timing_count = 0;
-  cudaEvent_t ev_cap_start = nullptr, ev_cap_end = nullptr;  // recorded during capture
-  std::vector<cudaEvent_t> ev_start, ev_end;                 // one pair per sample
-  cudaGraphNode_t node_start = nullptr, node_end = nullptr;  // event-record nodes in the graph
-  bool graph_has_timing = false;
-  std::vector<float> eager_ms;  // samples taken on eager iterations
-  double sweep_bytes = 0.0;  // algorithmic bytes of the sweeps of one iteration
-  long long sweep_steps = 0; // propagator steps (all sweeps) of one iteration
-};
-
-namespace psb {
-
-#define PS_CUDA(h, call)                                                               \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess) {                                                           \
-      (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
-      return PS_GPU_ERR;                                                               \
-    }                                                                                  \
-  } while (0)
 
 // PsBlockBase::setBlockSteps (psbase/PsBlockBase.cpp:252-326).
 static int set_block_steps(double bs, int force, int* out, std::string& err) {
@@ -229,10 +106,6 @@ static bool chain_sweeps(const ps_polymer_config& P, std::vector<std::pair<int, 
     if (!seen[i]) return false;
   return true;
 }
-
-template <typename T> Buffers<T>& bufs(ps_handle* h);
-template <> Buffers<float>& bufs<float>(ps_handle* h) { return h->bf; }
-template <> Buffers<double>& bufs<double>(ps_handle* h) { return h->bd; }
 
 template <typename T>
 static int alloc_copy(ps_handle* h, T** dst, const std::vector<T>& src) {
@@ -354,59 +227,20 @@ static int build_device_tables(ps_handle* h) {
   }
   rc = alloc_copy(h, &B.d_plane, pw);
   if (!rc) rc = alloc_copy(h, &B.d_pencil, xw);
+  B.h_plane = pw;
+  B.h_pencil = xw;
   return rc;
 }
 
 // Launch the propagator sweeps of one iteration.
 template <typename T>
 static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
-  Buffers<T>& B = bufs<T>(h);
-  const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
-  for (int k = 0; k <= h->kmax; ++k) {
-    const PlaneWork<T>* pw = B.d_plane + h->plane_off[k];
-    const int np = h->plane_cnt[k];
-    const PencilWork<T>* xw = B.d_pencil + h->pencil_off[k];
-    const int nxw = h->pencil_cnt[k];
-    if ((variant & VARIANT_XY) && h->xy_ok) {
-      PS_CUDA(h, launch_rows_t<T>(pw, np, nx, ny, nz, B.tw_zh, B.tw_z, h->st));
-      ++*nlaunch;
-      if (nxw > 0) {
-        PS_CUDA(h, launch_xy<T>(xw, nxw, nx, h->nzh, B.tw_x, variant, h->st));
-        ++*nlaunch;
-      }
-    } else if (h->fused_plane) {
-      PS_CUDA(h, launch_plane<T>(pw, np, nx, ny, nz, B.tw_y, B.tw_zh, B.tw_z, variant, h->st));
-      ++*nlaunch;
-      if (nxw > 0) {
-        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz,
-                                    variant, h->st));
-        ++*nlaunch;
-      }
-    } else {
-      PS_CUDA(h, launch_rows<T>(pw, np, nx * ny, nz, B.tw_zh, B.tw_z, h->st));
-      ++*nlaunch;
-      if (nxw > 0) {
-        if (ny > 1) {
-          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_FWD, ny, nx, h->nzh, B.tw_y, nx, ny, nz, variant,
-                                      h->st));
-          ++*nlaunch;
-        }
-        PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * h->nzh, B.tw_x, nx, ny, nz,
-                                    variant, h->st));
-        ++*nlaunch;
-        if (ny > 1) {
-          PS_CUDA(h, launch_pencil<T>(xw, nxw, PENCIL_INV, ny, nx, h->nzh, B.tw_y, nx, ny, nz, variant,
-                                      h->st));
-          ++*nlaunch;
-        }
-      }
-    }
-  }
+  PS_CUDA(h, launch_sweep_set<T>(handle_sweep_set<T>(h), variant, h->st, nlaunch));
   return PS_OK;
 }
 
 template <typename T>
-static int launch_iteration(ps_handle* h, long long* nlaunch) {
+static int launch_pre(ps_handle* h, long long* nlaunch) {
   Buffers<T>& B = bufs<T>(h);
   const long long N = h->N;
   PS_CUDA(h, launch_zero(h->d_phi, (long long)h->nf * N, h->st));
@@ -417,14 +251,30 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
     PS_CUDA(h, launch_wfac<T>(h->d_w + (size_t)f * N, B.wfac[i], -0.5 * ds, N, h->st));
     ++*nlaunch;
   }
+  return PS_OK;
+}
+
+template <typename T> static int launch_post(ps_handle* h, long long* nlaunch);
+
+template <typename T>
+static int launch_iteration(ps_handle* h, long long* nlaunch) {
+  int rc = launch_pre<T>(h, nlaunch);
+  if (rc) return rc;
   // cudaEventRecordExternal: inside stream capture this becomes an event-record
   // node of the graph (a plain record would only order the capture).
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_start, h->st, cudaEventRecordExternal));
-  int rc = launch_sweeps<T>(h, nlaunch, h->variant < 0 ? 0 : h->variant);
+  rc = launch_sweeps<T>(h, nlaunch, h->variant < 0 ? 0 : h->variant);
   if (rc) return rc;
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_end, h->st, cudaEventRecordExternal));
+  return launch_post<T>(h, nlaunch);
+}
+
+template <typename T>
+static int launch_post(ps_handle* h, long long* nlaunch) {
+  Buffers<T>& B = bufs<T>(h);
+  const long long N = h->N;
   auto slice = [&](int sweep, int idx) -> const T* {
     return B.slices[h->sweeps[sweep].storage] + (size_t)idx * N;
   };
@@ -478,38 +328,9 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
 // warm-up and one timed sweep each) and keep the fastest.
 template <typename T>
 static int autotune_t(ps_handle* h) {
-  cudaEvent_t a, b;
-  PS_CUDA(h, cudaEventCreate(&a));
-  PS_CUDA(h, cudaEventCreate(&b));
-  float best = 1e30f;
-  int best_v = 0;
-  for (int v = 0; v < VARIANT_COUNT; ++v) {
-    h->tune_ms[v] = -1.f;
-    if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
-    long long nl = 0;
-    int rc = launch_sweeps<T>(h, &nl, v);
-    if (!rc) {
-      PS_CUDA(h, cudaEventRecord(a, h->st));
-      rc = launch_sweeps<T>(h, &nl, v);
-      PS_CUDA(h, cudaEventRecord(b, h->st));
-    }
-    if (rc) {
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
-      return rc;
-    }
-    PS_CUDA(h, cudaEventSynchronize(b));
-    float ms = 0.f;
-    PS_CUDA(h, cudaEventElapsedTime(&ms, a, b));
-    h->tune_ms[v] = ms;
-    if (ms < best) {
-      best = ms;
-      best_v = v;
-    }
-  }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  h->variant = best_v;
+  int best = 0;
+  PS_CUDA(h, autotune_sweep_set<T>(handle_sweep_set<T>(h), h->st, h->tune_ms, &best));
+  h->variant = best;
   return PS_OK;
 }
 
@@ -522,6 +343,14 @@ static int run_iteration(ps_handle* h, long long* nlaunch) {
                                     : launch_iteration<double>(h, nlaunch);
 }
 
+int engine_pre(ps_handle* h, long long* nlaunch) {
+  return (h->prec == PS_PREC_MIXED) ? launch_pre<float>(h, nlaunch) : launch_pre<double>(h, nlaunch);
+}
+
+int engine_post(ps_handle* h, long long* nlaunch) {
+  return (h->prec == PS_PREC_MIXED) ? launch_post<float>(h, nlaunch) : launch_post<double>(h, nlaunch);
+}
+
 // Gaussian draws the reference makes every iteration even at noise = 0
 // (pseffhamil/PsPolymerUpdater.cpp:263-295); they are owed to the stream and
 // drawn lazily before anything else reads it.
@@ -532,7 +361,7 @@ static void settle_rng(ps_handle* h) {
   }
 }
 
-static int prepare_noise(ps_handle* h) {
+int engine_prepare_noise(ps_handle* h) {
   const double s = h->cfg.updater.noise;
   if (s == 0.0) {
     h->pending_gauss += (long long)h->nf * h->N;
@@ -825,7 +654,7 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   return PS_OK;
 }
 
-static int check_scalars(ps_handle* h) {
+int engine_check_scalars(ps_handle* h) {
   PS_CUDA(h, cudaMemcpyAsync(h->h_sc, h->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   if (h->h_sc->error_flags & 1) {
@@ -847,7 +676,7 @@ static int iterate_impl(ps_handle* h, int n) {
   PS_CUDA(h, cudaSetDevice(h->dev));
   const bool use_graph = (h->cfg.updater.noise == 0.0);
   for (int it = 0; it < n; ++it) {
-    int rc = prepare_noise(h);
+    int rc = engine_prepare_noise(h);
     if (rc) return rc;
     const bool sample = h->timing_cap > 0 && h->timing_count < h->timing_cap;
     if (!use_graph || h->eager_iters < 1) {
@@ -912,7 +741,7 @@ static int iterate_impl(ps_handle* h, int n) {
     }
     h->iterations++;
   }
-  return check_scalars(h);
+  return engine_check_scalars(h);
 }
 
 }  // namespace psb

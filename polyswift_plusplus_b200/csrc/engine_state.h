@@ -1,0 +1,174 @@
+// State of one SCFT instance on the device (ps_handle) and the engine
+// functions that the batch driver (batch.cu) composes into its own graph.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/pswift.h"
+#include "field_kernels.cuh"
+#include "kernels.h"
+#include "mt19937.h"
+#include "sweeps.cuh"
+
+namespace psb {
+
+enum { HEAD = 0, TAIL = 1 };
+
+struct Seg {
+  int block;
+  int from;   // HEAD: this sweep produces the block's qs; TAIL: its qts
+  int off;    // slice offset of the segment inside the sweep
+  int steps;
+  int wfac_id;
+  int ktab_id;
+};
+
+struct Sweep {
+  int polymer;
+  std::vector<Seg> segs;
+  int total = 0;
+  int storage = -1;  // index of the executed sweep holding its slices
+};
+
+struct BlockMap {
+  int steps;
+  int field;
+  double ds, bseg;
+  int sweep_head, off_head;  // qs[n]  = slices(sweep_head)[off_head + n]
+  int sweep_tail, off_tail;  // qts[n] = slices(sweep_tail)[off_tail + n]
+};
+
+template <typename T> struct Buffers {
+  std::vector<T*> slices;        // per executed sweep: (total+1)*N
+  std::vector<c2_t<T>*> spec;    // per executed sweep
+  std::vector<T*> wfac;          // per (field, ds) key
+  std::vector<T*> kx, kyz;       // per (ds, bseg) key
+  c2_t<T>* tw_x = nullptr;
+  c2_t<T>* tw_y = nullptr;
+  c2_t<T>* tw_z = nullptr;
+  c2_t<T>* tw_zh = nullptr;
+  PlaneWork<T>* d_plane = nullptr;
+  PencilWork<T>* d_pencil = nullptr;
+  std::vector<PlaneWork<T>> h_plane;    // host copies of the work tables
+  std::vector<PencilWork<T>> h_pencil;
+};
+
+}  // namespace psb
+
+struct ps_handle {
+  ps_config cfg;
+  int n[3];
+  long long N = 0;
+  int nzh = 0;
+  int nf = 0;
+  int prec = PS_PREC_FP64;
+  int dev = 0;
+  bool fused_plane = true;
+  cudaStream_t st = nullptr;
+  std::string err;
+
+  double* d_w = nullptr;    // nf*N
+  double* d_phi = nullptr;  // nf*N
+  double* d_p = nullptr;
+  double* d_noise = nullptr;
+  double* h_noise = nullptr;  // pinned
+
+  std::vector<std::vector<psb::BlockMap>> blocks;
+  std::vector<double> alpha;  // length ratios
+  std::vector<psb::Sweep> sweeps;
+  std::vector<int> exec;  // sweep indices that are executed (own storage)
+  std::vector<std::pair<int, double>> wfac_keys;
+  std::vector<std::pair<double, double>> ktab_keys;
+  int kmax = 0;
+  std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
+
+  psb::Buffers<float> bf;
+  psb::Buffers<double> bd;
+
+  double* d_qpart = nullptr;
+  double* d_upart = nullptr;
+  psb::DevScalars* d_sc = nullptr;
+  psb::DevScalars* h_sc = nullptr;  // pinned
+  psb::FieldModel fm;
+
+  // Anderson history
+  int am_slots = 0;
+  double* d_hw = nullptr;
+  double* d_hd = nullptr;
+  double* d_gram = nullptr;
+  double* d_gpart = nullptr;
+
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int eager_iters = 0;
+  long long launches_per_iter = 0;
+  int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
+  float tune_ms[psb::VARIANT_COUNT] = {};
+  bool xy_ok = false;  // the row + x-y plane design exists for this grid
+
+  psb::Mt19937 rng;
+  long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
+  long long iterations = 0;
+
+  // Sweep timing: CUDA events around the propagator sweeps of each iteration.
+  int timing_cap = 0;
+  int timing_count = 0;
+  cudaEvent_t ev_cap_start = nullptr, ev_cap_end = nullptr;  // recorded during capture
+  std::vector<cudaEvent_t> ev_start, ev_end;                 // one pair per sample
+  cudaGraphNode_t node_start = nullptr, node_end = nullptr;  // event-record nodes in the graph
+  bool graph_has_timing = false;
+  std::vector<float> eager_ms;  // samples taken on eager iterations
+  double sweep_bytes = 0.0;  // algorithmic bytes of the sweeps of one iteration
+  long long sweep_steps = 0; // propagator steps (all sweeps) of one iteration
+};
+
+namespace psb {
+
+#define PS_CUDA(h, call)                                                               \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+      return PS_GPU_ERR;                                                               \
+    }                                                                                  \
+  } while (0)
+
+// Pieces of one iteration, all on h->st (engine.cu):
+//   engine_pre:  reset phi, Boltzmann factors of every (field, ds);
+//   the sweeps:  handle_sweep_set(h) under launch_sweep_set;
+//   engine_post: Q, contour quadrature into phi, field update, pressure shift.
+int engine_pre(ps_handle* h, long long* nlaunch);
+int engine_post(ps_handle* h, long long* nlaunch);
+// Host-side random-number bookkeeping owed before each iteration.
+int engine_prepare_noise(ps_handle* h);
+// Copy the device scalars back and turn error flags into status codes.
+int engine_check_scalars(ps_handle* h);
+
+template <typename T> Buffers<T>& bufs(ps_handle* h);
+template <> inline Buffers<float>& bufs<float>(ps_handle* h) { return h->bf; }
+template <> inline Buffers<double>& bufs<double>(ps_handle* h) { return h->bd; }
+
+template <typename T> SweepSet<T> handle_sweep_set(ps_handle* h) {
+  Buffers<T>& B = bufs<T>(h);
+  SweepSet<T> s;
+  for (int d = 0; d < 3; ++d) s.n[d] = h->n[d];
+  s.nzh = h->nzh;
+  s.fused_plane = h->fused_plane;
+  s.xy_ok = h->xy_ok;
+  s.kmax = h->kmax;
+  s.tw_x = B.tw_x;
+  s.tw_y = B.tw_y;
+  s.tw_z = B.tw_z;
+  s.tw_zh = B.tw_zh;
+  s.d_plane = B.d_plane;
+  s.d_pencil = B.d_pencil;
+  s.plane_off = h->plane_off.data();
+  s.plane_cnt = h->plane_cnt.data();
+  s.pencil_off = h->pencil_off.data();
+  s.pencil_cnt = h->pencil_cnt.data();
+  return s;
+}
+
+}  // namespace psb

@@ -20,13 +20,17 @@ from .config import ScftConfig
 
 
 class ScftSolver:
-    def __init__(self, cfg: ScftConfig):
+    def __init__(self, cfg: ScftConfig, _handle=None):
         self.cfg = cfg
         self._lib = A.load_library()
-        self._pc = cfg.to_ps_config()
-        h = C.c_void_p()
-        A.check(self._lib.ps_gpu_create(C.byref(self._pc), C.byref(h)), None)
-        self._h = h
+        self._owned = _handle is None
+        if _handle is None:
+            self._pc = cfg.to_ps_config()
+            h = C.c_void_p()
+            A.check(self._lib.ps_gpu_create(C.byref(self._pc), C.byref(h)), None)
+            self._h = h
+        else:
+            self._h = C.c_void_p(_handle)
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
         self.t = 0
@@ -34,7 +38,8 @@ class ScftSolver:
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self._lib.ps_gpu_destroy(self._h)
+            if self._owned:
+                self._lib.ps_gpu_destroy(self._h)
             self._h = None
 
     def __enter__(self):
@@ -160,6 +165,82 @@ class ScftSolver:
         self._check(self._lib.ps_gpu_sweep_timing(self._h, buf, max_out, C.byref(n), C.byref(b),
                                                   C.byref(s)))
         return [buf[i] for i in range(min(n.value, max_out))], b.value, s.value
+
+
+class ScftBatch:
+    """Many independent SCFT instances advanced together (``ps_gpu_batch_*``).
+
+    ``instance(i)`` is a ``ScftSolver`` view of instance i (restore, fields,
+    scalars); ``update(n)`` runs n iterations of every instance in one captured
+    graph per iteration, with each size class's propagator sweeps merged into
+    one launch per contour step.
+    """
+
+    def __init__(self, cfgs):
+        self.cfgs = list(cfgs)
+        self._lib = A.load_library()
+        self._pcs = (A.ps_config * len(self.cfgs))(*[c.to_ps_config() for c in self.cfgs])
+        b = C.c_void_p()
+        A.check(self._lib.ps_gpu_batch_create(self._pcs, len(self.cfgs), C.byref(b)),
+                batch=C.c_void_p())
+        self._b = b
+        self._views = [ScftSolver(c, _handle=self._lib.ps_gpu_batch_instance(b, i))
+                       for i, c in enumerate(self.cfgs)]
+        self.t = 0
+
+    def __len__(self) -> int:
+        return len(self.cfgs)
+
+    def instance(self, i: int) -> ScftSolver:
+        return self._views[i]
+
+    def update(self, n: int = 1) -> None:
+        A.check(self._lib.ps_gpu_batch_iterate(self._b, int(n)), batch=self._b)
+        self.t += n
+        for v in self._views:
+            v.t += n
+
+    def scalars(self) -> list[dict]:
+        return [v.scalars() for v in self._views]
+
+    def set_variant(self, variant: int) -> None:
+        A.check(self._lib.ps_gpu_batch_set_variant(self._b, int(variant)), batch=self._b)
+
+    def classes(self):
+        """(class index of each instance, kernel variant of each class)."""
+        n = C.c_int()
+        k = len(self.cfgs)
+        co = (C.c_int * k)()
+        va = (C.c_int * k)()
+        A.check(self._lib.ps_gpu_batch_classes(self._b, C.byref(n), co, k, va, k), batch=self._b)
+        return [co[i] for i in range(k)], [va[c] for c in range(n.value)]
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(self._lib.ps_gpu_batch_launches_per_iteration(self._b))
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self._lib.ps_gpu_batch_stream(self._b) or 0)
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            for v in self._views:
+                v.close()
+            self._lib.ps_gpu_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class B200FFT:
