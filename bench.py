@@ -11,7 +11,11 @@ Our arm prints one JSON line with the device-timed whole-job rate (`value`),
 the end-to-end rate through the public API with host buffers (`e2e`), the
 roofline of the propagator step (CUDA events around the sweeps inside the
 timed iterations), the CPU baseline (the FP64 oracle on the host cores) and
-the SM clocks sampled during the timed region.
+the SM clocks sampled during the timed region.  At N = 1 it adds the
+mixed-vs-FP64 precision check (1000 iterations of both), the FP64 path's rate
+on the same workload (`fp64_path`, `mixed_over_fp64`) and the batched blend
+workload (64 instances of uneven size as one batch against a loop of
+single-instance launches, `batched`).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -55,6 +59,11 @@ def parse_args():
                     help="iterations of the mixed-vs-FP64 comparison (0 = skip)")
     ap.add_argument("--prep", type=int, default=-1,
                     help="setup iterations before warm-up (default: fill the Anderson history)")
+    ap.add_argument("--fp64-steps", type=int, default=10,
+                    help="timed iterations of the FP64 path for the mixed/FP64 ratio (0 = skip)")
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="instances of the batched blend workload (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -199,6 +208,81 @@ def precision_check(n: int, iters: int, device: int) -> dict:
             "dh_norm_fp64": a["dh_norm"], "dh_norm_mixed": b["dh_norm"]}
 
 
+def fp64_rate(n: int, steps: int, device: int) -> dict:
+    """Device-timed iter/s of the plain FP64 path on the same workload and state
+    preparation (the comparison the mixed path is quoted against)."""
+    import torch
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftSolver
+    cfg, w = W.diblock128(precision="fp64", n=n)
+    cfg.device = device
+    s = ScftSolver(cfg)
+    s.restore(w)
+    s.update(cfg.updater.anderson_start + cfg.updater.anderson_depth + 3)
+    st = torch.cuda.ExternalStream(s.stream_ptr, device=torch.device("cuda", device))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    s.update(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    v, _ = s.variant()
+    s.close()
+    return {"value": steps / (ms / 1000.0), "unit": UNIT, "steps": steps, "kernel_variant": v}
+
+
+def batched_rate(count: int, steps: int, device: int) -> dict:
+    """The batched blend workload: `count` diblock / A-homopolymer instances of
+    uneven grid (32..96)^3, chiN and f_A, FP32 sweeps, Anderson depth 10, Ns = 100,
+    as one batch (merged sweeps, one graph per iteration) and as a loop of
+    single-instance launches; aggregate instance-iterations/s of each."""
+    import torch
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftBatch, ScftSolver
+    items = W.blend_instances(count=count)
+    for c, _ in items:
+        c.device = device
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b = ScftBatch([c for c, _ in items])
+    for i, (_, w) in enumerate(items):
+        b.instance(i).restore(w)
+    b.update(3)                      # eager iteration, per-class autotune, graph capture
+    st = torch.cuda.ExternalStream(b.stream_ptr, device=torch.device("cuda", device))
+    torch.cuda.synchronize()
+    e0.record(st)
+    b.update(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    _, variants = b.classes()
+    launches = b.launches_per_iteration
+    b.close()
+    ms_loop = 0.0
+    for c, w in items:
+        s = ScftSolver(c)
+        s.restore(w)
+        s.update(3)
+        st = torch.cuda.ExternalStream(s.stream_ptr, device=torch.device("cuda", device))
+        torch.cuda.synchronize()
+        e0.record(st)
+        s.update(steps)
+        e1.record(st)
+        e1.synchronize()
+        ms_loop += e0.elapsed_time(e1)
+        s.close()
+    sizes = sorted({c.n[0] for c, _ in items})
+    return {"workload": f"blend{count}: {count} AB-diblock/A-homopolymer instances, grids "
+                        f"{sizes}^3, chiN~U[12,30], f_A~U[0.2,0.5], phi_h~U[0,0.2], Ns=100, "
+                        "FP32 sweeps, Anderson depth 10",
+            "value": count * steps / (ms_batch / 1000.0), "unit": "instance-iter/s",
+            "single_loop_value": count * steps / (ms_loop / 1000.0),
+            "speedup_vs_single_loop": ms_loop / ms_batch, "steps": steps,
+            "class_variants": variants, "launches_per_iteration": launches}
+
+
 def run_reference(args, world, rank):
     """The reference's CPU path (its C restatement; the reference itself cannot be built)."""
     if world > 1 and rank != 0:
@@ -341,6 +425,11 @@ def run_ours(args, world, rank, local):
     solver.close()
     if rank == 0 and world == 1 and args.precision == "mixed" and args.precision_iters > 0:
         out["precision"] = precision_check(args.n, args.precision_iters, local)
+    if rank == 0 and world == 1 and args.precision == "mixed" and args.fp64_steps > 0:
+        out["fp64_path"] = fp64_rate(args.n, args.fp64_steps, local)
+        out["mixed_over_fp64"] = value / out["fp64_path"]["value"]
+    if rank == 0 and world == 1 and args.batch_instances > 0:
+        out["batched"] = batched_rate(args.batch_instances, args.batch_steps, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_full_iteration(args.n)
     if rank == 0:
