@@ -191,6 +191,14 @@ void* ps_gpu_stream(const ps_handle* h);
  * ps_gpu_get_variant also returns the measured sweep time of each variant (ms). */
 int ps_gpu_set_variant(ps_handle* h, int variant);
 int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune);
+
+/* Switch the arithmetic of the propagator sweeps between iterations (no
+ * reference counterpart).  w, p, phi and the FP64 Anderson history carry over
+ * unchanged, so a run can iterate in PS_PREC_MIXED until the FP32 noise floor
+ * of the sweeps and finish in PS_PREC_FP64 (precision escalation).  The first
+ * switch to a precision allocates its slice storage; the kernel variant is
+ * re-tuned.  Not allowed on a batch instance (PS_ATTRIB_ERR). */
+int ps_gpu_set_precision(ps_handle* h, int precision);
 int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
                         double* bytes_per_iter, long long* steps_per_iter);
 

@@ -106,6 +106,7 @@ SIGNATURES = {
     "ps_gpu_stream": (_vp, [_vp]),
     "ps_gpu_set_variant": (C.c_int, [_vp, C.c_int]),
     "ps_gpu_get_variant": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]),
+    "ps_gpu_set_precision": (C.c_int, [_vp, C.c_int]),
     "ps_gpu_sweep_timing": (C.c_int, [_vp, _dbl_p, C.c_int, C.POINTER(C.c_int), _dbl_p,
                                       C.POINTER(C.c_longlong)]),
     "ps_gpu_batch_create": (C.c_int, [C.POINTER(ps_config), C.c_int, C.POINTER(_vp)]),

@@ -273,6 +273,7 @@ static int batch_create(ps_batch* b, const ps_config* cfgs, int count) {
       b->err = "instance " + std::to_string(i) + ": " + ps_gpu_last_error(nullptr);
       return rc;
     }
+    h->in_batch = true;
     b->inst.push_back(h);
     auto key = std::make_tuple(h->n[0], h->n[1], h->n[2], h->prec);
     auto it = cls.find(key);

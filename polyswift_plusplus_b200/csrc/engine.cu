@@ -375,24 +375,25 @@ int engine_prepare_noise(ps_handle* h) {
   return PS_OK;
 }
 
+template <typename T> static void free_buffers(Buffers<T>& B) {
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  for (auto p : B.slices) f(p);
+  for (auto p : B.spec) f(p);
+  for (auto p : B.wfac) f(p);
+  for (auto p : B.kx) f(p);
+  for (auto p : B.kyz) f(p);
+  f(B.tw_x); f(B.tw_y); f(B.tw_z); f(B.tw_zh); f(B.d_plane); f(B.d_pencil);
+  B = Buffers<T>();
+}
+
 static void free_all(ps_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(h->d_w); f(h->d_phi); f(h->d_p); f(h->d_noise);
   if (h->h_noise) cudaFreeHost(h->h_noise);
-  for (auto p : h->bf.slices) f(p);
-  for (auto p : h->bf.spec) f(p);
-  for (auto p : h->bf.wfac) f(p);
-  for (auto p : h->bf.kx) f(p);
-  for (auto p : h->bf.kyz) f(p);
-  f(h->bf.tw_x); f(h->bf.tw_y); f(h->bf.tw_z); f(h->bf.tw_zh); f(h->bf.d_plane); f(h->bf.d_pencil);
-  for (auto p : h->bd.slices) f(p);
-  for (auto p : h->bd.spec) f(p);
-  for (auto p : h->bd.wfac) f(p);
-  for (auto p : h->bd.kx) f(p);
-  for (auto p : h->bd.kyz) f(p);
-  f(h->bd.tw_x); f(h->bd.tw_y); f(h->bd.tw_z); f(h->bd.tw_zh); f(h->bd.d_plane); f(h->bd.d_pencil);
+  free_buffers(h->bf);
+  free_buffers(h->bd);
   f(h->d_qpart); f(h->d_upart); f(h->d_sc);
   if (h->h_sc) cudaFreeHost(h->h_sc);
   f(h->d_hw); f(h->d_hd); f(h->d_gram); f(h->d_gpart);
@@ -927,6 +928,45 @@ int ps_gpu_set_variant(ps_handle* h, int variant) {
   h->node_start = h->node_end = nullptr;
   h->graph_has_timing = false;
   h->variant = variant;
+  return PS_OK;
+}
+
+int ps_gpu_set_precision(ps_handle* h, int precision) {
+  if (!h) return PS_ATTRIB_ERR;
+  if (precision != PS_PREC_FP64 && precision != PS_PREC_MIXED) {
+    h->err = "precision must be PS_PREC_FP64 or PS_PREC_MIXED";
+    return PS_ATTRIB_ERR;
+  }
+  if (precision == h->prec) return PS_OK;
+  if (h->in_batch) {
+    h->err = "the precision of a batch instance is fixed by its batch";
+    return PS_ATTRIB_ERR;
+  }
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  h->node_start = h->node_end = nullptr;
+  h->graph_has_timing = false;
+  const int old = h->prec;
+  const bool built = (precision == PS_PREC_MIXED) ? !h->bf.slices.empty() : !h->bd.slices.empty();
+  h->prec = precision;
+  if (!built) {
+    int rc = (precision == PS_PREC_MIXED) ? build_device_tables<float>(h) : build_device_tables<double>(h);
+    if (rc == PS_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = PS_GPU_ERR;
+    if (rc != PS_OK) {
+      if (precision == PS_PREC_MIXED) free_buffers(h->bf);
+      else free_buffers(h->bd);
+      h->prec = old;
+      return rc;
+    }
+  }
+  const int pb = (precision == PS_PREC_MIXED) ? 4 : 8;
+  h->fused_plane = plane_fused_supported(pb, h->n[1], h->n[2]);
+  h->xy_ok = xy_supported(pb, h->n[0], h->n[1], h->n[2]);
+  h->sweep_bytes = 3.0 * (double)h->N * (double)pb * (double)h->sweep_steps;
+  h->variant = -1;
+  h->eager_iters = 0;
   return PS_OK;
 }
 

@@ -107,6 +107,7 @@ struct ps_handle {
   int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
   float tune_ms[psb::VARIANT_COUNT] = {};
   bool xy_ok = false;  // the row + x-y plane design exists for this grid
+  bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)

@@ -144,6 +144,12 @@ class ScftSolver:
         """Force a kernel variant (0..7) or re-enable autotuning (-1)."""
         self._check(self._lib.ps_gpu_set_variant(self._h, int(variant)))
 
+    def set_precision(self, precision: str) -> None:
+        """Switch the sweeps to "fp64" or "mixed" between iterations; fields and
+        the Anderson history carry over (precision escalation)."""
+        code = {"fp64": A.PS_PREC_FP64, "mixed": A.PS_PREC_MIXED}[precision]
+        self._check(self._lib.ps_gpu_set_precision(self._h, code))
+
     def variant(self):
         """(chosen variant or -1 before tuning, measured sweep ms of each variant;
         -1 for variants that were not timed)."""

@@ -134,3 +134,11 @@ def test_batch_rejects_noise_and_bad_instances(gpu):
     with pytest.raises(A.PsError) as e:
         ScftBatch([cfg, bad])
     assert e.value.code == A.PS_INPUT_ERR
+
+
+def test_batch_instance_precision_is_fixed(gpu):
+    cfg = W.blend(16, 15.0, 0.3, 0.1, precision="mixed")
+    with ScftBatch([cfg]) as b:
+        with pytest.raises(A.PsError) as e:
+            b.instance(0).set_precision("fp64")
+        assert e.value.code == A.PS_ATTRIB_ERR

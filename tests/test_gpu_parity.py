@@ -349,3 +349,58 @@ def test_errors_are_status_codes(gpu):
     with pytest.raises(A.PsError) as e:
         ScftSolver(cfg3)
     assert e.value.code == A.PS_INPUT_ERR
+
+
+def test_precision_switch_carries_state(gpu):
+    """Switching the sweeps from FP32 to FP64 between iterations keeps w, p and
+    phi: with steepest descent (no history) the switched handle then runs
+    exactly like an FP64 handle restored from the same fields."""
+    cfg, w = W.diblock32(n=16, precision="mixed")
+    g = ScftSolver(cfg)
+    g.set_variant(0)
+    g.restore(w)
+    g.update(3)
+    w3 = [g.w(0), g.w(1)]
+    p3 = g.pressure()
+    g.set_precision("fp64")
+    g.set_variant(0)
+    g.update(4)
+    cfg64, _ = W.diblock32(n=16, precision="fp64")
+    f = ScftSolver(cfg64)
+    f.set_variant(0)
+    f.restore(w3, p3)
+    f.update(4)
+    for i in range(2):
+        assert np.array_equal(g.w(i), f.w(i))
+        assert np.array_equal(g.phi(i), f.phi(i))
+    assert g.scalars()["free_energy"] == f.scalars()["free_energy"]
+    assert g.scalars()["iteration"] == 7
+    g.set_precision("mixed")  # back again: buffers are kept, the run continues
+    g.update(2)
+    assert np.isfinite(g.scalars()["free_energy"])
+
+
+def test_precision_escalation_meets_fp64(gpu):
+    """Anderson run mostly in mixed precision, last 20 iterations in FP64 (the
+    history carries over): F lands within 1e-7 of the all-FP64 run, below the
+    FP32 noise floor of the mixed-only run."""
+    iters, finish = 300, 20
+    out = {}
+    for mode in ("fp64", "escalated"):
+        cfg, w = W.diblock32(n=32, precision="fp64" if mode == "fp64" else "mixed")
+        cfg.updater = Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=10,
+                              anderson_mix=1.0, anderson_start=100)
+        g = ScftSolver(cfg)
+        g.restore(w)
+        if mode == "fp64":
+            g.update(iters)
+        else:
+            g.update(iters - finish)
+            g.set_precision("fp64")
+            g.update(finish)
+        out[mode] = g.scalars()
+        g.close()
+    a, b = out["fp64"], out["escalated"]
+    assert a["iteration"] == b["iteration"] == iters
+    assert abs(b["free_energy"] - a["free_energy"]) < 1e-7 * abs(a["free_energy"])
+    assert abs(b["free_energy_nodis"] - a["free_energy_nodis"]) < 1e-7 * abs(a["free_energy_nodis"])
