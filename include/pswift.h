@@ -231,6 +231,30 @@ void* ps_gpu_batch_stream(const ps_batch* b);
 /* Message for the last error of a batch (or of the calling thread when b is NULL). */
 const char* ps_gpu_batch_last_error(const ps_batch* b);
 
+/* --- Adjoint of the propagator sweeps (no reference counterpart) ----------
+ * For one linear block copolymer melt (FP64, two distinct sweeps, block 0
+ * starting at a free chain end).  ps_adj_forward computes, from the fields
+ * w (device, n_fields*N doubles), the densities phi (device, n_fields*N) and
+ * ln Q exactly as one iteration of ps_gpu_iterate computes them
+ * (PsBlockCopolymer::update, pspolymer/PsBlockCopolymer.cpp:189-239).
+ * ps_adj_backward takes dL/dphi (device, n_fields*N) and dL/dlnQ for the
+ * last forward and returns dL/dw (device, n_fields*N), dL/dL_d for the three
+ * box lengths L_d = n_d * cell_d (host, 3) and dL/d(ds_b) for each block's
+ * contour step (host, n_blocks).  Slices are checkpointed every
+ * checkpoint_interval contour steps (1: full storage; 0: ceil(sqrt(steps)));
+ * the results do not depend on the interval.  ps_adj_info reports the steps
+ * per sweep, the interval and the bytes of slice storage. */
+typedef struct ps_adj ps_adj;
+int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out);
+int ps_adj_destroy(ps_adj* a);
+int ps_adj_forward(ps_adj* a, const double* w, double* phi, double* log_q);
+int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w, double* g_box,
+                    double* g_ds);
+int ps_adj_info(const ps_adj* a, int* contour_steps, int* checkpoint_interval, size_t* slice_bytes);
+void* ps_adj_stream(const ps_adj* a);
+/* Message for the last error of an adjoint (or of the calling thread when a is NULL). */
+const char* ps_adj_last_error(const ps_adj* a);
+
 /* --- FFT plugin: PsFFTBase<T,3>::scaledFFTPair with host pointers ---------
  * res = Re(IFFT(kdata * FFT(data))), both transforms unnormalised, as the
  * reference's FFTW c2c pair.  Inputs and outputs are host arrays of n[0]*n[1]*n[2]

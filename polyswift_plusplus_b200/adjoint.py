@@ -1,0 +1,205 @@
+"""Differentiable SCFT pieces: the adjoint of the propagator sweeps in torch.autograd.
+
+``ChainAdjoint`` wraps the native FP64 adjoint (``ps_adj_*``) of one linear
+block copolymer melt: ``forward(w)`` gives the monomer densities phi and ln Q
+(the same sweeps, contour quadrature and Q as one reference iteration,
+PsBlockCopolymer::update, pspolymer/PsBlockCopolymer.cpp:189-239), and
+``backward(g_phi, g_lnQ)`` runs the adjoint sweeps (propagator slices
+checkpointed every C ~ sqrt(Ns) contour steps) for dL/dw, dL/dL_box and
+dL/d(ds) of every block.
+
+``DifferentiableChain`` exposes that as a ``torch.autograd.Function`` of
+(w, box lengths, per-block contour steps): block lengths enter through
+ds_b = f_b / steps_b with the step counts fixed, so dL/df follows by the chain
+rule.  ``free_energy`` and ``steepest_descent_step`` restate the reference's
+free energy (pseffhamil/PsPolymerUpdater.cpp:173-226) and field update
+(pseffhamil/PsSteepDUpdater.cpp:159-203) in torch for two fields, so a loss
+can depend on chiN through F or through updated fields.  Nothing here falls
+back to the CPU: every sweep runs in the native library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+
+import numpy as np
+import torch
+
+from . import _abi as A
+from .config import ScftConfig
+
+
+def _chk(lib, rc, handle):
+    if rc != A.PS_OK:
+        raise A.PsError(rc, (lib.ps_adj_last_error(handle) or b"").decode(errors="replace"))
+
+
+class ChainAdjoint:
+    """Native forward/adjoint pair for one FP64 configuration (fixed box and ds)."""
+
+    def __init__(self, cfg: ScftConfig, checkpoint: int = 0):
+        if cfg.precision != "fp64":
+            cfg = dataclasses.replace(cfg, precision="fp64")
+        self.cfg = cfg
+        self._lib = A.load_library()
+        self._pc = cfg.to_ps_config()
+        h = C.c_void_p()
+        _chk(self._lib, self._lib.ps_adj_create(C.byref(self._pc), int(checkpoint), C.byref(h)), None)
+        self._h = h
+        self.N = cfg.n_total
+        self.nf = len(cfg.fields)
+        self.nb = len(cfg.polymers[0].blocks)
+        steps, ck, nbytes = C.c_int(), C.c_int(), C.c_size_t()
+        _chk(self._lib, self._lib.ps_adj_info(h, C.byref(steps), C.byref(ck), C.byref(nbytes)), h)
+        self.contour_steps, self.checkpoint, self.slice_bytes = steps.value, ck.value, nbytes.value
+        self.forward_count = 0
+
+    def forward(self, w: torch.Tensor):
+        """w: (n_fields, N) float64 CUDA tensor -> (phi (n_fields, N), ln Q)."""
+        w = w.detach().to(torch.float64).contiguous()
+        if not w.is_cuda or w.numel() != self.nf * self.N:
+            raise ValueError("w must be a CUDA float64 tensor of n_fields * N values")
+        phi = torch.empty_like(w)
+        lnq = C.c_double()
+        torch.cuda.current_stream(w.device).synchronize()
+        _chk(self._lib, self._lib.ps_adj_forward(self._h, C.c_void_p(w.data_ptr()), C.c_void_p(phi.data_ptr()),
+                                                 C.byref(lnq)), self._h)
+        self.forward_count += 1
+        return phi.view(self.nf, self.N), lnq.value
+
+    def backward(self, g_phi: torch.Tensor, g_lnq: float):
+        """Gradients for the last forward: (dL/dw (n_fields, N), dL/dL_box (3,), dL/dds (n_blocks,))."""
+        g_phi = g_phi.detach().to(torch.float64).contiguous()
+        gw = torch.empty_like(g_phi)
+        gbox = (C.c_double * 3)()
+        gds = (C.c_double * self.nb)()
+        torch.cuda.current_stream(g_phi.device).synchronize()
+        _chk(self._lib, self._lib.ps_adj_backward(self._h, C.c_void_p(g_phi.data_ptr()), float(g_lnq),
+                                                  C.c_void_p(gw.data_ptr()), gbox, gds), self._h)
+        return (gw.view(self.nf, self.N), np.array([gbox[i] for i in range(3)]),
+                np.array([gds[i] for i in range(self.nb)]))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ps_adj_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _ChainFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, w, box, ds, chain):
+        solver = chain.solver(box, ds)
+        phi, lnq = solver.forward(w)
+        ctx.solver = solver
+        ctx.token = solver.forward_count
+        ctx.save_for_backward(w)
+        return phi, torch.tensor(lnq, dtype=torch.float64, device=w.device)
+
+    @staticmethod
+    def backward(ctx, g_phi, g_lnq):
+        (w,) = ctx.saved_tensors
+        s = ctx.solver
+        if s.forward_count != ctx.token:  # another forward ran on this solver since
+            s.forward(w)
+        if g_phi is None:
+            g_phi = torch.zeros((s.nf, s.N), dtype=torch.float64, device=w.device)
+        gl = 0.0 if g_lnq is None else float(g_lnq)
+        gw, gbox, gds = s.backward(g_phi, gl)
+        return (gw.view_as(w), torch.as_tensor(gbox, dtype=torch.float64),
+                torch.as_tensor(gds, dtype=torch.float64), None)
+
+
+class DifferentiableChain:
+    """phi, ln Q = chain(w, box, ds) for one linear block copolymer melt.
+
+    ``box`` holds the three box lengths (Rg) and ``ds`` the contour step of
+    each block (CPU float64 tensors); the step counts are those of ``cfg``.
+    A native solver is built per distinct (box, ds) and cached.
+    """
+
+    def __init__(self, cfg: ScftConfig, checkpoint: int = 0, cache: int = 8):
+        self.cfg = dataclasses.replace(cfg, precision="fp64")
+        self.checkpoint = checkpoint
+        self._cache: dict = {}
+        self._order: list = []
+        self._max = cache
+        base = ChainAdjoint(self.cfg, checkpoint)
+        p = self.cfg.polymers[0]
+        scale = float(p.length)
+        self.alpha = p.length / scale
+        self.steps = [max(4, int(math.floor(self.alpha * b.lengthfrac / b.ds + 0.5))) if b.force_block_steps
+                      else int(round(self.alpha * b.lengthfrac / b.ds)) for b in p.blocks]
+        self.box0 = tuple(self.cfg.n[d] * self.cfg.cell[d] for d in range(3))
+        self.ds0 = tuple(b.ds for b in p.blocks)
+        self._put((self.box0, self.ds0), base)
+
+    def _put(self, key, solver):
+        self._cache[key] = solver
+        self._order.append(key)
+        while len(self._order) > self._max:
+            old = self._order.pop(0)
+            self._cache.pop(old).close()
+
+    def config_for(self, box, ds) -> ScftConfig:
+        p = self.cfg.polymers[0]
+        blocks = [dataclasses.replace(b, ds=float(d), lengthfrac=float(d) * s / self.alpha,
+                                      force_block_steps=True)
+                  for b, d, s in zip(p.blocks, ds, self.steps)]
+        cell = tuple(float(box[d]) / self.cfg.n[d] for d in range(3))
+        return dataclasses.replace(self.cfg, cell=cell,
+                                   polymers=[dataclasses.replace(p, blocks=blocks)])
+
+    def solver(self, box, ds) -> ChainAdjoint:
+        key = (tuple(float(x) for x in box), tuple(float(x) for x in ds))
+        if key not in self._cache:
+            self._put(key, ChainAdjoint(self.config_for(key[0], key[1]), self.checkpoint))
+        return self._cache[key]
+
+    def __call__(self, w, box=None, ds=None):
+        box = torch.tensor(self.box0, dtype=torch.float64) if box is None else box
+        ds = torch.tensor(self.ds0, dtype=torch.float64) if ds is None else ds
+        return _ChainFn.apply(w, box, ds, self)
+
+    def close(self):
+        for s in self._cache.values():
+            s.close()
+        self._cache.clear()
+        self._order.clear()
+
+
+def dens_avg(cfg: ScftConfig, f: torch.Tensor | None = None) -> list:
+    """Average density of each field, sum_polymers vf * (length fraction of its blocks)."""
+    p = cfg.polymers[0]
+    out = [0.0] * len(cfg.fields)
+    for i, b in enumerate(p.blocks):
+        frac = b.lengthfrac if f is None else f[i]
+        out[cfg.field_index(b.scfield)] = out[cfg.field_index(b.scfield)] + p.volfrac * frac
+    return out
+
+
+def free_energy(w, phi, lnq, chin, avg, vf=1.0, alpha=1.0):
+    """F = -vf ln Q / alpha + mean_r[-sum_i phi_i w_i + chiN (phi_A phi_B - avg_A avg_B)]
+    for two fields (pseffhamil/PsPolymerUpdater.cpp:173-226,
+    pseffhamil/PsFloryInteraction.cpp:275-321, disorder term subtracted)."""
+    field = (-(phi * w).sum(0) + chin * (phi[0] * phi[1] - avg[0] * avg[1])).mean()
+    return -vf * lnq / alpha + field
+
+
+def steepest_descent_step(w, p, phi, chin, avg, lambdas=(0.1, 0.05)):
+    """One reference steepest-descent update of two fields and the pressure
+    (pseffhamil/PsSteepDUpdater.cpp:159-203, :264-278; psphysf/PsConstraint.cpp:184-262):
+    dH_i = p - w_i + chiN (phi_j - avg_j), w_i += l0 (dH_i - l1 dH_j), p = mean-free (w_A + w_B)/2."""
+    l0, l1 = lambdas
+    dh_a = p - w[0] + chin * (phi[1] - avg[1])
+    dh_b = p - w[1] + chin * (phi[0] - avg[0])
+    wa = w[0] + l0 * (dh_a - l1 * dh_b)
+    wb = w[1] + l0 * (dh_b - l1 * dh_a)
+    pn = 0.5 * (wa + wb)
+    return torch.stack([wa, wb]), pn - pn.mean()

@@ -144,7 +144,7 @@ static int build_device_tables(ps_handle* h) {
   for (int s : h->exec) {
     const Sweep& sw = h->sweeps[s];
     T* sl = nullptr;
-    PS_CUDA(h, cudaMalloc((void**)&sl, sizeof(T) * (size_t)(sw.total + 1) * N));
+    if (!h->no_slices) PS_CUDA(h, cudaMalloc((void**)&sl, sizeof(T) * (size_t)(sw.total + 1) * N));
     B.slices.push_back(sl);
     c2_t<T>* sp = nullptr;
     PS_CUDA(h, cudaMalloc((void**)&sp, sizeof(c2_t<T>) * (size_t)h->n[0] * h->n[1] * h->nzh));
@@ -210,7 +210,7 @@ static int build_device_tables(ps_handle* h) {
       w.spec = B.spec[e];
       w.wfac_in = (k > 0) ? B.wfac[seg_of(sw, k - 1).wfac_id] : nullptr;
       w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
-      w.store = B.slices[e] + (size_t)k * N;
+      w.store = B.slices[e] ? B.slices[e] + (size_t)k * N : nullptr;
       w.status = &h->d_sc->error_flags;
       pw.push_back(w);
       if (k < sw.total) {
@@ -744,6 +744,10 @@ static int iterate_impl(ps_handle* h, int n) {
   }
   return engine_check_scalars(h);
 }
+
+int engine_create(ps_handle* h, const ps_config* cfg) { return create_impl(h, cfg); }
+
+void engine_free(ps_handle* h) { free_all(h); }
 
 }  // namespace psb
 

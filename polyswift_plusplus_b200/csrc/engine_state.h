@@ -108,6 +108,7 @@ struct ps_handle {
   float tune_ms[psb::VARIANT_COUNT] = {};
   bool xy_ok = false;  // the row + x-y plane design exists for this grid
   bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
+  bool no_slices = false; // tables only, no slice storage (the adjoint keeps its own)
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
@@ -140,6 +141,10 @@ namespace psb {
 //   engine_pre:  reset phi, Boltzmann factors of every (field, ds);
 //   the sweeps:  handle_sweep_set(h) under launch_sweep_set;
 //   engine_post: Q, contour quadrature into phi, field update, pressure shift.
+// Build an instance from a configuration (ps_gpu_create without the wrapper);
+// with h->no_slices set beforehand no propagator slice storage is allocated.
+int engine_create(ps_handle* h, const ps_config* cfg);
+void engine_free(ps_handle* h);
 int engine_pre(ps_handle* h, long long* nlaunch);
 int engine_post(ps_handle* h, long long* nlaunch);
 // Host-side random-number bookkeeping owed before each iteration.

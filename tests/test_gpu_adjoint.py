@@ -1,0 +1,227 @@
+"""Adjoint of the propagator sweeps against FP64 central finite differences.
+
+The adjoint (ps_adj_*) must reproduce the densities of one engine iteration,
+give gradients that agree with central differences (step 1e-6 relative) to
+1e-5, and give the same result for every checkpoint interval (full storage,
+square-root checkpointing, an uneven interval).  The last test runs the
+differentiation workload: a 64^3, Ns = 128 diblock at a lamellar state, loss
+sum (phi_A - phi_target)^2 after one self-consistent field update, external
+field h on w_A, gradients in w, h, chiN, f_A and the box, and the stress
+dF/dL_box.
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from polyswift_plusplus_b200 import workloads as W
+from polyswift_plusplus_b200.adjoint import (ChainAdjoint, DifferentiableChain, dens_avg, free_energy,
+                                             steepest_descent_step)
+from polyswift_plusplus_b200.config import Updater
+from polyswift_plusplus_b200.scft import ScftSolver
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+TOL = 1e-5
+
+
+def small_case(n=16, ns=32, cell=(0.2, 0.19, 0.21)):
+    cfg = W.diblock_config(n, 3.0, 0.40, 18.0, ns, Updater(kind="steepestDescent", relaxlambdas=(0.1, 0.05)),
+                           "fp64", force=True)
+    cfg = dataclasses.replace(cfg, cell=cell)
+    _, _, z = W.coords(cfg)
+    c = np.cos(2 * math.pi * z / cfg.box[2]).reshape(-1)
+    w = W.random_fields(cfg, 0.5)
+    return cfg, np.stack([w[0] + c, w[1] - c])
+
+
+def loss_terms(cfg, seed=5):
+    rng = np.random.default_rng(seed)
+    t = torch.tensor(rng.uniform(0.2, 0.8, cfg.n_total), device=DEV)
+    r = torch.tensor(rng.standard_normal(cfg.n_total), device=DEV)
+
+    def L(phi, lnq):
+        return ((phi[0] - t) ** 2).sum() + 0.5 * (phi[1] * r).sum() + 0.3 * lnq
+    return L
+
+
+def eval_loss(adj, w, L):
+    phi, lnq = adj.forward(w)
+    return float(L(phi, torch.tensor(lnq, dtype=torch.float64, device=DEV)))
+
+
+def grads(adj, w, L):
+    phi, lnq = adj.forward(w)
+    phi = phi.clone().requires_grad_(True)
+    lq = torch.tensor(lnq, dtype=torch.float64, device=DEV, requires_grad=True)
+    L(phi, lq).backward()
+    return adj.backward(phi.grad, float(lq.grad))
+
+
+def test_adjoint_forward_matches_engine(gpu):
+    cfg, w = small_case()
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.update(1)  # phi of the first iteration is phi(w0)
+    adj = ChainAdjoint(cfg, checkpoint=1)
+    phi, lnq = adj.forward(torch.tensor(w, device=DEV))
+    for i in range(2):
+        ref = s.phi(i)
+        assert np.abs(phi[i].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert lnq == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    assert adj.contour_steps == 32
+
+
+def test_adjoint_field_gradient_matches_finite_differences(gpu):
+    cfg, w = small_case()
+    L = loss_terms(cfg)
+    adj = ChainAdjoint(cfg)  # square-root checkpointing
+    wt = torch.tensor(w, device=DEV)
+    gw, _, _ = grads(adj, wt, L)
+    rng = np.random.default_rng(11)
+    for k in range(3):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        if k == 2:  # a localised direction
+            d = torch.zeros_like(wt)
+            d[0, 1234] = 1.0
+            d[1, 77] = -0.5
+        eps = 1e-6
+        fd = (eval_loss(adj, wt + eps * d, L) - eval_loss(adj, wt - eps * d, L)) / (2 * eps)
+        an = float((gw * d).sum())
+        print(f"dL/dw direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+
+
+def test_adjoint_box_and_ds_gradients_match_finite_differences(gpu):
+    cfg, w = small_case()
+    L = loss_terms(cfg, seed=7)
+    chain = DifferentiableChain(cfg)
+    wt = torch.tensor(w, device=DEV)
+    box = torch.tensor(chain.box0, dtype=torch.float64, requires_grad=True)
+    ds = torch.tensor(chain.ds0, dtype=torch.float64, requires_grad=True)
+    phi, lnq = chain(wt, box, ds)
+    L(phi, lnq).backward()
+
+    def at(b, d):
+        with torch.no_grad():
+            p, q = chain(wt, torch.tensor(b, dtype=torch.float64), torch.tensor(d, dtype=torch.float64))
+            return float(L(p, q))
+    for dim in range(3):
+        h = 1e-6 * chain.box0[dim]
+        bp, bm = list(chain.box0), list(chain.box0)
+        bp[dim] += h
+        bm[dim] -= h
+        fd = (at(bp, chain.ds0) - at(bm, chain.ds0)) / (2 * h)
+        print(f"dL/dL_{dim}: adjoint {box.grad[dim].item():.12e} central difference {fd:.12e}")
+        assert abs(box.grad[dim].item() - fd) <= TOL * abs(fd), (dim, box.grad[dim].item(), fd)
+    for b in range(2):
+        h = 1e-6 * chain.ds0[b]
+        dp, dm = list(chain.ds0), list(chain.ds0)
+        dp[b] += h
+        dm[b] -= h
+        fd = (at(chain.box0, dp) - at(chain.box0, dm)) / (2 * h)
+        print(f"dL/dds_{b}: adjoint {ds.grad[b].item():.12e} central difference {fd:.12e}")
+        assert abs(ds.grad[b].item() - fd) <= TOL * abs(fd), (b, ds.grad[b].item(), fd)
+    chain.close()
+
+
+def test_adjoint_checkpoint_interval_does_not_change_results(gpu):
+    cfg, w = small_case(n=16, ns=40)
+    L = loss_terms(cfg)
+    wt = torch.tensor(w, device=DEV)
+    out = []
+    for ck in (1, 0, 7):  # full storage, ceil(sqrt(40)) = 7, uneven 7 -> 6 segments
+        adj = ChainAdjoint(cfg, checkpoint=ck)
+        phi, lnq = adj.forward(wt)
+        gw, gbox, gds = grads(adj, wt, L)
+        out.append((phi.cpu().numpy(), lnq, gw.cpu().numpy(), gbox, gds, adj.slice_bytes))
+        adj.close()
+    for o in out[1:]:
+        assert np.array_equal(o[0], out[0][0]) and o[1] == out[0][1]
+        assert np.array_equal(o[2], out[0][2])
+        assert np.array_equal(o[3], out[0][3]) and np.array_equal(o[4], out[0][4])
+    assert out[1][5] < out[0][5] / 2  # checkpointing stores far fewer slices
+
+
+def test_differentiation_workload_64cubed(gpu):
+    """cfg: 64^3, box 6.0, f_A 0.40 (51 + 77 steps), chiN 18, Ns 128, FP64, lamellar
+    state.  L = sum (phi_A[w'] - 0.5 - 0.4 cos(2 pi z / L))^2, w' = one steepest-descent
+    update of (w_A + h, w_B) with phi[w + h]; gradients vs central differences."""
+    cfg, w0 = W.diblock64_adjoint()
+    s = ScftSolver(cfg)
+    s.restore(w0)
+    s.update(60)  # relax towards the lamellar saddle point
+    w = torch.tensor(np.stack([s.w(0), s.w(1)]), device=DEV)
+    p = torch.tensor(s.pressure(), device=DEV)
+    s.close()
+    rng = np.random.default_rng(2024)
+    h = torch.tensor(rng.normal(0.0, 0.05, cfg.n_total), device=DEV)
+    _, _, z = W.coords(cfg)
+    target = torch.tensor(0.5 + 0.4 * np.cos(2 * math.pi * z / cfg.box[2]).reshape(-1), device=DEV)
+    chain = DifferentiableChain(cfg)
+    assert chain.steps == [51, 77]
+    assert chain.solver(chain.box0, chain.ds0).checkpoint == 12
+
+    def objective(w, h, chin, f, box):
+        ds = torch.stack([f / 51.0, (1.0 - f) / 77.0])
+        avg = [f, 1.0 - f]
+        wh = torch.stack([w[0] + h, w[1]])
+        phi, lnq = chain(wh, box, ds)
+        w1, _ = steepest_descent_step(wh, p, phi, chin, avg)
+        phi1, _ = chain(w1, box, ds)
+        loss = ((phi1[0] - target) ** 2).sum()
+        F = free_energy(wh, phi, lnq, chin, avg)
+        return loss, F
+
+    wv = w.clone().requires_grad_(True)
+    hv = h.clone().requires_grad_(True)
+    chin = torch.tensor(18.0, dtype=torch.float64, requires_grad=True)
+    f = torch.tensor(0.40, dtype=torch.float64, requires_grad=True)
+    box = torch.tensor(chain.box0, dtype=torch.float64, requires_grad=True)
+    loss, F = objective(wv, hv, chin, f, box)
+    g_w, g_h, g_chin, g_f, _ = torch.autograd.grad(loss, [wv, hv, chin, f, box], retain_graph=True)
+    dF_dbox = torch.autograd.grad(F, box)[0]
+
+    def val(which, **kw):
+        args = dict(w=w, h=h, chin=torch.tensor(18.0, dtype=torch.float64),
+                    f=torch.tensor(0.40, dtype=torch.float64), box=torch.tensor(chain.box0, dtype=torch.float64))
+        args.update(kw)
+        with torch.no_grad():
+            lo, Fv = objective(**args)
+        return float(lo if which == "L" else Fv)
+
+    def check(an, plus, minus, eps, what):
+        fd = (plus - minus) / (2 * eps)
+        print(f"{what}: adjoint {an:.12e} central difference {fd:.12e} rel {abs(an - fd) / abs(fd):.2e}")
+        assert abs(an - fd) <= TOL * abs(fd), (what, an, fd)
+
+    d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+    check(float((g_w * d).sum()), val("L", w=w + 1e-6 * d), val("L", w=w - 1e-6 * d), 1e-6, "dL/dw.d")
+    dh = torch.tensor(rng.standard_normal(cfg.n_total), device=DEV)
+    check(float((g_h * dh).sum()), val("L", h=h + 1e-6 * dh), val("L", h=h - 1e-6 * dh), 1e-6, "dL/dh.d")
+    e = 18.0 * 1e-6
+    check(g_chin.item(), val("L", chin=torch.tensor(18.0 + e, dtype=torch.float64)),
+          val("L", chin=torch.tensor(18.0 - e, dtype=torch.float64)), e, "dL/dchiN")
+    e = 0.4 * 1e-6
+    check(g_f.item(), val("L", f=torch.tensor(0.4 + e, dtype=torch.float64)),
+          val("L", f=torch.tensor(0.4 - e, dtype=torch.float64)), e, "dL/df_A")
+    # The stress is checked as a vector: each component to 1e-5 of the largest
+    # one.  Along x and y (in the lamellar planes) it is about 1e-6 of F, below
+    # what a central difference of F can resolve at this step.
+    an, fd = [], []
+    for dim in range(3):
+        e = chain.box0[dim] * 1e-6
+        bp = torch.tensor(chain.box0, dtype=torch.float64)
+        bm = bp.clone()
+        bp[dim] += e
+        bm[dim] -= e
+        an.append(dF_dbox[dim].item())
+        fd.append((val("F", box=bp) - val("F", box=bm)) / (2 * e))
+        print(f"dF/dL_{'xyz'[dim]}: adjoint {an[-1]:.12e} central difference {fd[-1]:.12e}")
+    scale = max(abs(x) for x in fd)
+    assert abs(fd[2]) == scale
+    for a_, f_ in zip(an, fd):
+        assert abs(a_ - f_) <= TOL * scale, (an, fd)
+    chain.close()
