@@ -105,6 +105,64 @@ __device__ __forceinline__ void c2r_pre(C* buf, const C* twn, int rows) {
   }
 }
 
+// Radix plan of the y FFT of a plane: 128 = 16 x 8 (two passes; with the kz = 0
+// and kz = nz/2 columns packed the 512 threads each take one radix-16 and two
+// radix-8 butterflies).
+template <int L> struct PlanY { using type = typename Plan<L>::type; };
+template <> struct PlanY<128> { using type = RadixList<16, 8>; };
+
+// y FFTs of a whole plane S[y][kz].  In y-space the kz = 0 and kz = nz/2
+// columns are real (the DC and Nyquist bins of a real z transform), so the two
+// share one complex transform: the inverse of A_0 + i A_h is a_0 + i a_h, and
+// the forward transform of x_0 + i x_h is split by Hermitian symmetry,
+// A_0[k] = (C[k] + conj(C[-k]))/2, A_h[k] = -i (C[k] - conj(C[-k]))/2.  The y
+// FFT then runs over nz/2 columns instead of nz/2 + 1.
+template <int ROWS, int NZH, int TH, typename C>
+__device__ __forceinline__ void plane_y_inverse(C* buf, const C* tw) {
+  if constexpr (NZH > 1 && ROWS > 1) {
+    for (int y = threadIdx.x; y < ROWS; y += TH) {
+      const C a = buf[y * NZH], b = buf[y * NZH + NZH - 1];
+      buf[y * NZH] = C{a.x - b.y, a.y + b.x};
+    }
+    __syncthreads();
+    smem_fft<ROWS, NZH - 1, TH, true, true, C, typename PlanY<ROWS>::type>(buf, 1, NZH, tw);
+    using S = decltype(buf[0].x);
+    for (int y = threadIdx.x; y < ROWS; y += TH) {
+      const C c = buf[y * NZH];
+      buf[y * NZH] = C{c.x, S(0)};
+      buf[y * NZH + NZH - 1] = C{c.y, S(0)};
+    }
+    __syncthreads();
+  } else {
+    smem_fft<ROWS, NZH, TH, true, true>(buf, 1, NZH, tw);
+  }
+}
+
+template <int ROWS, int NZH, int TH, typename C>
+__device__ __forceinline__ void plane_y_forward(C* buf, const C* tw) {
+  if constexpr (NZH > 1 && ROWS > 1) {
+    for (int y = threadIdx.x; y < ROWS; y += TH) buf[y * NZH] = C{buf[y * NZH].x, buf[y * NZH + NZH - 1].x};
+    __syncthreads();
+    smem_fft<ROWS, NZH - 1, TH, false, true, C, typename PlanY<ROWS>::type>(buf, 1, NZH, tw);
+    using S = decltype(buf[0].x);
+    for (int k = threadIdx.x; k <= ROWS / 2; k += TH) {
+      const int km = (ROWS - k) % ROWS;
+      const C c = buf[k * NZH], d = buf[km * NZH];
+      const C a0 = {S(0.5) * (c.x + d.x), S(0.5) * (c.y - d.y)};
+      const C ah = {S(0.5) * (c.y + d.y), S(0.5) * (d.x - c.x)};
+      buf[k * NZH] = a0;
+      buf[k * NZH + NZH - 1] = ah;
+      if (km != k) {
+        buf[km * NZH] = C{a0.x, -a0.y};
+        buf[km * NZH + NZH - 1] = C{ah.x, -ah.y};
+      }
+    }
+    __syncthreads();
+  } else {
+    smem_fft<ROWS, NZH, TH, false, true>(buf, 1, NZH, tw);
+  }
+}
+
 // Real-space part of a step on the tile held in shared memory (row stride RS
 // reals): MID: q = a*wfac_in, store q, a = q*wfac_out; LAST: q = a*wfac_in,
 // store q; FIRST: a = src (or 1), store a, a = a*wfac_out.
@@ -302,7 +360,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
       }
     }
     __syncthreads();
-    if constexpr (DO_Y) smem_fft<ROWS, NZH, TH, true, true>(buf, 1, NZH, s_tw_y);
+    if constexpr (DO_Y) plane_y_inverse<ROWS, NZH, TH>(buf, s_tw_y);
     if constexpr (NZ > 1) {
       c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
       __syncthreads();
@@ -340,7 +398,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     __syncthreads();
   }
 forward_y:
-  if constexpr (DO_Y) smem_fft<ROWS, NZH, TH, false, true>(buf, 1, NZH, s_tw_y);
+  if constexpr (DO_Y) plane_y_forward<ROWS, NZH, TH>(buf, s_tw_y);
   if constexpr (BULK) {
     fence_proxy_async_smem();
     __syncthreads();
