@@ -185,9 +185,12 @@ int ps_gpu_enable_sweep_timing(ps_handle* h, int max_samples);
 void* ps_gpu_stream(const ps_handle* h);
 
 /* Kernel variant of the propagator sweeps (no reference counterpart).  Every
- * variant computes the same result; they differ in how passes are fused.
- * variant = -1 (the default) times all variants on the handle's own sweeps
- * before its first captured iteration and keeps the fastest; 0..3 forces one.
+ * variant computes the same result; they differ in how passes are fused
+ * (bits 0, 1), in the FFT decomposition (bit 2: row + x-y planes) and in
+ * whether an instance's sweeps share launches or run as concurrent launch
+ * chains (bit 3).  variant = -1 (the default) times all variants on the
+ * handle's own sweeps before its first captured iteration and keeps the
+ * fastest; 0..15 forces one.
  * ps_gpu_get_variant also returns the measured sweep time of each variant (ms). */
 int ps_gpu_set_variant(ps_handle* h, int variant);
 int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune);

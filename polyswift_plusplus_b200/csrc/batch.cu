@@ -121,7 +121,7 @@ static int build_class_tables(ps_batch* b, BatchClass& c) {
 static int class_variant(ps_batch* b, const BatchClass& c) {
   int v = (b->forced_variant >= 0) ? b->forced_variant : (c.variant < 0 ? 0 : c.variant);
   if ((v & VARIANT_XY) && !b->inst[c.members[0]]->xy_ok) v &= ~VARIANT_XY;
-  return v;
+  return v & ~VARIANT_SPLIT;  // a class's sweeps always share launches
 }
 
 static int launch_class(ps_batch* b, BatchClass& c, long long* nl) {

@@ -197,12 +197,23 @@ static int build_device_tables(ps_handle* h) {
       if (step >= g.off && step < g.off + g.steps) return g;
     return sw.segs.back();
   };
+  const size_t ne = h->exec.size();
+  h->sw_plane_off.assign(ne, std::vector<int>(h->kmax + 1, 0));
+  h->sw_plane_cnt.assign(ne, std::vector<int>(h->kmax + 1, 0));
+  h->sw_pencil_off.assign(ne, std::vector<int>(h->kmax + 1, 0));
+  h->sw_pencil_cnt.assign(ne, std::vector<int>(h->kmax + 1, 0));
   for (int k = 0; k <= h->kmax; ++k) {
     h->plane_off[k] = (int)pw.size();
     h->pencil_off[k] = (int)xw.size();
     for (size_t e = 0; e < h->exec.size(); ++e) {
       const Sweep& sw = h->sweeps[h->exec[e]];
       if (k > sw.total) continue;
+      h->sw_plane_off[e][k] = (int)pw.size();
+      h->sw_plane_cnt[e][k] = 1;
+      if (k < sw.total) {
+        h->sw_pencil_off[e][k] = (int)xw.size();
+        h->sw_pencil_cnt[e][k] = 1;
+      }
       PlaneWork<T> w;
       memset(&w, 0, sizeof(w));
       w.mode = (k == 0) ? MODE_FIRST : (k == sw.total ? MODE_LAST : MODE_MID);
@@ -235,7 +246,23 @@ static int build_device_tables(ps_handle* h) {
 // Launch the propagator sweeps of one iteration.
 template <typename T>
 static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
-  PS_CUDA(h, launch_sweep_set<T>(handle_sweep_set<T>(h), variant, h->st, nlaunch));
+  if (!(variant & VARIANT_SPLIT) || h->sw_st.empty()) {
+    PS_CUDA(h, launch_sweep_set<T>(handle_sweep_set<T>(h), variant, h->st, nlaunch));
+    return PS_OK;
+  }
+  // one launch chain per executed sweep, forked from and joined back into h->st
+  PS_CUDA(h, cudaEventRecord(h->ev_split, h->st));
+  for (size_t e = 0; e < h->sw_st.size(); ++e) {
+    SweepSet<T> s = handle_sweep_set<T>(h);
+    s.plane_off = h->sw_plane_off[e].data();
+    s.plane_cnt = h->sw_plane_cnt[e].data();
+    s.pencil_off = h->sw_pencil_off[e].data();
+    s.pencil_cnt = h->sw_pencil_cnt[e].data();
+    PS_CUDA(h, cudaStreamWaitEvent(h->sw_st[e], h->ev_split, 0));
+    PS_CUDA(h, launch_sweep_set<T>(s, variant & ~VARIANT_SPLIT, h->sw_st[e], nlaunch));
+    PS_CUDA(h, cudaEventRecord(h->sw_ev[e], h->sw_st[e]));
+    PS_CUDA(h, cudaStreamWaitEvent(h->st, h->sw_ev[e], 0));
+  }
   return PS_OK;
 }
 
@@ -328,9 +355,36 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
 // warm-up and one timed sweep each) and keep the fastest.
 template <typename T>
 static int autotune_t(ps_handle* h) {
-  int best = 0;
-  PS_CUDA(h, autotune_sweep_set<T>(handle_sweep_set<T>(h), h->st, h->tune_ms, &best));
-  h->variant = best;
+  cudaEvent_t a = nullptr, b = nullptr;
+  PS_CUDA(h, cudaEventCreate(&a));
+  cudaError_t e = cudaEventCreate(&b);
+  float best = 1e30f;
+  int best_v = 0;
+  int rc = PS_OK;
+  for (int v = 0; v < VARIANT_COUNT && e == cudaSuccess && rc == PS_OK; ++v) {
+    h->tune_ms[v] = -1.f;
+    if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
+    if ((v & VARIANT_SPLIT) && h->sw_st.empty()) continue;                 // one sweep only
+    long long nl = 0;
+    rc = launch_sweeps<T>(h, &nl, v);  // warm-up
+    if (rc == PS_OK) e = cudaEventRecord(a, h->st);
+    if (rc == PS_OK && e == cudaSuccess) rc = launch_sweeps<T>(h, &nl, v);
+    if (rc == PS_OK && e == cudaSuccess) e = cudaEventRecord(b, h->st);
+    if (rc == PS_OK && e == cudaSuccess) e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (rc == PS_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (rc != PS_OK || e != cudaSuccess) break;
+    h->tune_ms[v] = ms;
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (rc) return rc;
+  PS_CUDA(h, e);
+  h->variant = best_v;
   return PS_OK;
 }
 
@@ -401,6 +455,9 @@ static void free_all(ps_handle* h) {
   if (h->ev_cap_end) cudaEventDestroy(h->ev_cap_end);
   for (auto e : h->ev_start) cudaEventDestroy(e);
   for (auto e : h->ev_end) cudaEventDestroy(e);
+  for (auto s : h->sw_st) cudaStreamDestroy(s);
+  for (auto e : h->sw_ev) cudaEventDestroy(e);
+  if (h->ev_split) cudaEventDestroy(h->ev_split);
   if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -615,6 +672,17 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   h->dev = c.device;
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  if (h->exec.size() > 1) {
+    PS_CUDA(h, cudaEventCreateWithFlags(&h->ev_split, cudaEventDisableTiming));
+    for (size_t e = 0; e < h->exec.size(); ++e) {
+      cudaStream_t s = nullptr;
+      cudaEvent_t ev = nullptr;
+      PS_CUDA(h, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      h->sw_st.push_back(s);
+      PS_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      h->sw_ev.push_back(ev);
+    }
+  }
   const int pb = (h->prec == PS_PREC_MIXED) ? 4 : 8;
   h->fused_plane = plane_fused_supported(pb, c.n[1], c.n[2]);
   h->xy_ok = xy_supported(pb, c.n[0], c.n[1], c.n[2]);

@@ -82,6 +82,12 @@ struct ps_handle {
   std::vector<std::pair<double, double>> ktab_keys;
   int kmax = 0;
   std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
+  // the same tables restricted to one executed sweep (VARIANT_SPLIT), and the
+  // streams and events of its launch chain
+  std::vector<std::vector<int>> sw_plane_off, sw_plane_cnt, sw_pencil_off, sw_pencil_cnt;
+  std::vector<cudaStream_t> sw_st;
+  std::vector<cudaEvent_t> sw_ev;
+  cudaEvent_t ev_split = nullptr;
 
   psb::Buffers<float> bf;
   psb::Buffers<double> bd;

@@ -44,7 +44,10 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // inverse first pass.
 // bit 2: the sweeps use the row + x-y plane design (transposed half spectrum
 // S[kz][x][y]) instead of the y-z plane + x pencil design.
-enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_XY = 4, VARIANT_COUNT = 8 };
+// bit 3: each sweep of an instance runs as its own chain of launches on its
+// own stream (parallel graph branches) instead of all sweeps in lockstep in
+// shared launches; single-instance engine only (kernels ignore the bit).
+enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_XY = 4, VARIANT_SPLIT = 8, VARIANT_COUNT = 16 };
 
 // The x-y plane design exists for this grid (square x-y planes that fit in
 // shared memory).

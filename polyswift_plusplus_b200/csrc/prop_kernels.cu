@@ -166,10 +166,22 @@ __device__ __forceinline__ void plane_y_forward(C* buf, const C* tw) {
 // Real-space part of a step on the tile held in shared memory (row stride RS
 // reals): MID: q = a*wfac_in, store q, a = q*wfac_out; LAST: q = a*wfac_in,
 // store q; FIRST: a = src (or 1), store a, a = a*wfac_out.
+// Pairs of reals: one 8-byte (FP32) or 16-byte (FP64) access, aligned in the
+// shared tile (rows of 2*(nz/2+1) reals) and conflict-free for consecutive threads.
+template <typename T> struct RVec;
+template <> struct RVec<float> {
+  using type = float2;
+  static constexpr int n = 2;
+};
+template <> struct RVec<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
 template <typename T, int ROWS, int NZ, int TH>
 __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_t roff, int rows) {
   constexpr int RS = 2 * (NZ / 2 + 1);
-  using VT = Vec16<T>;
+  using VT = RVec<T>;
   using V = typename VT::type;
   constexpr int VN = VT::n;
   if constexpr (NZ % VN == 0 && (ROWS * NZ / VN) % TH == 0) {
@@ -205,24 +217,27 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
         const int z = (g - r * ZV) * VN;
         if (r >= rows) continue;
         const size_t gi = roff + (size_t)r * NZ + z;
-        T* sp = rbuf + r * RS + z;
+        V* sp = reinterpret_cast<V*>(rbuf + r * RS + z);
+        const V cur = (w.mode == MODE_FIRST) ? V{} : *sp;
         V q;
 #pragma unroll
         for (int i = 0; i < VN; ++i) {
           T v;
           if (w.mode == MODE_FIRST) v = need_src ? vget<V, T>(a[c], i) : T(1);
-          else v = sp[i] * (need_in ? vget<V, T>(a[c], i) : T(1));
+          else v = vget<V, T>(cur, i) * (need_in ? vget<V, T>(a[c], i) : T(1));
           vset(q, i, v);
         }
         if (w.store) *reinterpret_cast<V*>(w.store + gi) = q;
         if (w.mode != MODE_LAST) {
+          V o;
 #pragma unroll
           for (int i = 0; i < VN; ++i) {
             T f = T(1);
             if (need_out) f = vget<V, T>(b[c], i);
             else if (w.mode == MODE_MID && same && need_in) f = vget<V, T>(a[c], i);
-            sp[i] = vget<V, T>(q, i) * f;
+            vset(o, i, vget<V, T>(q, i) * f);
           }
+          *sp = o;
         }
       }
     }

@@ -81,6 +81,7 @@ cudaError_t autotune_sweep_set(const SweepSet<T>& s, cudaStream_t st, float* tun
   for (int v = 0; v < VARIANT_COUNT && e == cudaSuccess; ++v) {
     tune_ms[v] = -1.f;
     if ((v & VARIANT_XY) && (!s.xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
+    if (v & VARIANT_SPLIT) continue;  // a property of how an instance's sweeps are launched
     long long nl = 0;
     e = launch_sweep_set<T>(s, v, st, &nl);
     if (e == cudaSuccess) e = cudaEventRecord(a, st);
