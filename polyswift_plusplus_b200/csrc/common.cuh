@@ -15,6 +15,32 @@ template <typename C>
 __device__ __forceinline__ C cadd(C a, C b) { return {a.x + b.x, a.y + b.y}; }
 template <typename C>
 __device__ __forceinline__ C csub(C a, C b) { return {a.x - b.x, a.y - b.y}; }
+
+#if !defined(PSB_SCALAR_F32)
+#define PSB_PACKED_F32X2 1
+#endif
+#if defined(PSB_PACKED_F32X2)
+// FP32 complex add / subtract as one packed two-lane instruction (sm_100
+// f32x2 arithmetic, round to nearest: the same result as two scalar ops).
+template <>
+__device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+template <>
+__device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+#endif
 template <typename C>
 __device__ __forceinline__ C cmul(C a, C b) {
   return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
