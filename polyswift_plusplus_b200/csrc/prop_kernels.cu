@@ -105,6 +105,136 @@ __device__ __forceinline__ void c2r_pre(C* buf, const C* twn, int rows) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// nz = 128 rows (half length H = 64 = 8 x 8): the c2r pre-processing is folded
+// into the first inverse z pass and the r2c post-processing into the last
+// forward z pass, removing two shared-memory round trips.  Thread -> (row
+// b = t % ROWS, pair p = t / ROWS): butterflies j1 = p and j2 = 8 - p
+// (p = 1..3), or 0 and 4 (p = 0).  The elements {j + 8r} of the two butterflies
+// hold every partner pair (k, 64 - k) that the pre- and post-processing combine.
+// ---------------------------------------------------------------------------
+template <typename C>
+__device__ __forceinline__ C c2r_pre_one(C a, C b, C w) {
+  // C'[k] = (A[k] + conj(A[h-k])) + i conj(W^k) (A[k] - conj(A[h-k]))
+  const C ep = {a.x + b.x, a.y - b.y};
+  const C dm = {a.x - b.x, a.y + b.y};
+  const C op = cmulc(dm, w);
+  return {ep.x - op.y, ep.y + op.x};
+}
+
+template <typename C>
+__device__ __forceinline__ C r2c_post_one(C c, C d, C w) {
+  // E = (C[k] + conj(C[km]))/2, O = -i (C[k] - conj(C[km]))/2, A[k] = E + W^k O
+  using S = decltype(c.x);
+  const C E = {S(0.5) * (c.x + d.x), S(0.5) * (c.y - d.y)};
+  const C O = {S(0.5) * (c.y + d.y), S(0.5) * (d.x - c.x)};
+  return cadd(E, cmul(w, O));
+}
+
+template <int ROWS, int TH, typename C>
+__device__ __forceinline__ void z64_inverse_first(C* buf, const C* tw_z) {
+  static_assert(ROWS * 4 == TH, "one butterfly pair per thread");
+  constexpr int NZH = 65;
+  const int b = threadIdx.x % ROWS;
+  const int p = threadIdx.x / ROWS;  // uniform over a warp
+  const int j1 = p, j2 = (p == 0) ? 4 : 8 - p;
+  C* row = buf + b * NZH;
+  C a1[8], a2[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    a1[r] = row[j1 + 8 * r];
+    a2[r] = row[j2 + 8 * r];
+  }
+  if (p == 0) {
+    const C nyq = row[64];
+    a1[0] = c2r_pre_one(a1[0], nyq, tw_z[0]);
+#pragma unroll
+    for (int r = 1; r < 4; ++r) {
+      const C x = a1[r], y = a1[8 - r];
+      a1[r] = c2r_pre_one(x, y, tw_z[8 * r]);
+      a1[8 - r] = c2r_pre_one(y, x, tw_z[8 * (8 - r)]);
+    }
+    a1[4] = c2r_pre_one(a1[4], a1[4], tw_z[32]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const C x = a2[r], y = a2[7 - r];
+      a2[r] = c2r_pre_one(x, y, tw_z[4 + 8 * r]);
+      a2[7 - r] = c2r_pre_one(y, x, tw_z[4 + 8 * (7 - r)]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const C x = a1[r], y = a2[7 - r];
+      a1[r] = c2r_pre_one(x, y, tw_z[j1 + 8 * r]);
+      a2[7 - r] = c2r_pre_one(y, x, tw_z[j2 + 8 * (7 - r)]);
+    }
+  }
+  __syncthreads();  // every element read before any is overwritten
+  Dft<8, true, C>::run(a1);
+  Dft<8, true, C>::run(a2);
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    row[8 * j1 + r] = a1[r];
+    row[8 * j2 + r] = a2[r];
+  }
+  __syncthreads();
+}
+
+template <int ROWS, int TH, typename C>
+__device__ __forceinline__ void z64_forward_last(C* buf, const C* tw_zh, const C* tw_z) {
+  static_assert(ROWS * 4 == TH, "one butterfly pair per thread");
+  constexpr int NZH = 65;
+  const int b = threadIdx.x % ROWS;
+  const int p = threadIdx.x / ROWS;
+  const int j1 = p, j2 = (p == 0) ? 4 : 8 - p;
+  C* row = buf + b * NZH;
+  C v1[8], v2[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    v1[r] = row[j1 + 8 * r];
+    v2[r] = row[j2 + 8 * r];
+  }
+  __syncthreads();
+  // last Stockham pass of the 64-point forward FFT (radix 8, 8 already applied)
+#pragma unroll
+  for (int r = 1; r < 8; ++r) {
+    v1[r] = cmul(v1[r], tw_zh[r * j1]);
+    v2[r] = cmul(v2[r], tw_zh[r * j2]);
+  }
+  Dft<8, false, C>::run(v1);
+  Dft<8, false, C>::run(v2);
+  // v1[r] = C[j1 + 8r], v2[r] = C[j2 + 8r] (natural order); post-process pairs
+  if (p == 0) {
+    using S = decltype(v1[0].x);
+    const C c0 = v1[0];
+    const C E = {c0.x, S(0)};
+    const C O = {c0.y, S(0)};
+    row[64] = C{E.x - O.x, S(0)};
+    row[0] = C{E.x + O.x, S(0)};
+#pragma unroll
+    for (int r = 1; r < 4; ++r) {
+      const C x = v1[r], y = v1[8 - r];
+      row[8 * r] = r2c_post_one(x, y, tw_z[8 * r]);
+      row[8 * (8 - r)] = r2c_post_one(y, x, tw_z[8 * (8 - r)]);
+    }
+    row[32] = r2c_post_one(v1[4], v1[4], tw_z[32]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const C x = v2[r], y = v2[7 - r];
+      row[4 + 8 * r] = r2c_post_one(x, y, tw_z[4 + 8 * r]);
+      row[4 + 8 * (7 - r)] = r2c_post_one(y, x, tw_z[4 + 8 * (7 - r)]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const C x = v1[r], y = v2[7 - r];
+      row[j1 + 8 * r] = r2c_post_one(x, y, tw_z[j1 + 8 * r]);
+      row[j2 + 8 * (7 - r)] = r2c_post_one(y, x, tw_z[j2 + 8 * (7 - r)]);
+    }
+  }
+  __syncthreads();
+}
+
 // Radix plan of the y FFT of a plane: 128 = 16 x 8 (two passes; with the kz = 0
 // and kz = nz/2 columns packed the 512 threads each take one radix-16 and two
 // radix-8 butterflies).
@@ -377,9 +507,9 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     __syncthreads();
     if constexpr (DO_Y) plane_y_inverse<ROWS, NZH, TH>(buf, s_tw_y);
     if constexpr (NZ > 1) {
-      c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
-      __syncthreads();
       if (FZ && w.mode == MODE_MID && w.wfac_in && w.wfac_in == w.wfac_out && w.store) {
+        c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
+        __syncthreads();
         // inverse z FFT, real-space step and forward z FFT with the last inverse
         // pass, the step and the first forward pass in one round trip
         using PI = typename Plan<H>::type;
@@ -397,7 +527,14 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
         __syncthreads();
         goto forward_y;
       }
-      smem_fft<H, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
+      if constexpr (NZ == 128 && DO_Y && ROWS * 4 == TH) {
+        z64_inverse_first<ROWS, TH>(buf, s_tw_z);
+        stockham_pass<H, 8, 8, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
+      } else {
+        c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
+        __syncthreads();
+        smem_fft<H, ROWS, TH, true, true>(buf, NZH, 1, s_tw_zh);
+      }
     }
   }
   real_space<T, ROWS, NZ, TH>(w, rbuf, roff, rows);
@@ -408,9 +545,14 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
   }
   __syncthreads();
   if constexpr (NZ > 1) {
-    smem_fft<H, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
-    r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
-    __syncthreads();
+    if constexpr (NZ == 128 && DO_Y && ROWS * 4 == TH) {
+      stockham_pass<H, 8, 1, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
+      z64_forward_last<ROWS, TH>(buf, s_tw_zh, s_tw_z);
+    } else {
+      smem_fft<H, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
+      r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
+      __syncthreads();
+    }
   }
 forward_y:
   if constexpr (DO_Y) plane_y_forward<ROWS, NZH, TH>(buf, s_tw_y);
