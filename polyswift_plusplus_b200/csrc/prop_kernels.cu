@@ -508,6 +508,21 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     if constexpr (DO_Y) plane_y_inverse<ROWS, NZH, TH>(buf, s_tw_y);
     if constexpr (NZ > 1) {
       if (FZ && w.mode == MODE_MID && w.wfac_in && w.wfac_in == w.wfac_out && w.store) {
+        if constexpr (NZ == 128 && DO_Y && ROWS * 4 == TH) {
+          // pre-processing + first inverse pass; last inverse pass + real-space
+          // step + first forward pass (index-fastest: each warp covers 4 rows x
+          // 8 butterflies, so the wfac loads and q stores are 64-byte segments);
+          // last forward pass + post-processing
+          z64_inverse_first<ROWS, TH>(buf, s_tw_z);
+          RealStepOp<T, NZ, 8> op;
+          op.wfac = w.wfac_in;
+          op.store = w.store;
+          op.roff = roff;
+          op.rows = rows;
+          fused_pass_pair<H, 8, ROWS, TH, true, false, false>(buf, NZH, 1, s_tw_zh, op);
+          z64_forward_last<ROWS, TH>(buf, s_tw_zh, s_tw_z);
+          goto forward_y;
+        }
         c2r_pre<NZ, ROWS, TH>(buf, s_tw_z, rows);
         __syncthreads();
         // inverse z FFT, real-space step and forward z FFT with the last inverse

@@ -72,7 +72,7 @@ def test_fp64_diblock_parity(gpu, oracle_lib, n):
     assert g.launches_per_iteration > 0
 
 
-@pytest.mark.parametrize("variant", list(range(8)) + [8, 10, 14])
+@pytest.mark.parametrize("variant", list(range(8)) + [8, 9, 10, 11, 14])
 @pytest.mark.parametrize("n", [16, 32])
 def test_every_kernel_variant_matches_oracle(gpu, oracle_lib, variant, n):
     cfg, w = W.diblock32(n=n)
@@ -404,3 +404,28 @@ def test_precision_escalation_meets_fp64(gpu):
     assert a["iteration"] == b["iteration"] == iters
     assert abs(b["free_energy"] - a["free_energy"]) < 1e-7 * abs(a["free_energy"])
     assert abs(b["free_energy_nodis"] - a["free_energy_nodis"]) < 1e-7 * abs(a["free_energy_nodis"])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 9, 11])
+def test_128_square_plane_variants_match_oracle(gpu, oracle_lib, variant):
+    """8 x 128 x 128 grid: the 128 x 128 y-z plane kernel, whose z passes fold the
+    real-transform pre/post-processing into the first/last pass and (bit 0) fuse
+    the real-space step into the middle pass; FP64 against the oracle at 1e-10."""
+    import dataclasses
+    cfg, _ = W.diblock32(n=16)
+    cfg = dataclasses.replace(cfg, n=(8, 128, 128), cell=(0.5, 4.0 / 128, 4.0 / 128))
+    _, y, z = W.coords(cfg)
+    w = W.random_fields(cfg, 0.2)
+    c = (np.cos(2 * math.pi * z / cfg.box[2]) * np.cos(2 * math.pi * y / cfg.box[1])).reshape(-1)
+    w = [w[0] + c, w[1] - c]
+    g = ScftSolver(cfg)
+    g.set_variant(variant)
+    g.restore(w)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(3)
+    hg = []
+    for _ in range(3):
+        g.update(1)
+        hg.append(g.scalars())
+    assert_parity(cfg, g, o, hg, ho)
