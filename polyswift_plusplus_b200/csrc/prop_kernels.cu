@@ -1077,6 +1077,9 @@ cudaError_t launch_pencil_impl(const PencilWork<T>* d_works, int nworks, int mod
   PSB_PENCIL_CASE(T, 48, 256)
   PSB_PENCIL_CASE(T, 64, 256)
   PSB_PENCIL_CASE(T, 96, 256)
+  if (len == 128 && sizeof(T) == 4)
+    return launch_pencil_modes<T, 128, 16, 128>(d_works, nworks, mode, outer, inner, tw, nx, ny, nz,
+                                                variant, st);
   PSB_PENCIL_CASE(T, 128, 256)
   PSB_PENCIL_CASE(T, 256, 256)
   return cudaErrorInvalidValue;
