@@ -184,11 +184,17 @@ def dens_avg(cfg: ScftConfig, f: torch.Tensor | None = None) -> list:
     return out
 
 
-def free_energy(w, phi, lnq, chin, avg, vf=1.0, alpha=1.0):
-    """F = -vf ln Q / alpha + mean_r[-sum_i phi_i w_i + chiN (phi_A phi_B - avg_A avg_B)]
-    for two fields (pseffhamil/PsPolymerUpdater.cpp:173-226,
-    pseffhamil/PsFloryInteraction.cpp:275-321, disorder term subtracted)."""
-    field = (-(phi * w).sum(0) + chin * (phi[0] * phi[1] - avg[0] * avg[1])).mean()
+def free_energy(w, phi, lnq, chin, avg, vf=1.0, alpha=1.0, pairs=None):
+    """F = -vf ln Q / alpha + mean_r[-sum_i phi_i w_i + sum_pairs chiN_ij (phi_i phi_j - avg_i avg_j)]
+    (pseffhamil/PsPolymerUpdater.cpp:173-226, pseffhamil/PsFloryInteraction.cpp:275-321,
+    disorder term subtracted).  Two fields: ``chin`` is the A-B chiN; otherwise ``pairs`` lists
+    (i, j, chiN_ij) and ``chin`` is ignored."""
+    if pairs is None:
+        pairs = [(0, 1, chin)]
+    inter = 0.0
+    for i, j, c in pairs:
+        inter = inter + c * (phi[i] * phi[j] - avg[i] * avg[j])
+    field = (-(phi * w).sum(0) + inter).mean()
     return -vf * lnq / alpha + field
 
 
