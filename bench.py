@@ -42,6 +42,8 @@ METRIC = "SCFT iter/s at 128³ Ns=200: mixed vs FP64 at |ΔF/F|<1e-6; % HBM roof
 UNIT = "iter/s"
 WORKLOAD = ("diblock128: AB diblock melt 128^3, box 8.0 Rg, f_A=0.35, chiN=25, Ns=200, "
             "Anderson depth 10, mixed precision")
+TRIBLOCK = ("triblock256: ABC linear triblock 256^3, box 16 Rg, fractions (0.3, 0.4, 0.3), "
+            "chiN AB 30, BC 30, AC 45, Ns=400, Anderson depth 20, mixed precision")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -64,6 +66,9 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched blend workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--workload", choices=["diblock128", "triblock256"], default="diblock128",
+                    help="triblock256: the 256^3 ABC scale case (about 75 GB on the device; "
+                         "reports the variable-cell stress step instead of the 128^3 extras)")
     return ap.parse_args()
 
 
@@ -358,7 +363,13 @@ def run_ours(args, world, rank, local):
     from polyswift_plusplus_b200.scft import ScftSolver
 
     torch.cuda.set_device(local)
-    cfg, w = W.diblock128(precision=args.precision, n=args.n)
+    tri = args.workload == "triblock256"
+    if tri:
+        cfg, w = W.triblock256(precision=args.precision)
+        wl, grid, ns, upd = TRIBLOCK, 256, 400, "anderson20"
+    else:
+        cfg, w = W.diblock128(precision=args.precision, n=args.n)
+        wl, grid, ns, upd = WORKLOAD, args.n, 200, "anderson10"
     cfg.device = local
     solver = ScftSolver(cfg)
     solver.restore(w)
@@ -432,7 +443,7 @@ def run_ours(args, world, rank, local):
     per_step_ms = mean_sweep / max(sweep_steps, 1)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": profile_traffic(args.n, args.precision),
+                "traffic": profile_traffic(grid, args.precision),
                 "kernel": "propagator step (plane_kernel + pencil_kernel per step of every sweep)",
                 "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_step": 3 * N * (4 if args.precision == "mixed" else 8),
@@ -442,20 +453,35 @@ def run_ours(args, world, rank, local):
            "scaling": "weak", "vs_baseline": None,
            "dtype": "f32 propagators + f64 reductions" if args.precision == "mixed" else "f64",
            "data": "synthetic",
-           "config": {"workload": WORKLOAD if args.precision == "mixed" else
-                      WORKLOAD.replace("mixed precision", "FP64"),
-                      "grid": args.n, "ns": 200, "precision": args.precision, "updater": "anderson10",
+           "config": {"workload": wl if args.precision == "mixed" else
+                      wl.replace("mixed precision", "FP64"),
+                      "grid": grid, "ns": ns, "precision": args.precision, "updater": upd,
                       "parallelism": f"replicas x{world}",
                       "kernel_variant": variant,
                       "variant_sweep_ms": [round(x, 3) for x in variant_ms],
                       "state": f"{prep} iterations before warm-up: timed iterations use the full "
                                "Anderson history",
-                      "l2": "inputs larger than L2: 3.4 GB of propagator slices per iteration"},
+                      "l2": "inputs larger than L2: "
+                            f"{sweep_steps * N * (4 if args.precision == 'mixed' else 8) / 1e9:.1f} GB "
+                            "of propagator slices per iteration"},
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
            "free_energy": last["free_energy"] if last else None}
+    wcell = [solver.w(i) for i in range(len(cfg.fields))] if tri and rank == 0 else None
     solver.close()
+    if tri:
+        # one variable-cell step's stress: FP64 adjoint with sqrt(Ns) checkpoints
+        if rank == 0 and world == 1:
+            from polyswift_plusplus_b200.cell import stress
+            t0 = time.perf_counter()
+            Fc, g = stress(cfg, wcell, 0, local)
+            out["cell_step"] = {"seconds": time.perf_counter() - t0, "F": Fc, "dF_dL_box": list(g),
+                                "what": "dF/dL_box of the current fields by the FP64 adjoint "
+                                        "(forward + backward sweeps, sqrt(Ns) checkpoints)"}
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
     if rank == 0 and world == 1 and args.precision == "mixed" and args.precision_iters > 0:
         out["precision"] = precision_check(args.n, args.precision_iters, local)
     if rank == 0 and world == 1 and args.precision == "mixed" and args.fp64_steps > 0:
