@@ -34,6 +34,7 @@ extern "C" {
 #define PS_MAX_POLYMERS 4
 #define PS_MAX_FIELDS 4
 #define PS_MAX_INTERACTIONS 6
+#define PS_MAX_SOLVENTS 2
 
 /* Status codes: same numbers as the reference's quitPolyswift() codes. */
 enum {
@@ -98,6 +99,12 @@ typedef struct ps_updater_config {
   int anderson_start;      /* plain steps before the history is used        */
 } ps_updater_config;
 
+/* <Solvent name> kind = simpleSolvent (psbase/PsSolvent.cpp:40-60). */
+typedef struct ps_solvent_config {
+  int field;               /* scfield: index of the monomerDens PhysField   */
+  double volfrac;          /* volfrac                                       */
+} ps_solvent_config;
+
 typedef struct ps_config {
   int n[3];                /* numCellsGlobal                                */
   double cell[3];          /* cellSizes (Rg units)                          */
@@ -111,6 +118,11 @@ typedef struct ps_config {
   unsigned long long seed; /* randomSeed (MT19937 init_genrand(seed+rank)) */
   int calc_disorder;       /* History freeEnergy calcDisorder (default 1)   */
   int device;              /* CUDA device ordinal                           */
+  /* <Solvent name> kind = simpleSolvent (pssolvent/PsSimpleSolvent.cpp:86-140):
+   * Q_s = <exp(-w_f / L)>, phi_f += volfrac exp(-w_f / L) / Q_s, F -= volfrac L ln Q_s,
+   * L = length of polymer 0.  Appended at the end so the fields above keep their offsets. */
+  int n_solvents;
+  ps_solvent_config solvents[PS_MAX_SOLVENTS];
 } ps_config;
 
 typedef struct ps_scalars {

@@ -98,6 +98,9 @@ class NpScft:
                 self.avg[f] = self.avg[f] + 1.0 * B.lengthfrac * P.volfrac
                 st.append(block_steps(self.alpha[ip] * B.lengthfrac / B.ds, B.force_block_steps))
             self.steps.append(st)
+        for S in getattr(cfg, "solvents", []):  # PsSimpleSolvent::buildSolvers: addToDensAverage
+            f = cfg.field_index(S.scfield)
+            self.avg[f] = self.avg[f] + S.volfrac
         self.w = [np.zeros(self.shape) for _ in range(self.nf)]
         self.p = np.zeros(self.shape)
         self.phi = [np.zeros(self.shape) for _ in range(self.nf)]
@@ -152,8 +155,18 @@ class NpScft:
             self.phi[f] = self.phi[f] + (1.0 * P.volfrac / self.alpha[ip]) * ((1.0 / Q) * acc)
         return Q, qs
 
+    def solvent(self, S):
+        """PsSimpleSolvent::setPhysFields (pssolvent/PsSimpleSolvent.cpp:86-140)."""
+        f = self.cfg.field_index(S.scfield)
+        wfactor = np.exp(self.w[f] * (-1.0 / self.L0))
+        Q = float(np.sum(wfactor)) / self.N
+        self.phi[f] = self.phi[f] + wfactor * (S.volfrac / Q)
+        return Q
+
     def iterate(self):
         self.phi = [np.zeros(self.shape) for _ in range(self.nf)]
+        solvents = list(getattr(self.cfg, "solvents", []))
+        Qsol = [self.solvent(S) for S in solvents]
         Qs = [self.polymer(ip)[0] for ip in range(len(self.cfg.polymers))]
         nf = self.nf
         dh = []
@@ -181,6 +194,7 @@ class NpScft:
             pr = (1.0 / 3.0) * pr
         self.p = pr - np.sum(pr) / self.N
         fe = -sum(P.volfrac * math.log(Q) / a for P, Q, a in zip(self.cfg.polymers, Qs, self.alpha))
+        fe -= sum(S.volfrac * math.log(Q) * self.L0 for S, Q in zip(solvents, Qsol))
         dens = -sum(self.phi[i] * self.w[i] for i in range(nf))
         for it, (a, b) in enumerate(self.ia):
             dens = dens + self.chin[it] * (self.phi[a] * self.phi[b] - self.avg[a] * self.avg[b])

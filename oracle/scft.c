@@ -90,6 +90,7 @@ struct oracle_state {
   int npol;
   opolymer pol[PS_MAX_POLYMERS];
   double scale_length;
+  double solv_q[PS_MAX_SOLVENTS];  /* simpleSolvent bigQ of the last iteration */
   mt_state rng;
   long long iter;
   /* scratch */
@@ -299,9 +300,25 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
     }
     for (int ib = 0; ib < P->nb; ++ib) build_k2(s, &P->b[ib], P->b[ib].k2);
   }
+  if (rc == PS_OK && (cfg->n_solvents < 0 || cfg->n_solvents > PS_MAX_SOLVENTS)) {
+    snprintf(err, errlen, "n_solvents out of range");
+    rc = PS_ATTRIB_ERR;
+  }
+  for (int is = 0; is < cfg->n_solvents && rc == PS_OK; ++is) {
+    const ps_solvent_config* S = &cfg->solvents[is];
+    if (S->field < 0 || S->field >= s->nf) {
+      snprintf(err, errlen, "solvent %d: scfield out of range", is);
+      rc = PS_ATTRIB_ERR;
+      break;
+    }
+    /* PsSimpleSolvent::buildSolvers: addToDensAverage(volfrac) */
+    s->dens_avg[S->field] = s->dens_avg[S->field] + S->volfrac;
+  }
   if (rc == PS_OK) {
-    /* sum of volume fractions (psphysf/PsPhysFieldHldr.cpp check) */
+    /* sum of volume fractions of polymers and solvents
+       (psphysf/PsPhysFieldHldr.cpp:190-257) */
     double vt = 0.0;
+    for (int is = 0; is < cfg->n_solvents; ++is) vt += cfg->solvents[is].volfrac;
     for (int ip = 0; ip < s->npol; ++ip) vt += cfg->polymers[ip].volfrac;
     if (fabs(vt - 1.0) > 0.00001) {
       snprintf(err, errlen, "sum of volume fractions %g != 1", vt);
@@ -653,6 +670,28 @@ static double rebuild_pressure(oracle_state* s) {
   return mean;
 }
 
+/* PsSimpleSolvent::setPhysFields (pssolvent/PsSimpleSolvent.cpp:86-140):
+ * wFactor = exp(-w / L), Q = sum(wFactor) / N, phi += (vf / Q) wFactor. */
+static void solvent_update(oracle_state* s, int is) {
+  const long N = s->N;
+  const ps_solvent_config* S = &s->cfg.solvents[is];
+  const double* w = s->w[S->field];
+  double* wf = s->res;  /* N doubles of scratch */
+  const double negscale = -1.0 / s->scale_length;
+  double tot = 0.0;
+  for (long r = 0; r < N; ++r) {
+    double v = 0.0 + w[r];
+    v = v * negscale;
+    wf[r] = exp(v);
+    tot = tot + wf[r];
+  }
+  const double q = tot / ((double)1 * (double)N);
+  s->solv_q[is] = q;
+  const double f = S->volfrac / q;
+  double* phi = s->phi[S->field];
+  for (long r = 0; r < N; ++r) phi[r] = phi[r] + wf[r] * f;
+}
+
 /* PsPolymerUpdater::calcFeField (pseffhamil/PsPolymerUpdater.cpp:172-226). */
 static void calc_fe(oracle_state* s, double* fe_out, double* fe_nodis_out) {
   const long N = s->N;
@@ -663,6 +702,13 @@ static void calc_fe(oracle_state* s, double* fe_out, double* fe_nodis_out) {
     double logq = log(s->pol[ip].bigq);
     double vf = s->pol[ip].cfg.volfrac;
     double lr = s->pol[ip].length_ratio;
+    sum_tmp = sum_tmp - ((vf * logq) / lr);
+  }
+  /* solvents: length ratio 1 / (length of polymer 0) */
+  for (int is = 0; is < s->cfg.n_solvents; ++is) {
+    double logq = log(s->solv_q[is]);
+    double vf = s->cfg.solvents[is].volfrac;
+    double lr = 1.0 / s->scale_length;
     sum_tmp = sum_tmp - ((vf * logq) / lr);
   }
   double tot = 0.0, tot_nd = 0.0;
@@ -847,6 +893,8 @@ int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
     const double t_begin = now_s();
     s->t_sweeps = 0.0;
     for (int i = 0; i < s->nf; ++i) memset(s->phi[i], 0, sizeof(double) * (size_t)N);
+    /* PsDomain::update: solvents, then polymers (pstrol/PsDomain.cpp:359-362) */
+    for (int is = 0; is < s->cfg.n_solvents; ++is) solvent_update(s, is);
     for (int ip = 0; ip < s->npol; ++ip) {
       int rc = polymer_update(s, &s->pol[ip]);
       if (rc != PS_OK) return rc;

@@ -14,6 +14,7 @@ PS_MAX_JOINS = 4
 PS_MAX_POLYMERS = 4
 PS_MAX_FIELDS = 4
 PS_MAX_INTERACTIONS = 6
+PS_MAX_SOLVENTS = 2
 
 PS_OK = 0
 PS_ATTRIB_ERR = 3
@@ -57,6 +58,10 @@ class ps_updater_config(C.Structure):
                 ("anderson_start", C.c_int)]
 
 
+class ps_solvent_config(C.Structure):
+    _fields_ = [("field", C.c_int), ("volfrac", C.c_double)]
+
+
 class ps_config(C.Structure):
     _fields_ = [("n", C.c_int * 3), ("cell", C.c_double * 3), ("precision", C.c_int),
                 ("n_fields", C.c_int), ("n_polymers", C.c_int),
@@ -64,7 +69,8 @@ class ps_config(C.Structure):
                 ("n_interactions", C.c_int),
                 ("interactions", ps_interaction_config * PS_MAX_INTERACTIONS),
                 ("updater", ps_updater_config), ("seed", C.c_ulonglong),
-                ("calc_disorder", C.c_int), ("device", C.c_int)]
+                ("calc_disorder", C.c_int), ("device", C.c_int),
+                ("n_solvents", C.c_int), ("solvents", ps_solvent_config * PS_MAX_SOLVENTS)]
 
 
 class ps_scalars(C.Structure):

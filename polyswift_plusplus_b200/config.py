@@ -66,6 +66,15 @@ class Interaction:
 
 
 @dataclass
+class Solvent:
+    """<Solvent name> kind = simpleSolvent (psbase/PsSolvent.cpp:40-60)."""
+    name: str
+    scfield: str
+    volfrac: float
+    kind: str = "simpleSolvent"
+
+
+@dataclass
 class Updater:
     name: str = "updater"
     kind: str = "steepestDescent"
@@ -88,6 +97,7 @@ class ScftConfig:
     precision: str = "fp64"           # "fp64" or "mixed"
     nsteps: int = 1
     device: int = 0
+    solvents: list = field(default_factory=list)  # Solvent entries
 
     @property
     def n_total(self) -> int:
@@ -161,6 +171,14 @@ class ScftConfig:
         c.updater.anderson_depth = int(U.anderson_depth)
         c.updater.anderson_mix = float(U.anderson_mix)
         c.updater.anderson_start = int(U.anderson_start)
+        if len(self.solvents) > A.PS_MAX_SOLVENTS:
+            raise ValueError("too many solvents")
+        c.n_solvents = len(self.solvents)
+        for i_s, S in enumerate(self.solvents):
+            if S.kind not in ("simpleSolvent", "simpleSolventGPU"):
+                raise ValueError(f"Solvent kind {S.kind!r} is not on the device path")
+            c.solvents[i_s].field = self.field_index(S.scfield)
+            c.solvents[i_s].volfrac = float(S.volfrac)
         c.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
         c.calc_disorder = 1
         c.device = int(self.device)
@@ -291,6 +309,14 @@ def config_from_text(text: str) -> ScftConfig:
                                 force_block_steps=fbs in (1, "on", "true", "1")))
         polymers.append(Polymer(name=pname, volfrac=float(pa.get("volfrac", 1.0)),
                                 length=int(pa.get("length", 1)), blocks=blocks))
+    solvents = []
+    for sname, snode in _find(root, "Solvent"):
+        sa = snode["attrs"]
+        kind = str(sa.get("kind", "simpleSolvent"))
+        if kind not in ("simpleSolvent", "simpleSolventGPU"):
+            raise InputError(f"Solvent kind {kind!r} is not on the device path")
+        solvents.append(Solvent(name=sname, scfield=str(sa["scfield"]),
+                                volfrac=float(sa.get("volfrac", 0.0)), kind=kind))
     interactions, updater = [], None
     for hname, hnode in _find(root, "EffHamil"):
         for iname, inode in _find(hnode, "Interaction"):
@@ -322,7 +348,7 @@ def config_from_text(text: str) -> ScftConfig:
     return ScftConfig(n=n, cell=cell, fields=fields, polymers=polymers, interactions=interactions,
                       updater=updater, seed=int(ra.get("randomSeed", 0)),
                       precision=str(ra.get("precision", "fp64")), nsteps=int(ra.get("nsteps", 1)),
-                      device=int(ra.get("device", 0)))
+                      device=int(ra.get("device", 0)), solvents=solvents)
 
 
 def config_from_file(path: str | Path) -> ScftConfig:

@@ -554,8 +554,8 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
     a->err = "the adjoint runs in FP64 (precision must be PS_PREC_FP64)";
     return PS_ATTRIB_ERR;
   }
-  if (cfg->n_polymers != 1) {
-    a->err = "the adjoint takes one polymer (a linear block copolymer melt)";
+  if (cfg->n_polymers != 1 || cfg->n_solvents != 0) {
+    a->err = "the adjoint takes one polymer (a linear block copolymer melt) and no solvent";
     return PS_INPUT_ERR;
   }
   a->h = new ps_handle();

@@ -305,6 +305,13 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
   auto slice = [&](int sweep, int idx) -> const T* {
     return B.slices[h->sweeps[sweep].storage] + (size_t)idx * N;
   };
+  // solvents before polymers (PsDomain::update, pstrol/PsDomain.cpp:359-362)
+  for (int is = 0; is < h->cfg.n_solvents; ++is) {
+    const ps_solvent_config& S = h->cfg.solvents[is];
+    PS_CUDA(h, launch_solvent(h->d_w + (size_t)S.field * N, -1.0 / h->fm.scale_len, S.volfrac, N, is,
+                              h->d_qpart, h->d_sc, h->d_phi + (size_t)S.field * N, h->st));
+    *nlaunch += 3;
+  }
   for (int ip = 0; ip < h->cfg.n_polymers; ++ip) {
     const BlockMap& b0 = h->blocks[ip][0];
     PS_CUDA(h, launch_dot_partials<T>(slice(b0.sweep_head, b0.off_head),
@@ -551,8 +558,25 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
       h->blocks[ip].push_back(bm);
     }
   }
+  // simpleSolvent: density average and volume fraction (pssolvent/PsSimpleSolvent.cpp:56-80,
+  // psphysf/PsPhysFieldHldr.cpp:190-257)
+  if (c.n_solvents < 0 || c.n_solvents > PS_MAX_SOLVENTS) {
+    h->err = "n_solvents out of range";
+    return PS_ATTRIB_ERR;
+  }
+  for (int is = 0; is < c.n_solvents; ++is) {
+    const ps_solvent_config& S = c.solvents[is];
+    if (S.field < 0 || S.field >= h->nf) {
+      h->err = "solvent " + std::to_string(is) + ": scfield out of range";
+      return PS_ATTRIB_ERR;
+    }
+    dens_avg[S.field] = dens_avg[S.field] + S.volfrac;
+  }
+  double vsolv = 0.0;
+  for (int is = 0; is < c.n_solvents; ++is) vsolv += c.solvents[is].volfrac;
+  vtot = vsolv + vtot;
   if (fabs(vtot - 1.0) > 0.00001) {
-    h->err = "sum of polymer volume fractions != 1";
+    h->err = "sum of polymer and solvent volume fractions != 1";
     return PS_INPUT_ERR;
   }
   // Sweeps
@@ -660,6 +684,9 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
     fm.vf[ip] = c.polymers[ip].volfrac;
     fm.alpha[ip] = h->alpha[ip];
   }
+  fm.nsolv = c.n_solvents;
+  for (int is = 0; is < c.n_solvents; ++is) fm.solv_vf[is] = c.solvents[is].volfrac;
+  fm.scale_len = scale_len;
   fm.N = h->N;
 
   // Device

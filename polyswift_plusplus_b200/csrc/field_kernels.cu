@@ -142,6 +142,53 @@ cudaError_t launch_finalize_q(const double* partials, double N, int ip, DevScala
 }
 
 // ---------------------------------------------------------------------------
+// simpleSolvent: wFactor = exp(-w / L), Q = sum(wFactor) / N, phi += (vf / Q) wFactor
+// (pssolvent/PsSimpleSolvent.cpp:86-140).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double solvent_factor(double w, double neg_inv_len) {
+  double v = 0.0 + w;
+  v = v * neg_inv_len;
+  return exp(v);
+}
+
+__global__ void solvent_partials_kernel(const double* __restrict__ w, double neg_inv_len, long long N,
+                                        double* __restrict__ partials) {
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < N;
+       i += (long long)kRedBlocks * kRedThreads)
+    v[0] += solvent_factor(w[i], neg_inv_len);
+  block_reduce_write<1>(v, 0u, partials + blockIdx.x);
+}
+
+__global__ void solvent_finalize_kernel(const double* partials, double N, int is, DevScalars* sc) {
+  const double tot = cta_reduce_partials(partials, kRedBlocks, 1, false);
+  if (threadIdx.x == 0) {
+    const double q = tot / (1.0 * N);
+    sc->solv_q[is] = q;
+    if (q != q) sc->error_flags |= 1;
+  }
+}
+
+__global__ void solvent_density_kernel(const double* __restrict__ w, double neg_inv_len, double volfrac,
+                                       long long N, int is, const DevScalars* __restrict__ sc,
+                                       double* __restrict__ phi) {
+  const double f = volfrac / sc->solv_q[is];
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x)
+    phi[r] = phi[r] + solvent_factor(w[r], neg_inv_len) * f;
+}
+
+cudaError_t launch_solvent(const double* w, double neg_inv_len, double volfrac, long long N, int is,
+                           double* partials, DevScalars* sc, double* phi, cudaStream_t st) {
+  solvent_partials_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, neg_inv_len, N, partials);
+  solvent_finalize_kernel<<<1, kRedThreads, 0, st>>>(partials, (double)N, is, sc);
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  solvent_density_kernel<<<blocks, 256, 0, st>>>(w, neg_inv_len, volfrac, N, is, sc, phi);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Contour quadrature (pspolymer/PsBlock.cpp:255-380) and density update
 // (pspolymer/PsBlock.cpp:153-196): extended Simpson with the reference's
 // 0.33333 factor, trapezoid on the last interval for an even point count.
@@ -550,6 +597,10 @@ __global__ void update_finalize_kernel(FieldModel fm, const double* __restrict__
     for (int ip = 0; ip < fm.npol; ++ip) {
       const double logq = sc->log_q[ip];
       sum_tmp = sum_tmp - ((fm.vf[ip] * logq) / fm.alpha[ip]);
+    }
+    for (int is = 0; is < fm.nsolv; ++is) {
+      const double logq = log(sc->solv_q[is]);
+      sum_tmp = sum_tmp - ((fm.solv_vf[is] * logq) / (1.0 / fm.scale_len));
     }
     sc->pressure_mean = psum / ((double)fm.N * 1.0);
     sc->free_energy = sum_tmp + fe;

@@ -29,6 +29,7 @@ struct DevScalars {
   int am_use;
   double am_c[64];      // solved coefficients
   double am_mix;        // mixing applied to the combined residual
+  double solv_q[PS_MAX_SOLVENTS];  // simpleSolvent bigQ
 };
 
 // Static description of the field model handed to the update kernels.
@@ -43,6 +44,9 @@ struct FieldModel {
   int npol;
   double vf[PS_MAX_POLYMERS];
   double alpha[PS_MAX_POLYMERS];
+  int nsolv;
+  double solv_vf[PS_MAX_SOLVENTS];
+  double scale_len;  // length of polymer 0 (a solvent's length ratio is 1 / scale_len)
   long long N;
 };
 
@@ -72,6 +76,11 @@ cudaError_t launch_quadrature(const T* qs, const T* qts, int steps, long long N,
                               cudaStream_t st);
 
 cudaError_t launch_zero(double* p, long long n, cudaStream_t st);
+
+// simpleSolvent (pssolvent/PsSimpleSolvent.cpp:86-140): Q = <exp(-w/L)> into
+// sc->solv_q[is], then phi += (volfrac / Q) exp(-w/L).
+cudaError_t launch_solvent(const double* w, double neg_inv_len, double volfrac, long long N, int is,
+                           double* partials, DevScalars* sc, double* phi, cudaStream_t st);
 
 // Steepest-descent update, pressure rebuild and free-energy partial sums.
 cudaError_t launch_sd_update(const FieldModel& fm, const FieldPtrs& fp, double* partials,

@@ -137,3 +137,54 @@ setupPS(NX, NX, NX, DX, DX, DX, "'off'")
     pc = cfg.to_ps_config()
     assert pc.polymers[0].blocks[1].n_head == 1 and pc.polymers[0].blocks[1].head_joined[0] == 0
     assert pc.interactions[0].chi == pytest.approx(0.12)
+
+
+def test_config_parser_reads_simple_solvent():
+    """<Solvent name> kind = simpleSolvent (psbase/PsSolvent.cpp:40-60) with its
+    scfield and volfrac reaches ps_config.solvents."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
+<EffHamil h>
+  <Updater u>
+    kind = steepestDescent
+    relaxlambdas = [0.1 0.05]
+  </Updater>
+  <Interaction AB>
+    kind = flory
+    chi = 0.2
+    scfields = [A B]
+  </Interaction>
+</EffHamil>
+<PhysField A>
+  kind = monomerDens
+</PhysField>
+<PhysField B>
+  kind = monomerDens
+</PhysField>
+<PhysField defaultPressure>
+  kind = constraint
+</PhysField>
+<Polymer homoB>
+  kind = blockCopolymer
+  volfrac = 0.7
+  length = 100
+  <Block b>
+    scfield = B
+    ds = 0.01
+    lengthfrac = 1.0
+    headjoined = [freeEnd]
+    tailjoined = [freeEnd]
+  </Block>
+</Polymer>
+<Solvent solvA>
+  kind = simpleSolvent
+  scfield = A
+  volfrac = 0.3
+</Solvent>
+"""
+    cfg = config_from_text(text)
+    assert len(cfg.solvents) == 1 and cfg.solvents[0].scfield == "A"
+    pc = cfg.to_ps_config()
+    assert pc.n_solvents == 1 and pc.solvents[0].field == 0
+    assert pc.solvents[0].volfrac == pytest.approx(0.3)

@@ -429,3 +429,41 @@ def test_128_square_plane_variants_match_oracle(gpu, oracle_lib, variant):
         g.update(1)
         hg.append(g.scalars())
     assert_parity(cfg, g, o, hg, ho)
+
+
+@pytest.mark.parametrize("variant", [0, 11])
+def test_fp64_solvent_blend_parity(gpu, oracle_lib, variant):
+    """Diblock + simpleSolvent on the A field (pssolvent/PsSimpleSolvent.cpp:86-140):
+    the solvent's Q and density on the device, and its -vf L ln Q term in F, against the
+    oracle at 1e-10."""
+    import dataclasses
+    from polyswift_plusplus_b200.config import Solvent
+    cfg, w = W.diblock32(n=16)
+    cfg.polymers[0].volfrac = 0.8
+    cfg = dataclasses.replace(cfg, solvents=[Solvent("solv", "A", 0.2)])
+    g = ScftSolver(cfg)
+    g.set_variant(variant)
+    g.restore(w)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(8)
+    hg = []
+    for _ in range(8):
+        g.update(1)
+        hg.append(g.scalars())
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_mixed_solvent_blend_close_to_fp64(gpu):
+    import dataclasses
+    from polyswift_plusplus_b200.config import Solvent
+    out = []
+    for prec in ("fp64", "mixed"):
+        cfg, w = W.diblock32(n=16, precision=prec)
+        cfg.polymers[0].volfrac = 0.8
+        cfg = dataclasses.replace(cfg, solvents=[Solvent("solv", "B", 0.2)])
+        g = ScftSolver(cfg)
+        g.restore(w)
+        g.update(20)
+        out.append(g.scalars()["free_energy"])
+    assert abs(out[1] - out[0]) < 1e-5 * max(abs(out[0]), 1.0)
