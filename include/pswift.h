@@ -217,6 +217,28 @@ int ps_gpu_set_precision(ps_handle* h, int precision);
 int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
                         double* bytes_per_iter, long long* steps_per_iter);
 
+/* --- Spectral filter updater: <Updater name> kind = simpleSpecFilter
+ * (pseffhamil/PsSimpleSpecFilter.cpp:75-140, pseffhamil/PsSpecFilterUpdater.cpp:155-250;
+ * schedule psbase/PsUpdater.cpp:60-206).  After each iteration t (0-based) with
+ * apply_start <= t <= apply_end (apply_end < 0: no end) and (t - apply_start) %
+ * apply_frequency == 0, every listed conjugate field w loses its mean and is
+ * filtered: w = Re(IFFT(mask FFT(w))) / N with mask = filter_strength where
+ * |FFT(w)|^2 < cutoff_factor * max |FFT(w)|^2 and 1 elsewhere.  cutoff_factor
+ * <= 0 leaves the fields alone.  FP64 whatever the sweep precision.  Passing
+ * NULL removes the filter; not allowed on a batch instance. */
+typedef struct ps_filter_config {
+  int n_fields;              /* updatefields                                  */
+  int fields[PS_MAX_FIELDS]; /* monomerDens PhysField indices                 */
+  double cutoff_factor;      /* cutoffFactor                                  */
+  double filter_strength;    /* filterStrength                                */
+  long long apply_start;     /* applyStart                                    */
+  long long apply_frequency; /* applyFrequency                                */
+  long long apply_end;       /* applyEnd (< 0: until the end of the run)      */
+} ps_filter_config;
+int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* filter);
+/* Apply the filter once now, outside its schedule. */
+int ps_gpu_apply_spectral_filter(ps_handle* h);
+
 /* --- Batched instances (no reference counterpart: the reference runs one
  * PsDomain per process, polyswift/polyswift/polyswift.cxx:544-588) ----------
  * ps_gpu_batch_create builds `count` independent instances on one device

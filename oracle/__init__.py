@@ -40,6 +40,9 @@ def lib() -> C.CDLL:
         L.oracle_block_steps.argtypes = [vp, C.c_int, C.c_int]
         L.oracle_init_random.argtypes = [vp]
         L.oracle_set_field.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.oracle_set_filter.restype = C.c_int
+        L.oracle_set_filter.argtypes = [vp, C.POINTER(A.ps_filter_config)]
+        L.oracle_apply_filter.argtypes = [vp]
         L.oracle_get_field.argtypes = [vp, C.c_int, C.c_int, vp]
         L.oracle_iterate.restype = C.c_int
         L.oracle_iterate.argtypes = [vp, C.c_int, C.POINTER(A.ps_scalars)]
@@ -109,6 +112,8 @@ class Oracle:
         self._h = h
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
+        if getattr(cfg, "spec_filter", None) is not None:
+            self.set_spectral_filter(cfg.spec_filter)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -131,6 +136,16 @@ class Oracle:
         for i, x in enumerate(w):
             self.set_field(A.PS_FIELD_W, i, x)
         self.set_field(A.PS_FIELD_PRES, 0, np.zeros(self.N) if p is None else p)
+
+    def set_spectral_filter(self, spec_filter):
+        """spec_filter: a config.SpecFilter, or None to remove the updater."""
+        self._fcfg = spec_filter.to_ps(self.cfg) if spec_filter is not None else None
+        rc = lib().oracle_set_filter(self._h, C.byref(self._fcfg) if self._fcfg is not None else None)
+        if rc != A.PS_OK:
+            raise A.PsError(rc, "bad spectral filter")
+
+    def apply_spectral_filter(self):
+        lib().oracle_apply_filter(self._h)
 
     def set_field(self, which, index, data):
         x = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)

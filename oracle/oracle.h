@@ -41,6 +41,8 @@ void oracle_scaled_fft_pair(const int n[3], const double* data, const double* kd
 /* Build a whole SCFT instance (same checks as the device path). */
 int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errlen);
 void oracle_destroy(oracle_state* s);
+int oracle_set_filter(oracle_state* s, const ps_filter_config* f);
+void oracle_apply_filter(oracle_state* s);
 int oracle_block_steps(const oracle_state* s, int polymer, int block);
 void oracle_init_random(oracle_state* s);
 void oracle_set_field(oracle_state* s, int which, int index, const double* data);

@@ -91,6 +91,9 @@ struct oracle_state {
   opolymer pol[PS_MAX_POLYMERS];
   double scale_length;
   double solv_q[PS_MAX_SOLVENTS];  /* simpleSolvent bigQ of the last iteration */
+  int has_filter;                  /* simpleSpecFilter updater after the field update */
+  ps_filter_config fcfg;
+  double* fpow;                    /* N: |FFT(w)|^2, then the mask */
   mt_state rng;
   long long iter;
   /* scratch */
@@ -360,7 +363,7 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
 void oracle_destroy(oracle_state* s) {
   if (!s) return;
   for (int i = 0; i < PS_MAX_FIELDS; ++i) { free(s->w[i]); free(s->phi[i]); free(s->dh[i]); }
-  free(s->p); free(s->cwork); free(s->qw); free(s->res);
+  free(s->p); free(s->cwork); free(s->qw); free(s->res); free(s->fpow);
   for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip)
     for (int ib = 0; ib < PS_MAX_BLOCKS; ++ib) {
       oblock* B = &s->pol[ip].b[ib];
@@ -692,6 +695,54 @@ static void solvent_update(oracle_state* s, int is) {
   for (long r = 0; r < N; ++r) phi[r] = phi[r] + wf[r] * f;
 }
 
+/* PsSimpleSpecFilter::update / applyFilter (pseffhamil/PsSimpleSpecFilter.cpp:75-140),
+ * PsSpecFilterUpdater::subtractAverage and findMaxVal (pseffhamil/PsSpecFilterUpdater.cpp:
+ * 180-250), scaledFFTPair and scaleFFT = 1/N. */
+static void filter_apply(oracle_state* s) {
+  const ps_filter_config* F = &s->fcfg;
+  if (F->cutoff_factor <= 0.0) return;
+  const long N = s->N;
+  double* c = s->cwork;
+  double* pw = s->fpow;
+  for (int i = 0; i < F->n_fields; ++i) {
+    double* w = s->w[F->fields[i]];
+    double sum = 0.0;
+    for (long r = 0; r < N; ++r) sum = sum + w[r];
+    const double wtot = -1.0 * (sum / ((double)1 * (double)N));
+    for (long r = 0; r < N; ++r) w[r] = w[r] + wtot;
+    for (long r = 0; r < N; ++r) { c[2 * r] = w[r]; c[2 * r + 1] = 0.0; }
+    oracle_fftnd_inplace(s->n, c, -1);
+    double mx = -1000000.00;
+    for (long r = 0; r < N; ++r) {
+      pw[r] = (c[2 * r] * c[2 * r]) + (c[2 * r + 1] * c[2 * r + 1]);
+      if (pw[r] > mx) mx = pw[r];
+    }
+    const double cut = F->cutoff_factor * mx;
+    for (long r = 0; r < N; ++r) pw[r] = (pw[r] < cut) ? F->filter_strength : 1.0;
+    oracle_scaled_pair_buf(s->n, w, pw, s->res, c);
+    const double scale = 1.0 / (double)N;
+    for (long r = 0; r < N; ++r) w[r] = scale * s->res[r];
+  }
+}
+
+int oracle_set_filter(oracle_state* s, const ps_filter_config* f) {
+  if (!f) {
+    s->has_filter = 0;
+    return PS_OK;
+  }
+  if (f->n_fields < 1 || f->n_fields > s->nf || f->apply_frequency < 1) return PS_ATTRIB_ERR;
+  for (int i = 0; i < f->n_fields; ++i)
+    if (f->fields[i] < 0 || f->fields[i] >= s->nf) return PS_ATTRIB_ERR;
+  if (!s->fpow) s->fpow = (double*)xcalloc((size_t)s->N, sizeof(double));
+  s->fcfg = *f;
+  s->has_filter = 1;
+  return PS_OK;
+}
+
+void oracle_apply_filter(oracle_state* s) {
+  if (s->has_filter) filter_apply(s);
+}
+
 /* PsPolymerUpdater::calcFeField (pseffhamil/PsPolymerUpdater.cpp:172-226). */
 static void calc_fe(oracle_state* s, double* fe_out, double* fe_nodis_out) {
   const long N = s->N;
@@ -910,6 +961,13 @@ int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
     }
     sc.max_incomp = mx;
     update_fields(s, &sc);
+    if (s->has_filter) {  /* PsUpdater::update schedule (psbase/PsUpdater.cpp:180-206) */
+      const long long t = s->iter;
+      const ps_filter_config* F = &s->fcfg;
+      if (t >= F->apply_start && (F->apply_end < 0 || t <= F->apply_end) &&
+          (t - F->apply_start) % F->apply_frequency == 0)
+        filter_apply(s);
+    }
     s->t_total = now_s() - t_begin;
     s->iter++;
     sc.iteration = s->iter;

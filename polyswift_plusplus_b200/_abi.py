@@ -73,6 +73,13 @@ class ps_config(C.Structure):
                 ("n_solvents", C.c_int), ("solvents", ps_solvent_config * PS_MAX_SOLVENTS)]
 
 
+class ps_filter_config(C.Structure):
+    _fields_ = [("n_fields", C.c_int), ("fields", C.c_int * PS_MAX_FIELDS),
+                ("cutoff_factor", C.c_double), ("filter_strength", C.c_double),
+                ("apply_start", C.c_longlong), ("apply_frequency", C.c_longlong),
+                ("apply_end", C.c_longlong)]
+
+
 class ps_scalars(C.Structure):
     _fields_ = [("free_energy", C.c_double), ("free_energy_nodis", C.c_double),
                 ("log_q", C.c_double * PS_MAX_POLYMERS), ("q", C.c_double * PS_MAX_POLYMERS),
@@ -113,6 +120,8 @@ SIGNATURES = {
     "ps_gpu_set_variant": (C.c_int, [_vp, C.c_int]),
     "ps_gpu_get_variant": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]),
     "ps_gpu_set_precision": (C.c_int, [_vp, C.c_int]),
+    "ps_gpu_set_spectral_filter": (C.c_int, [_vp, C.POINTER(ps_filter_config)]),
+    "ps_gpu_apply_spectral_filter": (C.c_int, [_vp]),
     "ps_gpu_sweep_timing": (C.c_int, [_vp, _dbl_p, C.c_int, C.POINTER(C.c_int), _dbl_p,
                                       C.POINTER(C.c_longlong)]),
     "ps_gpu_batch_create": (C.c_int, [C.POINTER(ps_config), C.c_int, C.POINTER(_vp)]),

@@ -75,6 +75,31 @@ class Solvent:
 
 
 @dataclass
+class SpecFilter:
+    """<Updater name> kind = simpleSpecFilter (pseffhamil/PsSpecFilterUpdater.cpp:56-90,
+    psbase/PsUpdater.cpp:60-120)."""
+    name: str = "filter"
+    updatefields: list = field(default_factory=list)
+    cutoff_factor: float = 0.0
+    filter_strength: float = 0.0
+    apply_start: int = 0
+    apply_frequency: int = 1
+    apply_end: int = -1
+
+    def to_ps(self, cfg: "ScftConfig") -> A.ps_filter_config:
+        f = A.ps_filter_config()
+        f.n_fields = len(self.updatefields)
+        for i, name in enumerate(self.updatefields):
+            f.fields[i] = cfg.field_index(name)
+        f.cutoff_factor = float(self.cutoff_factor)
+        f.filter_strength = float(self.filter_strength)
+        f.apply_start = int(self.apply_start)
+        f.apply_frequency = int(self.apply_frequency)
+        f.apply_end = int(self.apply_end)
+        return f
+
+
+@dataclass
 class Updater:
     name: str = "updater"
     kind: str = "steepestDescent"
@@ -98,6 +123,7 @@ class ScftConfig:
     nsteps: int = 1
     device: int = 0
     solvents: list = field(default_factory=list)  # Solvent entries
+    spec_filter: "SpecFilter | None" = None       # simpleSpecFilter updater
 
     @property
     def n_total(self) -> int:
@@ -317,7 +343,7 @@ def config_from_text(text: str) -> ScftConfig:
             raise InputError(f"Solvent kind {kind!r} is not on the device path")
         solvents.append(Solvent(name=sname, scfield=str(sa["scfield"]),
                                 volfrac=float(sa.get("volfrac", 0.0)), kind=kind))
-    interactions, updater = [], None
+    interactions, updater, spec_filter = [], None, None
     for hname, hnode in _find(root, "EffHamil"):
         for iname, inode in _find(hnode, "Interaction"):
             ia = inode["attrs"]
@@ -326,6 +352,18 @@ def config_from_text(text: str) -> ScftConfig:
             interactions.append(Interaction(name=iname, chi=float(ia.get("chi", 0.01)),
                                             scfields=[str(x) for x in ia["scfields"]]))
         ups = _find(hnode, "Updater")
+        filters = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) == "simpleSpecFilter"]
+        ups = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) != "simpleSpecFilter"]
+        if filters:
+            fname, fnode = filters[0]
+            fa = fnode["attrs"]
+            upf = fa.get("updatefields", [])
+            spec_filter = SpecFilter(name=fname, updatefields=[str(x) for x in (upf if isinstance(upf, list) else [upf])],
+                                     cutoff_factor=float(fa.get("cutoffFactor", 0.0)),
+                                     filter_strength=float(fa.get("filterStrength", 0.0)),
+                                     apply_start=int(fa.get("applyStart", 0)),
+                                     apply_frequency=int(fa.get("applyFrequency", 1)),
+                                     apply_end=int(fa.get("applyEnd", -1)))
         if ups:
             uname, unode = ups[0]
             ua = unode["attrs"]
@@ -348,7 +386,7 @@ def config_from_text(text: str) -> ScftConfig:
     return ScftConfig(n=n, cell=cell, fields=fields, polymers=polymers, interactions=interactions,
                       updater=updater, seed=int(ra.get("randomSeed", 0)),
                       precision=str(ra.get("precision", "fp64")), nsteps=int(ra.get("nsteps", 1)),
-                      device=int(ra.get("device", 0)), solvents=solvents)
+                      device=int(ra.get("device", 0)), solvents=solvents, spec_filter=spec_filter)
 
 
 def config_from_file(path: str | Path) -> ScftConfig:

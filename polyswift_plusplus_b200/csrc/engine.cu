@@ -448,6 +448,7 @@ template <typename T> static void free_buffers(Buffers<T>& B) {
 }
 
 static void free_all(ps_handle* h) {
+  filter_free(h);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   auto f = [](void* p) { if (p) cudaFree(p); };
@@ -834,6 +835,11 @@ static int iterate_impl(ps_handle* h, int n) {
         h->timing_count++;
       }
       PS_CUDA(h, cudaGraphLaunch(h->gexec, h->st));
+    }
+    if (h->filter) {
+      // updaterSequence order: the filter runs after the field updater of the same step
+      int rc = filter_after_iteration(h, h->iterations);
+      if (rc) return rc;
     }
     h->iterations++;
   }

@@ -115,6 +115,7 @@ struct ps_handle {
   bool xy_ok = false;  // the row + x-y plane design exists for this grid
   bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
   bool no_slices = false; // tables only, no slice storage (the adjoint keeps its own)
+  void* filter = nullptr;  // spectral filter updater (filter.cu), or nullptr
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
@@ -151,6 +152,10 @@ namespace psb {
 // with h->no_slices set beforehand no propagator slice storage is allocated.
 int engine_create(ps_handle* h, const ps_config* cfg);
 void engine_free(ps_handle* h);
+// Spectral filter updater (filter.cu): applied after iteration `step` (0-based)
+// when its schedule says so; freed with the handle.
+int filter_after_iteration(ps_handle* h, long long step);
+void filter_free(ps_handle* h);
 int engine_pre(ps_handle* h, long long* nlaunch);
 int engine_post(ps_handle* h, long long* nlaunch);
 // Host-side random-number bookkeeping owed before each iteration.

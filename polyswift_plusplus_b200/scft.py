@@ -34,6 +34,8 @@ class ScftSolver:
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
         self.t = 0
+        if self._owned and getattr(cfg, "spec_filter", None) is not None:
+            self.set_spectral_filter(cfg.spec_filter)
 
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -143,6 +145,17 @@ class ScftSolver:
     def set_variant(self, variant: int) -> None:
         """Force a kernel variant (0..15) or re-enable autotuning (-1)."""
         self._check(self._lib.ps_gpu_set_variant(self._h, int(variant)))
+
+    def set_spectral_filter(self, spec_filter) -> None:
+        """Install a simpleSpecFilter updater (config.SpecFilter) or remove it (None)."""
+        if spec_filter is None:
+            self._check(self._lib.ps_gpu_set_spectral_filter(self._h, None))
+            return
+        self._fcfg = spec_filter.to_ps(self.cfg)
+        self._check(self._lib.ps_gpu_set_spectral_filter(self._h, C.byref(self._fcfg)))
+
+    def apply_spectral_filter(self) -> None:
+        self._check(self._lib.ps_gpu_apply_spectral_filter(self._h))
 
     def set_precision(self, precision: str) -> None:
         """Switch the sweeps to "fp64" or "mixed" between iterations; fields and

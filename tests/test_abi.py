@@ -223,3 +223,71 @@ def test_dump_restore_round_trip_on_host(tmp_path):
     for which in a.f:
         for x, y in zip(a.f[which], b.f[which]):
             assert np.array_equal(x, y)
+
+
+def test_config_parser_reads_simple_spec_filter():
+    """<Updater name> kind = simpleSpecFilter (pseffhamil/PsSpecFilterUpdater.cpp:55-90 and
+    psbase/PsUpdater.cpp:55-110) beside the field updater."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
+<EffHamil h>
+  <Updater u>
+    kind = steepestDescent
+    relaxlambdas = [0.1 0.05]
+  </Updater>
+  <Updater filt>
+    kind = simpleSpecFilter
+    updatefields = [B A]
+    cutoffFactor = 0.02
+    filterStrength = 0.1
+    applyStart = 5
+    applyFrequency = 10
+    applyEnd = 200
+    fftKind = fftw3
+  </Updater>
+  <Interaction AB>
+    kind = flory
+    chi = 0.2
+    scfields = [A B]
+  </Interaction>
+</EffHamil>
+<PhysField A>
+  kind = monomerDens
+</PhysField>
+<PhysField B>
+  kind = monomerDens
+</PhysField>
+<PhysField defaultPressure>
+  kind = constraint
+</PhysField>
+<Polymer di>
+  kind = blockCopolymer
+  volfrac = 1.0
+  length = 100
+  <Block a>
+    kind = flexPseudoSpec
+    scfield = A
+    ds = 0.05
+    lengthfrac = 0.3
+    headjoined = [freeEnd]
+    tailjoined = [b]
+  </Block>
+  <Block b>
+    kind = flexPseudoSpec
+    scfield = B
+    ds = 0.05
+    lengthfrac = 0.7
+    headjoined = [a]
+    tailjoined = [freeEnd]
+  </Block>
+</Polymer>
+"""
+    cfg = config_from_text(text)
+    assert cfg.updater.kind == "steepestDescent"
+    f = cfg.spec_filter
+    assert f.updatefields == ["B", "A"]
+    assert (f.cutoff_factor, f.filter_strength) == (0.02, 0.1)
+    assert (f.apply_start, f.apply_frequency, f.apply_end) == (5, 10, 200)
+    pf = f.to_ps(cfg)
+    assert pf.n_fields == 2 and list(pf.fields[:2]) == [1, 0]

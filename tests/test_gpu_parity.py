@@ -489,3 +489,79 @@ def test_dump_restore_continues_a_run_exactly(gpu, tmp_path):
         assert np.array_equal(a.w(i), b.w(i))
         assert np.array_equal(a.phi(i), b.phi(i))
     assert a.scalars()["free_energy"] == b.scalars()["free_energy"]
+
+
+def _spec_filter(fields, cutoff, strength, start=0, freq=1, end=-1):
+    from polyswift_plusplus_b200.config import SpecFilter
+    return SpecFilter(updatefields=list(fields), cutoff_factor=cutoff, filter_strength=strength,
+                      apply_start=start, apply_frequency=freq, apply_end=end)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 32, 32), (8, 4, 256), (64, 64, 1),
+                                   (24, 48, 48), (128, 128, 128)])
+def test_spectral_filter_matches_oracle(gpu, oracle_lib, shape):
+    """simpleSpecFilter on the device (fused plane and split-plane FFT paths, a 2-D grid)
+    against the oracle: w after one application at 1e-12 of max|w|."""
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = shape
+    rng = np.random.default_rng(11)
+    w = [rng.standard_normal(cfg.n_total) + 0.3, rng.standard_normal(cfg.n_total) - 0.2]
+    f = _spec_filter(["B", "A"], 0.25, 0.1)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.set_spectral_filter(f)
+    g.apply_spectral_filter()
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.set_spectral_filter(f)
+    o.apply_spectral_filter()
+    for i in range(2):
+        assert rel(g.w(i), o.w(i)) < 1e-12
+        assert abs(g.w(i).mean()) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_spectral_filter_scheduled_in_iterations(gpu, oracle_lib, precision):
+    """The filter runs after the field update of the scheduled steps (PsUpdater::update);
+    FP64 sweeps: parity with the oracle at 1e-10 over the run; mixed sweeps: the filter
+    itself stays FP64 and F tracks the FP64 run."""
+    import dataclasses
+    cfg, w = W.diblock32(n=16, precision=precision)
+    cfg = dataclasses.replace(cfg, spec_filter=_spec_filter(["A", "B"], 0.02, 0.5, start=1, freq=2, end=9))
+    g = ScftSolver(cfg)
+    g.restore(w)
+    if precision == "fp64":
+        cfgo = dataclasses.replace(cfg, precision="fp64")
+        o = O.Oracle(cfgo)
+        o.restore(w)
+        ho = o.update(12)
+        hg = []
+        for _ in range(12):
+            g.update(1)
+            hg.append(g.scalars())
+        assert_parity(cfg, g, o, hg, ho)
+    else:
+        g.update(12)
+        c64, _ = W.diblock32(n=16)
+        c64 = dataclasses.replace(c64, spec_filter=cfg.spec_filter)
+        g64 = ScftSolver(c64)
+        g64.restore(w)
+        g64.update(12)
+        f32, f64 = g.scalars()["free_energy"], g64.scalars()["free_energy"]
+        assert abs(f32 - f64) < 1e-5 * max(abs(f64), 1.0)
+
+
+def test_spectral_filter_errors(gpu):
+    cfg, w = W.diblock32(n=16)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    with pytest.raises(A.PsError):
+        g.apply_spectral_filter()            # none installed
+    with pytest.raises(A.PsError):
+        g.set_spectral_filter(_spec_filter(["A"], 0.1, 0.0, start=5, end=5))
+    with pytest.raises(A.PsError):
+        g.set_spectral_filter(_spec_filter(["A"], 0.1, 0.0, start=0, freq=10, end=10))
+    g.set_spectral_filter(_spec_filter(["A"], 0.1, 0.0))
+    g.set_spectral_filter(None)              # removed again
+    g.update(2)
+    assert math.isfinite(g.scalars()["free_energy"])

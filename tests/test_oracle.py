@@ -223,3 +223,82 @@ def test_volume_fractions_must_include_solvents(oracle_lib):
     with pytest.raises(A.PsError) as e:
         O.Oracle(bad)
     assert e.value.code == A.PS_INPUT_ERR
+
+
+def np_spec_filter(w, shape, cutoff, strength):
+    """numpy restatement of PsSimpleSpecFilter::update (pseffhamil/PsSimpleSpecFilter.cpp:75-140)."""
+    x = np.asarray(w, dtype=np.float64).reshape(shape)
+    x = x - x.mean()
+    k = np.fft.fftn(x)
+    p = np.abs(k) ** 2
+    mask = np.where(p < cutoff * p.max(), strength, 1.0)
+    return np.real(np.fft.ifftn(mask * k)).reshape(-1)
+
+
+def _filter(fields, cutoff, strength, start=0, freq=1, end=-1):
+    from polyswift_plusplus_b200.config import SpecFilter
+    return SpecFilter(updatefields=list(fields), cutoff_factor=cutoff, filter_strength=strength,
+                      apply_start=start, apply_frequency=freq, apply_end=end)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (8, 4, 32), (32, 32, 1), (6, 10, 12)])
+def test_spec_filter_matches_numpy(oracle_lib, shape):
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = shape
+    rng = np.random.default_rng(3)
+    w = [rng.standard_normal(cfg.n_total) + 0.3, rng.standard_normal(cfg.n_total) - 0.2]
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.set_spectral_filter(_filter(["A"], 0.3, 0.25))
+    o.apply_spectral_filter()
+    np.testing.assert_allclose(o.w(0), np_spec_filter(w[0], shape, 0.3, 0.25), rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(o.w(1), w[1])  # only the listed field is filtered
+
+
+def test_spec_filter_known_answer(oracle_lib):
+    """mean + A cos(k1 x) + B cos(k2 y) with (B/A)^2 below the cutoff: the mean goes,
+    the strong mode stays, the weak one is scaled by filterStrength."""
+    cfg, _ = W.diblock32(n=16)
+    i, j, _k = np.meshgrid(*[np.arange(n) for n in cfg.n], indexing="ij")
+    a = np.cos(2 * np.pi * i / 16).reshape(-1)
+    b = np.cos(2 * np.pi * 3 * j / 16).reshape(-1)
+    w0 = 0.7 + 1.0 * a + 0.1 * b
+    o = O.Oracle(cfg)
+    o.restore([w0, -w0])
+    o.set_spectral_filter(_filter(["A", "B"], 0.5, 0.2))
+    o.apply_spectral_filter()
+    np.testing.assert_allclose(o.w(0), 1.0 * a + 0.02 * b, atol=1e-13)
+    np.testing.assert_allclose(o.w(1), -(1.0 * a + 0.02 * b), atol=1e-13)
+    # cutoffFactor 0 (the reference's default) leaves the fields alone
+    o.restore([w0, -w0])
+    o.set_spectral_filter(_filter(["A"], 0.0, 0.2))
+    o.apply_spectral_filter()
+    np.testing.assert_array_equal(o.w(0), w0)
+
+
+def test_spec_filter_schedule(oracle_lib):
+    """PsUpdater::update (psbase/PsUpdater.cpp:180-206): applied after the field update
+    of step t when applyStart <= t <= applyEnd and (t - applyStart) % applyFrequency == 0."""
+    cfg, w = W.diblock32(n=8)
+    f = _filter(["A", "B"], 0.05, 0.3, start=1, freq=3, end=8)
+    o1 = O.Oracle(cfg)
+    o1.restore(w)
+    o1.set_spectral_filter(f)
+    o1.update(11)
+    o2 = O.Oracle(cfg)
+    o2.restore(w)
+    for t in range(11):
+        o2.update(1)
+        if t in (1, 4, 7):
+            for i in range(2):
+                o2.set_field(A.PS_FIELD_W, i, np_spec_filter(o2.w(i), cfg.n, 0.05, 0.3))
+    for i in range(2):
+        np.testing.assert_allclose(o1.w(i), o2.w(i), rtol=0, atol=1e-11)
+
+
+def test_spec_filter_rejects_bad_config(oracle_lib):
+    cfg, _ = W.diblock32(n=8)
+    o = O.Oracle(cfg)
+    bad = _filter(["A"], 0.1, 0.0, freq=0)
+    with pytest.raises(A.PsError):
+        o.set_spectral_filter(bad)
