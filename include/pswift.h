@@ -225,7 +225,16 @@ int ps_gpu_sweep_timing(ps_handle* h, double* ms_out, int max_out, int* n_out,
  * filtered: w = Re(IFFT(mask FFT(w))) / N with mask = filter_strength where
  * |FFT(w)|^2 < cutoff_factor * max |FFT(w)|^2 and 1 elsewhere.  cutoff_factor
  * <= 0 leaves the fields alone.  FP64 whatever the sweep precision.  Passing
- * NULL removes the filter; not allowed on a batch instance. */
+ * NULL removes the filter; not allowed on a batch instance.
+ *
+ * kind = multiSpecFilter (pseffhamil/PsMultiSpecFilter.cpp:130-262) sets
+ * spec_cells (specCellSizes, each dividing its grid extent): the spectrum is
+ * cut into (nx/sx)(ny/sy)(nz/sz) regions and the max, hence the cutoff, is
+ * taken per region.  The region of linear spectrum index n is found as the
+ * serial reference does, by reading n in (y, x, z) order:
+ * y = n / (nx nz), x = (n / nz) % nx, z = n % nz
+ * (pseffhamil/PsMultiSpecFilter.cpp:175-212).  The mask applies at n in
+ * (x, y, z) order.  All spec_cells 0 selects simpleSpecFilter. */
 typedef struct ps_filter_config {
   int n_fields;              /* updatefields                                  */
   int fields[PS_MAX_FIELDS]; /* monomerDens PhysField indices                 */
@@ -234,6 +243,8 @@ typedef struct ps_filter_config {
   long long apply_start;     /* applyStart                                    */
   long long apply_frequency; /* applyFrequency                                */
   long long apply_end;       /* applyEnd (< 0: until the end of the run)      */
+  int spec_cells[3];         /* specCellSizes (multiSpecFilter); 0 0 0: simple */
+  int pad;
 } ps_filter_config;
 int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* filter);
 /* Apply the filter once now, outside its schedule. */

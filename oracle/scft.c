@@ -94,6 +94,9 @@ struct oracle_state {
   int has_filter;                  /* simpleSpecFilter updater after the field update */
   ps_filter_config fcfg;
   double* fpow;                    /* N: |FFT(w)|^2, then the mask */
+  double* fcut;                    /* multiSpecFilter: max power per region */
+  long* fregion;                   /* multiSpecFilter: region of each spectrum index */
+  long fncells;
   mt_state rng;
   long long iter;
   /* scratch */
@@ -364,6 +367,7 @@ void oracle_destroy(oracle_state* s) {
   if (!s) return;
   for (int i = 0; i < PS_MAX_FIELDS; ++i) { free(s->w[i]); free(s->phi[i]); free(s->dh[i]); }
   free(s->p); free(s->cwork); free(s->qw); free(s->res); free(s->fpow);
+  free(s->fcut); free(s->fregion);
   for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip)
     for (int ib = 0; ib < PS_MAX_BLOCKS; ++ib) {
       oblock* B = &s->pol[ip].b[ib];
@@ -717,8 +721,19 @@ static void filter_apply(oracle_state* s) {
       pw[r] = (c[2 * r] * c[2 * r]) + (c[2 * r + 1] * c[2 * r + 1]);
       if (pw[r] > mx) mx = pw[r];
     }
-    const double cut = F->cutoff_factor * mx;
-    for (long r = 0; r < N; ++r) pw[r] = (pw[r] < cut) ? F->filter_strength : 1.0;
+    if (s->fregion) {
+      /* PsMultiSpecFilter::applyFilter (pseffhamil/PsMultiSpecFilter.cpp:222-262):
+       * the cutoff is cutoffFactor times the max power of the index's region. */
+      for (long c2 = 0; c2 < s->fncells; ++c2) s->fcut[c2] = 0.0;
+      for (long r = 0; r < N; ++r) {
+        const double kcut = F->cutoff_factor * pw[r];
+        if (kcut > s->fcut[s->fregion[r]]) s->fcut[s->fregion[r]] = kcut;
+      }
+      for (long r = 0; r < N; ++r) pw[r] = (pw[r] < s->fcut[s->fregion[r]]) ? F->filter_strength : 1.0;
+    } else {
+      const double cut = F->cutoff_factor * mx;
+      for (long r = 0; r < N; ++r) pw[r] = (pw[r] < cut) ? F->filter_strength : 1.0;
+    }
     oracle_scaled_pair_buf(s->n, w, pw, s->res, c);
     const double scale = 1.0 / (double)N;
     for (long r = 0; r < N; ++r) w[r] = scale * s->res[r];
@@ -733,7 +748,29 @@ int oracle_set_filter(oracle_state* s, const ps_filter_config* f) {
   if (f->n_fields < 1 || f->n_fields > s->nf || f->apply_frequency < 1) return PS_ATTRIB_ERR;
   for (int i = 0; i < f->n_fields; ++i)
     if (f->fields[i] < 0 || f->fields[i] >= s->nf) return PS_ATTRIB_ERR;
+  const int multi = f->spec_cells[0] || f->spec_cells[1] || f->spec_cells[2];
+  if (multi)
+    for (int d = 0; d < 3; ++d)
+      if (f->spec_cells[d] < 1 || s->n[d] % f->spec_cells[d] != 0) return PS_ATTRIB_ERR;
   if (!s->fpow) s->fpow = (double*)xcalloc((size_t)s->N, sizeof(double));
+  free(s->fcut); free(s->fregion);
+  s->fcut = NULL; s->fregion = NULL; s->fncells = 0;
+  if (multi) {
+    /* PsMultiSpecFilter::build_specCells_transpose (pseffhamil/PsMultiSpecFilter.cpp:
+     * 175-212), serial: loops j (y), i (x), k (z) and numbers the index
+     * nn = (j nx + i) nz + k, which the serial FFT then reads in (x, y, z) order. */
+    const long nx = s->n[0], ny = s->n[1], nz = s->n[2];
+    const long cx = nx / f->spec_cells[0], cy = ny / f->spec_cells[1], cz = nz / f->spec_cells[2];
+    s->fncells = cx * cy * cz;
+    s->fcut = (double*)xcalloc((size_t)s->fncells, sizeof(double));
+    s->fregion = (long*)xcalloc((size_t)s->N, sizeof(long));
+    for (long j = 0; j < ny; ++j)
+      for (long i = 0; i < nx; ++i)
+        for (long k = 0; k < nz; ++k) {
+          const long ic0 = i / f->spec_cells[0], ic1 = j / f->spec_cells[1], ic2 = k / f->spec_cells[2];
+          s->fregion[(j * nx + i) * nz + k] = ic2 * (cx * cy) + ic1 * cx + ic0;
+        }
+  }
   s->fcfg = *f;
   s->has_filter = 1;
   return PS_OK;

@@ -77,7 +77,7 @@ class ps_filter_config(C.Structure):
     _fields_ = [("n_fields", C.c_int), ("fields", C.c_int * PS_MAX_FIELDS),
                 ("cutoff_factor", C.c_double), ("filter_strength", C.c_double),
                 ("apply_start", C.c_longlong), ("apply_frequency", C.c_longlong),
-                ("apply_end", C.c_longlong)]
+                ("apply_end", C.c_longlong), ("spec_cells", C.c_int * 3), ("pad", C.c_int)]
 
 
 class ps_scalars(C.Structure):

@@ -76,9 +76,12 @@ class Solvent:
 
 @dataclass
 class SpecFilter:
-    """<Updater name> kind = simpleSpecFilter (pseffhamil/PsSpecFilterUpdater.cpp:56-90,
-    psbase/PsUpdater.cpp:60-120)."""
+    """<Updater name> kind = simpleSpecFilter | multiSpecFilter
+    (pseffhamil/PsSpecFilterUpdater.cpp:56-90, pseffhamil/PsMultiSpecFilter.cpp:50-67,
+    psbase/PsUpdater.cpp:60-120).  ``spec_cells`` (specCellSizes) is None for
+    simpleSpecFilter."""
     name: str = "filter"
+    spec_cells: tuple | None = None
     updatefields: list = field(default_factory=list)
     cutoff_factor: float = 0.0
     filter_strength: float = 0.0
@@ -96,6 +99,10 @@ class SpecFilter:
         f.apply_start = int(self.apply_start)
         f.apply_frequency = int(self.apply_frequency)
         f.apply_end = int(self.apply_end)
+        if self.spec_cells is not None:
+            cells = [int(x) for x in self.spec_cells] + [1] * (3 - len(self.spec_cells))
+            for d in range(3):
+                f.spec_cells[d] = cells[d]
         return f
 
 
@@ -352,18 +359,35 @@ def config_from_text(text: str) -> ScftConfig:
             interactions.append(Interaction(name=iname, chi=float(ia.get("chi", 0.01)),
                                             scfields=[str(x) for x in ia["scfields"]]))
         ups = _find(hnode, "Updater")
-        filters = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) == "simpleSpecFilter"]
-        ups = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) != "simpleSpecFilter"]
+        fkinds = ("simpleSpecFilter", "multiSpecFilter")
+        filters = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) in fkinds]
+        ups = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) not in fkinds]
+        # PsEffHamil::update runs the updaters named in updaterSequence, in its order
+        # (pseffhamil/PsEffHamil.cpp:190-203)
+        seq = hnode["attrs"].get("updaterSequence")
+        seq = [str(x) for x in (seq if isinstance(seq, list) else [seq])] if seq is not None else None
+        if seq is not None:
+            filters = [(n, u) for n, u in filters if n in seq]
+            if ups and filters and ups[0][0] in seq and seq.index(filters[0][0]) < seq.index(ups[0][0]):
+                raise InputError("a spectral filter before the field updater in updaterSequence "
+                                 "is not on the device path")
+        if len(filters) > 1:
+            raise InputError("one spectral filter per run is on the device path")
         if filters:
             fname, fnode = filters[0]
             fa = fnode["attrs"]
             upf = fa.get("updatefields", [])
+            cells = None
+            if str(fa["kind"]) == "multiSpecFilter":
+                if "specCellSizes" not in fa:
+                    raise InputError("PsMultiSpecFilter::setAttrib: specCellSizes not set")
+                cells = tuple(int(x) for x in fa["specCellSizes"])
             spec_filter = SpecFilter(name=fname, updatefields=[str(x) for x in (upf if isinstance(upf, list) else [upf])],
                                      cutoff_factor=float(fa.get("cutoffFactor", 0.0)),
                                      filter_strength=float(fa.get("filterStrength", 0.0)),
                                      apply_start=int(fa.get("applyStart", 0)),
                                      apply_frequency=int(fa.get("applyFrequency", 1)),
-                                     apply_end=int(fa.get("applyEnd", -1)))
+                                     apply_end=int(fa.get("applyEnd", -1)), spec_cells=cells)
         if ups:
             uname, unode = ups[0]
             ua = unode["attrs"]

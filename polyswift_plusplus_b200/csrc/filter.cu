@@ -10,6 +10,12 @@
 // half spectrum of an r2c transform carries all of it.  Runs in FP64 on the
 // FP64 fields whatever the sweep precision, on the handle's stream, after the
 // iteration's graph.
+//
+// multiSpecFilter (pseffhamil/PsMultiSpecFilter.cpp:130-262) takes the max per
+// region of spectrum indices.  Its region map is not even in k, so the mask M
+// is not either; Re(IFFT(M W)) of a real field equals IFFT(W (M(k) + M(-k))/2),
+// and the half spectrum carries that symmetrised mask: each element looks up
+// the regions of both k and -k.
 #include <math.h>
 #include <string.h>
 
@@ -29,7 +35,95 @@ struct FilterState {
   PencilWork<double>* d_xw = nullptr;
   double* part = nullptr;  // kRedBlocks partials
   double* scal = nullptr;  // [0] -mean, [1] max power
+  // multiSpecFilter
+  bool multi = false;
+  long long ncells = 0;
+  double* cut = nullptr;   // max power per region
 };
+
+// Region geometry of multiSpecFilter: cell sizes and cells per axis.
+struct Regions {
+  int nx, ny, nz, nzh;
+  int sx, sy, sz;
+  long long cx, cy;
+};
+
+// Region of linear spectrum index n, read in (y, x, z) order as the serial
+// reference numbers its map (pseffhamil/PsMultiSpecFilter.cpp:185-205).
+__device__ __forceinline__ long long region_of(const Regions& g, long long n) {
+  const long long jj = n / ((long long)g.nx * g.nz);
+  const long long ii = (n / g.nz) % g.nx;
+  const long long kk = n % g.nz;
+  return (kk / g.sz) * (g.cx * g.cy) + (jj / g.sy) * g.cx + ii / g.sx;
+}
+
+// Spectrum indices (x, y, z order) of half-spectrum element e and of its mirror -k.
+__device__ __forceinline__ void pair_indices(const Regions& g, long long e, long long& n1, long long& n2) {
+  const long long i = e / ((long long)g.ny * g.nzh);
+  const long long j = (e / g.nzh) % g.ny;
+  const long long kz = e % g.nzh;
+  n1 = (i * g.ny + j) * g.nz + kz;
+  n2 = (((g.nx - i) % g.nx) * g.ny + (g.ny - j) % g.ny) * g.nz + (g.nz - kz) % g.nz;
+}
+
+constexpr int kShCells = 4096;
+
+// Max power per region.  Powers are >= +0, so their bit patterns order like
+// the values and an integer atomicMax is a max on doubles.  With few regions
+// each block reduces into shared memory first.
+template <bool SH>
+__global__ void filter_region_max(const double2* __restrict__ spec, long long nspec, Regions g,
+                                  unsigned long long* __restrict__ cut, long long ncells) {
+  __shared__ unsigned long long sh[SH ? kShCells : 1];
+  if (SH) {
+    for (long long r = threadIdx.x; r < ncells; r += blockDim.x) sh[r] = 0ull;
+    __syncthreads();
+  }
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nspec;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double2 v = spec[e];
+    const unsigned long long p = (unsigned long long)__double_as_longlong(v.x * v.x + v.y * v.y);
+    long long n1, n2;
+    pair_indices(g, e, n1, n2);
+    const long long r1 = region_of(g, n1), r2 = region_of(g, n2);
+    if (SH) {
+      atomicMax(&sh[r1], p);
+      if (r2 != r1) atomicMax(&sh[r2], p);
+    } else {
+      atomicMax(&cut[r1], p);
+      if (r2 != r1) atomicMax(&cut[r2], p);
+    }
+  }
+  if (SH) {
+    __syncthreads();
+    for (long long r = threadIdx.x; r < ncells; r += blockDim.x)
+      if (sh[r]) atomicMax(&cut[r], sh[r]);
+  }
+}
+
+__global__ void filter_mask_multi(double2* __restrict__ spec, long long nspec, Regions g,
+                                  const double* __restrict__ cut, double cutoff_factor, double strength,
+                                  double inv_n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nspec;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double2 v = spec[e];
+    const double p = v.x * v.x + v.y * v.y;
+    long long n1, n2;
+    pair_indices(g, e, n1, n2);
+    const double m1 = (p < cutoff_factor * cut[region_of(g, n1)]) ? strength : 1.0;
+    const double m2 = (p < cutoff_factor * cut[region_of(g, n2)]) ? strength : 1.0;
+    const double m = 0.5 * (m1 + m2) * inv_n;
+    spec[e] = make_double2(v.x * m, v.y * m);
+  }
+}
+
+static Regions regions_of(const ps_handle* h, const ps_filter_config& c) {
+  Regions g;
+  g.nx = h->n[0]; g.ny = h->n[1]; g.nz = h->n[2]; g.nzh = (int)h->nzh;
+  g.sx = c.spec_cells[0]; g.sy = c.spec_cells[1]; g.sz = c.spec_cells[2];
+  g.cx = g.nx / g.sx; g.cy = g.ny / g.sy;
+  return g;
+}
 
 constexpr int kFT = 256;
 
@@ -101,7 +195,7 @@ void filter_free(ps_handle* h) {
   if (!f) return;
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(f->spec); fr(f->tw_x); fr(f->tw_y); fr(f->tw_z); fr(f->tw_zh);
-  fr(f->d_pw); fr(f->d_xw); fr(f->part); fr(f->scal);
+  fr(f->d_pw); fr(f->d_xw); fr(f->part); fr(f->scal); fr(f->cut);
   delete f;
   h->filter = nullptr;
 }
@@ -137,6 +231,11 @@ static int filter_build(ps_handle* h, const ps_filter_config* c) {
   PS_CUDA(h, cudaMemcpy(f->d_xw, &xw, sizeof(xw), cudaMemcpyHostToDevice));
   PS_CUDA(h, cudaMalloc((void**)&f->part, sizeof(double) * kRedBlocks));
   PS_CUDA(h, cudaMalloc((void**)&f->scal, sizeof(double) * 2));
+  f->multi = c->spec_cells[0] || c->spec_cells[1] || c->spec_cells[2];
+  if (f->multi) {
+    f->ncells = (long long)(nx / c->spec_cells[0]) * (ny / c->spec_cells[1]) * (nz / c->spec_cells[2]);
+    PS_CUDA(h, cudaMalloc((void**)&f->cut, sizeof(double) * (size_t)f->ncells));
+  }
   return PS_OK;
 }
 
@@ -164,10 +263,22 @@ static int filter_apply(ps_handle* h) {
       if (ny > 1) PS_CUDA(h, launch_pencil<double>(f->d_xw, 1, PENCIL_FWD, ny, nx, h->nzh, f->tw_y, nx, ny, nz, 0, st));
     }
     PS_CUDA(h, launch_pencil<double>(f->d_xw, 1, PENCIL_FWD, nx, 1, ny * h->nzh, f->tw_x, nx, ny, nz, 0, st));
-    filter_sum_partials<<<kRedBlocks, kFT, 0, st>>>(nullptr, nspec, f->part, 1, f->spec);
-    filter_finalize<<<1, kFT, 0, st>>>(f->part, kRedBlocks, 1, (double)N, f->scal + 1);
-    filter_mask<<<blocks, 256, 0, st>>>(f->spec, nspec, f->scal + 1, c.cutoff_factor, c.filter_strength,
-                                        1.0 / (double)N);
+    if (f->multi) {
+      const Regions g = regions_of(h, c);
+      PS_CUDA(h, cudaMemsetAsync(f->cut, 0, sizeof(double) * (size_t)f->ncells, st));
+      unsigned long long* cu = reinterpret_cast<unsigned long long*>(f->cut);
+      if (f->ncells <= kShCells)
+        filter_region_max<true><<<blocks, 256, 0, st>>>(f->spec, nspec, g, cu, f->ncells);
+      else
+        filter_region_max<false><<<blocks, 256, 0, st>>>(f->spec, nspec, g, cu, f->ncells);
+      filter_mask_multi<<<blocks, 256, 0, st>>>(f->spec, nspec, g, f->cut, c.cutoff_factor, c.filter_strength,
+                                                1.0 / (double)N);
+    } else {
+      filter_sum_partials<<<kRedBlocks, kFT, 0, st>>>(nullptr, nspec, f->part, 1, f->spec);
+      filter_finalize<<<1, kFT, 0, st>>>(f->part, kRedBlocks, 1, (double)N, f->scal + 1);
+      filter_mask<<<blocks, 256, 0, st>>>(f->spec, nspec, f->scal + 1, c.cutoff_factor, c.filter_strength,
+                                          1.0 / (double)N);
+    }
     PS_CUDA(h, cudaGetLastError());
     // inverse c2r, stored back into w
     PS_CUDA(h, launch_pencil<double>(f->d_xw, 1, PENCIL_INV, nx, 1, ny * h->nzh, f->tw_x, nx, ny, nz, 0, st));
@@ -215,6 +326,12 @@ int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* c) {
       h->err = "spectral filter: field index out of range";
       return PS_ATTRIB_ERR;
     }
+  if (c->spec_cells[0] || c->spec_cells[1] || c->spec_cells[2])
+    for (int d = 0; d < 3; ++d)
+      if (c->spec_cells[d] < 1 || h->n[d] % c->spec_cells[d] != 0) {
+        h->err = "multiSpecFilter: each specCellSizes entry must divide its grid extent";
+        return PS_ATTRIB_ERR;
+      }
   if (c->apply_frequency < 1) {
     h->err = "spectral filter: apply_frequency must be >= 1";
     return PS_ATTRIB_ERR;

@@ -225,11 +225,7 @@ def test_dump_restore_round_trip_on_host(tmp_path):
             assert np.array_equal(x, y)
 
 
-def test_config_parser_reads_simple_spec_filter():
-    """<Updater name> kind = simpleSpecFilter (pseffhamil/PsSpecFilterUpdater.cpp:55-90 and
-    psbase/PsUpdater.cpp:55-110) beside the field updater."""
-    from polyswift_plusplus_b200.config import config_from_text
-    text = """
+_SPEC_FILTER_DECK = """
 setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
 <EffHamil h>
   <Updater u>
@@ -283,6 +279,13 @@ setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
   </Block>
 </Polymer>
 """
+
+
+def test_config_parser_reads_simple_spec_filter():
+    """<Updater name> kind = simpleSpecFilter (pseffhamil/PsSpecFilterUpdater.cpp:55-90 and
+    psbase/PsUpdater.cpp:55-110) beside the field updater."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = _SPEC_FILTER_DECK
     cfg = config_from_text(text)
     assert cfg.updater.kind == "steepestDescent"
     f = cfg.spec_filter
@@ -291,3 +294,21 @@ setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
     assert (f.apply_start, f.apply_frequency, f.apply_end) == (5, 10, 200)
     pf = f.to_ps(cfg)
     assert pf.n_fields == 2 and list(pf.fields[:2]) == [1, 0]
+
+
+def test_config_parser_multi_spec_filter_and_updater_sequence():
+    """multiSpecFilter with specCellSizes (pseffhamil/PsMultiSpecFilter.cpp:50-67); a filter
+    runs only when updaterSequence names it (pseffhamil/PsEffHamil.cpp:190-203)."""
+    from polyswift_plusplus_b200.config import InputError, config_from_text
+    base = _SPEC_FILTER_DECK
+    deck = base.replace("kind = simpleSpecFilter", "kind = multiSpecFilter\n    specCellSizes = [4 4 1]")
+    cfg = config_from_text(deck.replace("<EffHamil h>", "<EffHamil h>\n  updaterSequence = [u filt]"))
+    assert cfg.spec_filter.spec_cells == (4, 4, 1)
+    pf = cfg.spec_filter.to_ps(cfg)
+    assert list(pf.spec_cells) == [4, 4, 1]
+    cfg = config_from_text(deck.replace("<EffHamil h>", "<EffHamil h>\n  updaterSequence = [u]"))
+    assert cfg.spec_filter is None
+    with pytest.raises(InputError):
+        config_from_text(deck.replace("<EffHamil h>", "<EffHamil h>\n  updaterSequence = [filt u]"))
+    with pytest.raises(InputError):
+        config_from_text(base.replace("kind = simpleSpecFilter", "kind = multiSpecFilter"))

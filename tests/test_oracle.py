@@ -302,3 +302,73 @@ def test_spec_filter_rejects_bad_config(oracle_lib):
     bad = _filter(["A"], 0.1, 0.0, freq=0)
     with pytest.raises(A.PsError):
         o.set_spectral_filter(bad)
+
+
+def np_multi_spec_filter(w, shape, cells, cutoff, strength, transposed_map=True):
+    """numpy restatement of PsMultiSpecFilter::applyFilter (pseffhamil/PsMultiSpecFilter.cpp:
+    222-262) with the serial region map of build_specCells_transpose (:175-212): linear
+    spectrum index n read in (y, x, z) order.  transposed_map=False reads it in (x, y, z)."""
+    nx, ny, nz = shape
+    sx, sy, sz = cells
+    cx, cy = nx // sx, ny // sy
+    x = np.asarray(w, dtype=np.float64).reshape(shape)
+    x = x - x.mean()
+    k = np.fft.fftn(x)
+    p = (np.abs(k) ** 2).reshape(-1)
+    n = np.arange(p.size)
+    if transposed_map:
+        yy, xx, zz = n // (nx * nz), (n // nz) % nx, n % nz
+    else:
+        xx, yy, zz = n // (ny * nz), (n // nz) % ny, n % nz
+    region = (zz // sz) * (cx * cy) + (yy // sy) * cx + xx // sx
+    cut = np.zeros(cx * cy * (nz // sz))
+    np.maximum.at(cut, region, cutoff * p)
+    mask = np.where(p < cut[region], strength, 1.0).reshape(shape)
+    return np.real(np.fft.ifftn(mask * k)).reshape(-1)
+
+
+def _multi(fields, cells, cutoff, strength, **kw):
+    f = _filter(fields, cutoff, strength, **kw)
+    f.spec_cells = tuple(cells)
+    return f
+
+
+@pytest.mark.parametrize("shape,cells", [((16, 16, 16), (4, 4, 1)), ((8, 16, 12), (2, 4, 3)),
+                                         ((12, 6, 8), (3, 2, 8)), ((32, 32, 1), (8, 4, 1))])
+def test_multi_spec_filter_matches_numpy(oracle_lib, shape, cells):
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = shape
+    rng = np.random.default_rng(5)
+    w = [rng.standard_normal(cfg.n_total), rng.standard_normal(cfg.n_total)]
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.set_spectral_filter(_multi(["A", "B"], cells, 0.6, 0.0))
+    o.apply_spectral_filter()
+    for i in range(2):
+        np.testing.assert_allclose(o.w(i), np_multi_spec_filter(w[i], shape, cells, 0.6, 0.0),
+                                   rtol=0, atol=1e-12)
+
+
+def test_multi_spec_filter_known_answers(oracle_lib):
+    """One region is simpleSpecFilter; on a square x-y grid with equal x and y cells the
+    serial (y, x, z) region map only relabels the natural (x, y, z) regions."""
+    cfg, _ = W.diblock32(n=16)
+    rng = np.random.default_rng(9)
+    w = [rng.standard_normal(cfg.n_total), rng.standard_normal(cfg.n_total)]
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.set_spectral_filter(_multi(["A"], (16, 16, 16), 0.3, 0.2))
+    o.apply_spectral_filter()
+    np.testing.assert_allclose(o.w(0), np_spec_filter(w[0], cfg.n, 0.3, 0.2), rtol=0, atol=1e-12)
+    o.restore(w)
+    o.set_spectral_filter(_multi(["B"], (4, 4, 8), 0.5, 0.1))
+    o.apply_spectral_filter()
+    np.testing.assert_allclose(o.w(1), np_multi_spec_filter(w[1], cfg.n, (4, 4, 8), 0.5, 0.1,
+                                                            transposed_map=False), rtol=0, atol=1e-12)
+
+
+def test_multi_spec_filter_rejects_cells_not_dividing_the_grid(oracle_lib):
+    cfg, _ = W.diblock32(n=8)
+    o = O.Oracle(cfg)
+    with pytest.raises(A.PsError):
+        o.set_spectral_filter(_multi(["A"], (3, 4, 1), 0.5, 0.0))
