@@ -45,7 +45,8 @@ def test_version_string(native_lib):
 def test_struct_layout_matches_header(tmp_path):
     """Every ctypes field offset and struct size equals gcc's offsetof/sizeof."""
     structs = [A.ps_block_config, A.ps_polymer_config, A.ps_interaction_config,
-               A.ps_updater_config, A.ps_config, A.ps_scalars]
+               A.ps_updater_config, A.ps_solvent_config, A.ps_config, A.ps_filter_config,
+               A.ps_scalars]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pswift.h"', 'int main(void){']
     for s in structs:
         n = s.__name__
