@@ -35,6 +35,7 @@ extern "C" {
 #define PS_MAX_FIELDS 4
 #define PS_MAX_INTERACTIONS 6
 #define PS_MAX_SOLVENTS 2
+#define PS_MAX_CHARGES 2
 
 /* Status codes: same numbers as the reference's quitPolyswift() codes. */
 enum {
@@ -53,8 +54,16 @@ enum { PS_PREC_FP64 = 0, PS_PREC_MIXED = 1 };
  * Anderson mixing (added; the reference has no Anderson updater). */
 enum { PS_UPD_STEEPEST = 0, PS_UPD_ANDERSON = 1 };
 
-/* Field selectors for get/set: conjugate field w_i, density phi_i, pressure p. */
-enum { PS_FIELD_W = 0, PS_FIELD_PHI = 1, PS_FIELD_PRES = 2 };
+/* Field selectors for get/set: conjugate field w_i, density phi_i, pressure p;
+ * for chargeDens PhysField c (psphysf/PsChargeDens.cpp:20-30) its charge
+ * density rho_c ("ChargeDensity") and electric potential psi_c
+ * ("ElectricPotential"). */
+enum { PS_FIELD_W = 0, PS_FIELD_PHI = 1, PS_FIELD_PRES = 2, PS_FIELD_CHARGE = 3,
+       PS_FIELD_POTENTIAL = 4 };
+
+/* Solvent kinds: simpleSolvent (pssolvent/PsSimpleSolvent.cpp) and
+ * simpleIons (pssolvent/PsSimpleIons.cpp). */
+enum { PS_SOLV_SIMPLE = 0, PS_SOLV_IONS = 1 };
 
 /* Block end selectors for propagator access. */
 enum { PS_FROM_HEAD = 0, PS_FROM_TAIL = 1 };
@@ -99,11 +108,30 @@ typedef struct ps_updater_config {
   int anderson_start;      /* plain steps before the history is used        */
 } ps_updater_config;
 
-/* <Solvent name> kind = simpleSolvent (psbase/PsSolvent.cpp:40-60). */
+/* <Solvent name> kind = simpleSolvent | simpleIons (psbase/PsSolvent.cpp:40-60,
+ * pssolvent/PsSimpleIons.cpp:30-60). */
 typedef struct ps_solvent_config {
   int field;               /* scfield: index of the monomerDens PhysField   */
   double volfrac;          /* volfrac                                       */
+  int kind;                /* PS_SOLV_SIMPLE or PS_SOLV_IONS                */
+  int charge_field;        /* simpleIons: chargefield (chargeDens index)    */
+  int has_block_field;     /* simpleIons: blockfield given                  */
+  int block_field;         /* simpleIons: blockfield (chargeDens index)     */
+  double zc;               /* simpleIons: zc, the ion charge                */
+  double neutral_factor;   /* simpleIons: neutralFactor                     */
 } ps_solvent_config;
+
+/* <Block name> kind = chargeFlexPseudoSpec (pspolymer/PsChargeFlexPseudoSpec.cpp:42-75):
+ * the block's Boltzmann factor gains exp(-ds/2 za alpha L psi_c) (L = length
+ * of polymer 0) and rho_c += za alpha phi_f after its density
+ * (pspolymer/PsChargeFlexPseudoSpec.cpp:97-165).  The device path needs the
+ * charged block to be the only contributor to its scfield. */
+typedef struct ps_block_charge {
+  int charged;             /* 0: flexPseudoSpec                              */
+  int charge_field;        /* chargefield (chargeDens index)                */
+  double za;               /* za                                            */
+  double alpha;            /* alpha                                         */
+} ps_block_charge;
 
 typedef struct ps_config {
   int n[3];                /* numCellsGlobal                                */
@@ -123,6 +151,11 @@ typedef struct ps_config {
    * L = length of polymer 0.  Appended at the end so the fields above keep their offsets. */
   int n_solvents;
   ps_solvent_config solvents[PS_MAX_SOLVENTS];
+  /* chargeDens PhysFields: rho_c is reset every iteration (PsChargeDens::update)
+   * and filled by simpleIons solvents and charged blocks; psi_c changes only
+   * through ps_gpu_set_fields and the Poisson updater.  Appended at the end. */
+  int n_charges;
+  ps_block_charge block_charge[PS_MAX_POLYMERS][PS_MAX_BLOCKS];
 } ps_config;
 
 typedef struct ps_scalars {
@@ -249,6 +282,26 @@ typedef struct ps_filter_config {
 int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* filter);
 /* Apply the filter once now, outside its schedule. */
 int ps_gpu_apply_spectral_filter(ps_handle* h);
+
+/* --- Poisson updater: <Updater name> kind = poissonUpdater
+ * (pseffhamil/PsPoissonUpdater.cpp:50-270; schedule psbase/PsUpdater.cpp:60-206).
+ * At the scheduled steps (as for the spectral filter), for every listed
+ * chargeDens field c: rho_c loses its mean (in place), res = IFFT(K FFT(rho_c))
+ * with K(k) = 4 (3.1415) bjerrum_len / |k|^2 (0 where |k|^2 < 1e-9), and
+ * psi_c = res / N, except where |res/N - psi_c| > 0.2 |psi_c|, which take
+ * 1.2 psi_c / N (the reference's clamp, psi_c = 0 included).  FP64, after the
+ * iteration's graph; updaters installed later run later.  NULL removes it. */
+typedef struct ps_poisson_config {
+  int n_fields;              /* updatefields: chargeDens indices              */
+  int fields[PS_MAX_CHARGES];
+  double bjerrum_len;        /* bjerrumLen                                    */
+  double relaxlambda;        /* relaxlambda (read, unused, as in the reference) */
+  long long apply_start;
+  long long apply_frequency;
+  long long apply_end;       /* < 0: no end                                   */
+} ps_poisson_config;
+int ps_gpu_set_poisson(ps_handle* h, const ps_poisson_config* poisson);
+int ps_gpu_apply_poisson(ps_handle* h);
 
 /* --- Batched instances (no reference counterpart: the reference runs one
  * PsDomain per process, polyswift/polyswift/polyswift.cxx:544-588) ----------

@@ -43,6 +43,9 @@ def lib() -> C.CDLL:
         L.oracle_set_filter.restype = C.c_int
         L.oracle_set_filter.argtypes = [vp, C.POINTER(A.ps_filter_config)]
         L.oracle_apply_filter.argtypes = [vp]
+        L.oracle_set_poisson.restype = C.c_int
+        L.oracle_set_poisson.argtypes = [vp, C.POINTER(A.ps_poisson_config)]
+        L.oracle_apply_poisson.argtypes = [vp]
         L.oracle_get_field.argtypes = [vp, C.c_int, C.c_int, vp]
         L.oracle_iterate.restype = C.c_int
         L.oracle_iterate.argtypes = [vp, C.c_int, C.POINTER(A.ps_scalars)]
@@ -112,8 +115,11 @@ class Oracle:
         self._h = h
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
-        if getattr(cfg, "spec_filter", None) is not None:
-            self.set_spectral_filter(cfg.spec_filter)
+        for kind, u in cfg.post_updaters():
+            if kind == "filter":
+                self.set_spectral_filter(u)
+            else:
+                self.set_poisson(u)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -146,6 +152,22 @@ class Oracle:
 
     def apply_spectral_filter(self):
         lib().oracle_apply_filter(self._h)
+
+    def set_poisson(self, poisson):
+        """poisson: a config.PoissonUpdater, or None to remove the updater."""
+        self._ppcfg = poisson.to_ps(self.cfg) if poisson is not None else None
+        rc = lib().oracle_set_poisson(self._h, C.byref(self._ppcfg) if self._ppcfg is not None else None)
+        if rc != A.PS_OK:
+            raise A.PsError(rc, "bad poisson updater")
+
+    def apply_poisson(self):
+        lib().oracle_apply_poisson(self._h)
+
+    def rho(self, c):
+        return self.get_field(A.PS_FIELD_CHARGE, c)
+
+    def psi(self, c):
+        return self.get_field(A.PS_FIELD_POTENTIAL, c)
 
     def set_field(self, which, index, data):
         x = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)

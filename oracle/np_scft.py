@@ -13,6 +13,8 @@ Reference order of one update (pstrol/PsDomain.cpp:332-372):
   densities    pspolymer/PsBlock.cpp:153-196
   update       pseffhamil/PsSteepDUpdater.cpp:159-453, psphysf/PsConstraint.cpp:184-262
   free energy  pseffhamil/PsPolymerUpdater.cpp:172-226, pseffhamil/PsFloryInteraction.cpp:274-321
+  charges      psphysf/PsChargeDens.cpp:180-190, pssolvent/PsSimpleIons.cpp:90-160,
+               pspolymer/PsChargeFlexPseudoSpec.cpp:97-165, pseffhamil/PsPoissonUpdater.cpp:140-262
 """
 from __future__ import annotations
 
@@ -38,8 +40,8 @@ def block_steps(bs: float, force: bool) -> int:
     return int(v)
 
 
-def k2_operator(cfg: ScftConfig, ds: float, bseg: float) -> np.ndarray:
-    """psbase/PsGridField.cpp:66-104 + pspolymer/PsFlexPseudoSpec.cpp:188-206"""
+def k_squared(cfg: ScftConfig) -> np.ndarray:
+    """psbase/PsGridField.cpp:66-104"""
     ks = []
     for d in range(3):
         n = cfg.n[d]
@@ -47,8 +49,19 @@ def k2_operator(cfg: ScftConfig, ds: float, bseg: float) -> np.ndarray:
         nk = n / 2.0 - np.abs(i - n / 2.0)
         ks.append((2.0 * math.pi * nk / n) / cfg.cell[d])
     kx, ky, kz = np.meshgrid(*ks, indexing="ij")
-    k2 = kx * kx + ky * ky + kz * kz
-    return np.exp(-1.0 * ds * k2 * bseg * bseg)
+    return kx * kx + ky * ky + kz * kz
+
+
+def k2_operator(cfg: ScftConfig, ds: float, bseg: float) -> np.ndarray:
+    """pspolymer/PsFlexPseudoSpec.cpp:188-206"""
+    return np.exp(-1.0 * ds * k_squared(cfg) * bseg * bseg)
+
+
+def coulomb_operator(cfg: ScftConfig, bjerrum_len: float) -> np.ndarray:
+    """PsPoissonUpdater::build_k2 (pseffhamil/PsPoissonUpdater.cpp:140-175)."""
+    k2 = k_squared(cfg)
+    with np.errstate(divide="ignore"):
+        return np.where(k2 < 0.000000001, 0.0, (4.0 * 3.1415 * bjerrum_len) / k2)
 
 
 def chain_order(poly) -> list[tuple[int, int]]:
@@ -99,8 +112,16 @@ class NpScft:
                 st.append(block_steps(self.alpha[ip] * B.lengthfrac / B.ds, B.force_block_steps))
             self.steps.append(st)
         for S in getattr(cfg, "solvents", []):  # PsSimpleSolvent::buildSolvers: addToDensAverage
+            if S.kind == "simpleIons":
+                continue
             f = cfg.field_index(S.scfield)
             self.avg[f] = self.avg[f] + S.volfrac
+        self.nq = len(getattr(cfg, "charge_fields", []))
+        self.rho = [np.zeros(tuple(cfg.n)) for _ in range(self.nq)]
+        self.psi = [np.zeros(tuple(cfg.n)) for _ in range(self.nq)]
+        self.t = 0
+        if getattr(cfg, "spec_filter", None) is not None:
+            raise NotImplementedError("the numpy restatement has no spectral filter")
         self.w = [np.zeros(self.shape) for _ in range(self.nf)]
         self.p = np.zeros(self.shape)
         self.phi = [np.zeros(self.shape) for _ in range(self.nf)]
@@ -130,6 +151,9 @@ class NpScft:
                 B = P.blocks[b]
                 f = self.cfg.field_index(B.scfield)
                 wfac = np.exp(-0.5 * B.ds * self.w[f])
+                if B.chargefield is not None:
+                    c = self.cfg.charge_index(B.chargefield)
+                    wfac = wfac * np.exp((B.za * B.alpha * self.L0) * (-0.5 * B.ds) * self.psi[c])
                 key = (B.ds, B.bseg_ratio)
                 if key not in self.k2:
                     self.k2[key] = k2_operator(self.cfg, B.ds, B.bseg_ratio)
@@ -153,6 +177,9 @@ class NpScft:
             if even:
                 acc = acc + (a[num - 2] * t[1] + a[num - 1] * t[0]) * (B.ds * 0.5)
             self.phi[f] = self.phi[f] + (1.0 * P.volfrac / self.alpha[ip]) * ((1.0 / Q) * acc)
+            if B.chargefield is not None:
+                c = self.cfg.charge_index(B.chargefield)
+                self.rho[c] = self.rho[c] + (self.phi[f] * B.alpha) * B.za
         return Q, qs
 
     def solvent(self, S):
@@ -163,10 +190,35 @@ class NpScft:
         self.phi[f] = self.phi[f] + wfactor * (S.volfrac / Q)
         return Q
 
+    def ions(self, S):
+        """PsSimpleIons::setPhysFields (pssolvent/PsSimpleIons.cpp:90-160)."""
+        c = self.cfg.charge_index(S.chargefield)
+        e = np.exp(self.psi[c] * (-1.0 * S.zc))
+        Q = float(np.sum(e)) / self.N
+        e = e * (-S.neutral_factor / (Q * S.zc))
+        if S.blockfield is not None:
+            self.rho[self.cfg.charge_index(S.blockfield)] = e.copy()
+        self.rho[c] = self.rho[c] + e * S.zc
+        return Q
+
+    def poisson(self, P):
+        """PsPoissonUpdater::update (pseffhamil/PsPoissonUpdater.cpp:196-262)."""
+        kc = coulomb_operator(self.cfg, P.bjerrum_len)
+        for name in P.updatefields:
+            c = self.cfg.charge_index(name)
+            self.rho[c] = self.rho[c] + (-1.0 * (float(np.sum(self.rho[c])) / self.N))
+            res = np.fft.ifftn(np.fft.fftn(self.rho[c]) * kc).real * self.N
+            psi0 = self.psi[c]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                frac = np.abs((res * (1.0 / self.N) - psi0) / psi0)
+            res = np.where(frac > 0.2, psi0 * 1.2, res)
+            self.psi[c] = res * (1.0 / self.N)
+
     def iterate(self):
         self.phi = [np.zeros(self.shape) for _ in range(self.nf)]
+        self.rho = [np.zeros(self.shape) for _ in range(self.nq)]
         solvents = list(getattr(self.cfg, "solvents", []))
-        Qsol = [self.solvent(S) for S in solvents]
+        Qsol = [self.ions(S) if S.kind == "simpleIons" else self.solvent(S) for S in solvents]
         Qs = [self.polymer(ip)[0] for ip in range(len(self.cfg.polymers))]
         nf = self.nf
         dh = []
@@ -200,4 +252,9 @@ class NpScft:
             dens = dens + self.chin[it] * (self.phi[a] * self.phi[b] - self.avg[a] * self.avg[b])
         fe += float(np.sum(dens)) / self.N
         inc = float(np.max(np.abs(sum(self.phi, np.zeros(self.shape)) - 1.0)))
+        P = getattr(self.cfg, "poisson", None)
+        if P is not None and self.t >= P.apply_start and (P.apply_end < 0 or self.t <= P.apply_end) \
+                and (self.t - P.apply_start) % P.apply_frequency == 0:
+            self.poisson(P)
+        self.t += 1
         return {"free_energy": fe, "q": Qs, "max_incomp": inc}

@@ -43,6 +43,8 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
 void oracle_destroy(oracle_state* s);
 int oracle_set_filter(oracle_state* s, const ps_filter_config* f);
 void oracle_apply_filter(oracle_state* s);
+int oracle_set_poisson(oracle_state* s, const ps_poisson_config* p);
+void oracle_apply_poisson(oracle_state* s);
 int oracle_block_steps(const oracle_state* s, int polymer, int block);
 void oracle_init_random(oracle_state* s);
 void oracle_set_field(oracle_state* s, int which, int index, const double* data);

@@ -97,6 +97,15 @@ struct oracle_state {
   double* fcut;                    /* multiSpecFilter: max power per region */
   long* fregion;                   /* multiSpecFilter: region of each spectrum index */
   long fncells;
+  /* chargeDens PhysFields: charge density and electric potential */
+  int nq;
+  double* rho[PS_MAX_CHARGES];
+  double* psi[PS_MAX_CHARGES];
+  int has_poisson;                 /* poissonUpdater after the field update */
+  ps_poisson_config pcfg;
+  double* kcoul;                   /* N: 4 (3.1415) lB / |k|^2, 0 at |k|^2 < 1e-9 */
+  int post[2];                     /* post-update updaters in run order: 1 filter, 2 Poisson */
+  int npost;
   mt_state rng;
   long long iter;
   /* scratch */
@@ -153,26 +162,30 @@ static int set_block_steps(double bs, int force, int* out, char* err, int errlen
   return PS_OK;
 }
 
-/* PsGridField::calck2 (psbase/PsGridField.cpp:66-104) then
- * PsFlexPseudoSpec::build_k2 (pspolymer/PsFlexPseudoSpec.cpp:188-206). */
-static void build_k2(const oracle_state* s, const oblock* b, double* k2) {
+/* PsGridField::calck2 (psbase/PsGridField.cpp:66-104): |k|^2 at grid index (i, j, k). */
+static double calck2(const oracle_state* s, int i, int j, int k) {
   const double twopi = 2.0 * acos(-1.0);
   double n2[3];
   for (int d = 0; d < 3; ++d) n2[d] = (double)s->n[d] / 2.0;
+  double nk2 = n2[2] - fabs((double)k - n2[2]);
+  double nk1 = n2[1] - fabs((double)j - n2[1]);
+  double nk0 = n2[0] - fabs((double)i - n2[0]);
+  double kv2 = twopi * nk2 / (double)s->n[2];
+  double kv1 = twopi * nk1 / (double)s->n[1];
+  double kv0 = twopi * nk0 / (double)s->n[0];
+  kv2 = kv2 / s->cfg.cell[2];
+  kv1 = kv1 / s->cfg.cell[1];
+  kv0 = kv0 / s->cfg.cell[0];
+  return kv0 * kv0 + kv1 * kv1 + kv2 * kv2;
+}
+
+/* PsFlexPseudoSpec::build_k2 (pspolymer/PsFlexPseudoSpec.cpp:188-206). */
+static void build_k2(const oracle_state* s, const oblock* b, double* k2) {
   long idx = 0;
   for (int i = 0; i < s->n[0]; ++i)
     for (int j = 0; j < s->n[1]; ++j)
       for (int k = 0; k < s->n[2]; ++k) {
-        double nk2 = n2[2] - fabs((double)k - n2[2]);
-        double nk1 = n2[1] - fabs((double)j - n2[1]);
-        double nk0 = n2[0] - fabs((double)i - n2[0]);
-        double kv2 = twopi * nk2 / (double)s->n[2];
-        double kv1 = twopi * nk1 / (double)s->n[1];
-        double kv0 = twopi * nk0 / (double)s->n[0];
-        kv2 = kv2 / s->cfg.cell[2];
-        kv1 = kv1 / s->cfg.cell[1];
-        kv0 = kv0 / s->cfg.cell[0];
-        double k2val = kv0 * kv0 + kv1 * kv1 + kv2 * kv2;
+        double k2val = calck2(s, i, j, k);
         k2[idx++] = exp(-1.0 * b->cfg.ds * k2val * b->cfg.bseg_ratio * b->cfg.bseg_ratio);
       }
 }
@@ -310,6 +323,17 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
     snprintf(err, errlen, "n_solvents out of range");
     rc = PS_ATTRIB_ERR;
   }
+  if (rc == PS_OK && (cfg->n_charges < 0 || cfg->n_charges > PS_MAX_CHARGES)) {
+    snprintf(err, errlen, "n_charges out of range");
+    rc = PS_ATTRIB_ERR;
+  }
+  if (rc == PS_OK) {
+    s->nq = cfg->n_charges;
+    for (int c = 0; c < s->nq; ++c) {
+      s->rho[c] = (double*)xcalloc((size_t)N, sizeof(double));
+      s->psi[c] = (double*)xcalloc((size_t)N, sizeof(double));
+    }
+  }
   for (int is = 0; is < cfg->n_solvents && rc == PS_OK; ++is) {
     const ps_solvent_config* S = &cfg->solvents[is];
     if (S->field < 0 || S->field >= s->nf) {
@@ -317,9 +341,47 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
       rc = PS_ATTRIB_ERR;
       break;
     }
-    /* PsSimpleSolvent::buildSolvers: addToDensAverage(volfrac) */
-    s->dens_avg[S->field] = s->dens_avg[S->field] + S->volfrac;
+    if (S->kind == PS_SOLV_IONS) {
+      if (S->charge_field < 0 || S->charge_field >= s->nq ||
+          (S->has_block_field && (S->block_field < 0 || S->block_field >= s->nq)) || S->zc == 0.0) {
+        snprintf(err, errlen, "solvent %d: simpleIons needs chargefield (and blockfield) and zc != 0", is);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+    } else if (S->kind == PS_SOLV_SIMPLE) {
+      /* PsSimpleSolvent::buildSolvers: addToDensAverage(volfrac) */
+      s->dens_avg[S->field] = s->dens_avg[S->field] + S->volfrac;
+    } else {
+      snprintf(err, errlen, "solvent %d: unknown kind", is);
+      rc = PS_ATTRIB_ERR;
+      break;
+    }
   }
+  /* chargeFlexPseudoSpec blocks: chargefield in range, and (a restriction of this
+   * restatement and of the device path) the only contributor to their scfield, so
+   * that rho += za alpha phi_f sees the block's own density as the reference does */
+  for (int ip = 0; ip < s->npol && rc == PS_OK; ++ip)
+    for (int ib = 0; ib < s->pol[ip].nb && rc == PS_OK; ++ib) {
+      const ps_block_charge* Z = &cfg->block_charge[ip][ib];
+      if (!Z->charged) continue;
+      if (Z->charge_field < 0 || Z->charge_field >= s->nq) {
+        snprintf(err, errlen, "polymer %d block %d: chargefield out of range", ip, ib);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+      const int f = s->pol[ip].b[ib].cfg.field;
+      int others = 0;
+      for (int jp = 0; jp < s->npol; ++jp)
+        for (int jb = 0; jb < s->pol[jp].nb; ++jb)
+          if ((jp != ip || jb != ib) && s->pol[jp].b[jb].cfg.field == f) ++others;
+      for (int is = 0; is < cfg->n_solvents; ++is)
+        if (cfg->solvents[is].kind == PS_SOLV_SIMPLE && cfg->solvents[is].field == f) ++others;
+      if (others) {
+        snprintf(err, errlen, "polymer %d block %d: a charged block must be the only density "
+                 "source of its scfield", ip, ib);
+        rc = PS_INPUT_ERR;
+      }
+    }
   if (rc == PS_OK) {
     /* sum of volume fractions of polymers and solvents
        (psphysf/PsPhysFieldHldr.cpp:190-257) */
@@ -367,7 +429,8 @@ void oracle_destroy(oracle_state* s) {
   if (!s) return;
   for (int i = 0; i < PS_MAX_FIELDS; ++i) { free(s->w[i]); free(s->phi[i]); free(s->dh[i]); }
   free(s->p); free(s->cwork); free(s->qw); free(s->res); free(s->fpow);
-  free(s->fcut); free(s->fregion);
+  free(s->fcut); free(s->fregion); free(s->kcoul);
+  for (int c = 0; c < PS_MAX_CHARGES; ++c) { free(s->rho[c]); free(s->psi[c]); }
   for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip)
     for (int ib = 0; ib < PS_MAX_BLOCKS; ++ib) {
       oblock* B = &s->pol[ip].b[ib];
@@ -395,15 +458,22 @@ void oracle_init_random(oracle_state* s) {
   memset(s->p, 0, sizeof(double) * (size_t)s->N);
 }
 
+static double* field_ptr(const oracle_state* s, int which, int index) {
+  switch (which) {
+    case PS_FIELD_W: return s->w[index];
+    case PS_FIELD_PHI: return s->phi[index];
+    case PS_FIELD_CHARGE: return s->rho[index];
+    case PS_FIELD_POTENTIAL: return s->psi[index];
+    default: return s->p;
+  }
+}
+
 void oracle_set_field(oracle_state* s, int which, int index, const double* data) {
-  double* dst = (which == PS_FIELD_W) ? s->w[index] : (which == PS_FIELD_PHI ? s->phi[index] : s->p);
-  memcpy(dst, data, sizeof(double) * (size_t)s->N);
+  memcpy(field_ptr(s, which, index), data, sizeof(double) * (size_t)s->N);
 }
 
 void oracle_get_field(const oracle_state* s, int which, int index, double* data) {
-  const double* src =
-      (which == PS_FIELD_W) ? s->w[index] : (which == PS_FIELD_PHI ? s->phi[index] : s->p);
-  memcpy(data, src, sizeof(double) * (size_t)s->N);
+  memcpy(data, field_ptr(s, which, index), sizeof(double) * (size_t)s->N);
 }
 
 void oracle_get_propagator(const oracle_state* s, int ip, int ib, int end, int n, double* out) {
@@ -555,6 +625,14 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     const double* w = s->w[B->cfg.field];
 #pragma omp parallel for schedule(static)
     for (long n = 0; n < N; ++n) B->wfac[n] = exp(ds2 * w[n]);
+    /* PsChargeFlexPseudoSpec::reset (pspolymer/PsChargeFlexPseudoSpec.cpp:97-130):
+     * wfac *= exp(facZ ds2 psi), facZ = za alpha L */
+    const ps_block_charge* Z = &s->cfg.block_charge[P - s->pol][ib];
+    if (Z->charged) {
+      const double facz = Z->za * Z->alpha * s->scale_length;
+      const double* psi = s->psi[Z->charge_field];
+      for (long n = 0; n < N; ++n) B->wfac[n] = B->wfac[n] * exp(facz * ds2 * psi[n]);
+    }
   }
   int guard = 0;
   const double t0 = now_s();
@@ -592,6 +670,18 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     for (long r = 0; r < N; ++r) {
       double v = densfac * B->qqt[r];
       phi[r] = phi[r] + v;
+    }
+    /* PsChargeFlexPseudoSpec::setPhysFields (pspolymer/PsChargeFlexPseudoSpec.cpp:136-165):
+     * rho += (phi_f alpha) za */
+    const ps_block_charge* Z = &s->cfg.block_charge[P - s->pol][ib];
+    if (Z->charged) {
+      double* rho = s->rho[Z->charge_field];
+      for (long r = 0; r < N; ++r) {
+        double t = 0.0 + phi[r];
+        t = t * Z->alpha;
+        t = t * Z->za;
+        rho[r] = rho[r] + t;
+      }
     }
   }
   return PS_OK;
@@ -699,6 +789,98 @@ static void solvent_update(oracle_state* s, int is) {
   for (long r = 0; r < N; ++r) phi[r] = phi[r] + wf[r] * f;
 }
 
+/* PsSimpleIons::setPhysFields (pssolvent/PsSimpleIons.cpp:90-160):
+ * e = exp(-zc psi), Q = sum(e) / N, e *= -neutralFactor / (Q zc);
+ * blockfield density = e; rho += zc e. */
+static void ions_update(oracle_state* s, int is) {
+  const long N = s->N;
+  const ps_solvent_config* S = &s->cfg.solvents[is];
+  const double* psi = s->psi[S->charge_field];
+  double* e = s->res;  /* N doubles of scratch */
+  const double negfac = -1.0 * S->zc;
+  double tot = 0.0;
+  for (long r = 0; r < N; ++r) {
+    double v = 0.0 + psi[r];
+    v = v * negfac;
+    e[r] = exp(v);
+    tot = tot + e[r];
+  }
+  const double q = tot / ((double)1 * (double)N);
+  s->solv_q[is] = q;
+  const double cfac = -S->neutral_factor / (q * S->zc);
+  for (long r = 0; r < N; ++r) e[r] = e[r] * cfac;
+  if (S->has_block_field) {
+    double* bf = s->rho[S->block_field];
+    for (long r = 0; r < N; ++r) bf[r] = 0.0 + e[r];
+  }
+  double* rho = s->rho[S->charge_field];
+  for (long r = 0; r < N; ++r) rho[r] = rho[r] + e[r] * S->zc;
+}
+
+/* PsPoissonUpdater::update (pseffhamil/PsPoissonUpdater.cpp:196-262) on every listed
+ * chargeDens field; k2 list from build_k2 (:140-175). */
+static void poisson_apply(oracle_state* s) {
+  const ps_poisson_config* P = &s->pcfg;
+  const long N = s->N;
+  const double scale = 1.0 / ((double)N);
+  for (int i = 0; i < P->n_fields; ++i) {
+    double* rho = s->rho[P->fields[i]];
+    double* psi = s->psi[P->fields[i]];
+    double sum = 0.0;
+    for (long r = 0; r < N; ++r) sum = sum + rho[r];
+    const double gcd = sum / ((double)1 * (double)N);
+    const double totc = -1.0 * gcd;
+    for (long r = 0; r < N; ++r) rho[r] = rho[r] + totc;
+    oracle_scaled_pair_buf(s->n, rho, s->kcoul, s->res, s->cwork);
+    for (long r = 0; r < N; ++r) {
+      const double psi0 = psi[r];
+      const double psi1 = s->res[r] * scale;
+      const double frac = fabs((psi1 - psi0) / psi0);
+      if (frac > 0.2) s->res[r] = psi0 * 1.2;
+    }
+    for (long r = 0; r < N; ++r) psi[r] = s->res[r] * (1.0 * scale);
+  }
+}
+
+static void post_order_set(oracle_state* s, int code, int on) {
+  int k = 0;
+  for (int i = 0; i < s->npost; ++i)
+    if (s->post[i] != code) s->post[k++] = s->post[i];
+  if (on) s->post[k++] = code;
+  s->npost = k;
+}
+
+int oracle_set_poisson(oracle_state* s, const ps_poisson_config* p) {
+  if (!p) {
+    s->has_poisson = 0;
+    post_order_set(s, 2, 0);
+    return PS_OK;
+  }
+  if (p->n_fields < 1 || p->n_fields > s->nq || p->apply_frequency < 1) return PS_ATTRIB_ERR;
+  for (int i = 0; i < p->n_fields; ++i)
+    if (p->fields[i] < 0 || p->fields[i] >= s->nq) return PS_ATTRIB_ERR;
+  if (!s->kcoul) s->kcoul = (double*)xcalloc((size_t)s->N, sizeof(double));
+  long n = 0;
+  for (int i = 0; i < s->n[0]; ++i)
+    for (int j = 0; j < s->n[1]; ++j)
+      for (int k = 0; k < s->n[2]; ++k) {
+        const double k2 = calck2(s, i, j, k);
+        s->kcoul[n++] = (k2 < 0.000000001) ? 0.0 : (4.0 * 3.1415 * p->bjerrum_len) / k2;
+      }
+  s->pcfg = *p;
+  s->has_poisson = 1;
+  post_order_set(s, 2, 1);
+  return PS_OK;
+}
+
+void oracle_apply_poisson(oracle_state* s) {
+  if (s->has_poisson) poisson_apply(s);
+}
+
+static int scheduled(long long t, long long start, long long freq, long long end) {
+  return t >= start && (end < 0 || t <= end) && (t - start) % freq == 0;
+}
+
 /* PsSimpleSpecFilter::update / applyFilter (pseffhamil/PsSimpleSpecFilter.cpp:75-140),
  * PsSpecFilterUpdater::subtractAverage and findMaxVal (pseffhamil/PsSpecFilterUpdater.cpp:
  * 180-250), scaledFFTPair and scaleFFT = 1/N. */
@@ -743,6 +925,7 @@ static void filter_apply(oracle_state* s) {
 int oracle_set_filter(oracle_state* s, const ps_filter_config* f) {
   if (!f) {
     s->has_filter = 0;
+    post_order_set(s, 1, 0);
     return PS_OK;
   }
   if (f->n_fields < 1 || f->n_fields > s->nf || f->apply_frequency < 1) return PS_ATTRIB_ERR;
@@ -773,6 +956,7 @@ int oracle_set_filter(oracle_state* s, const ps_filter_config* f) {
   }
   s->fcfg = *f;
   s->has_filter = 1;
+  post_order_set(s, 1, 1);
   return PS_OK;
 }
 
@@ -981,8 +1165,13 @@ int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
     const double t_begin = now_s();
     s->t_sweeps = 0.0;
     for (int i = 0; i < s->nf; ++i) memset(s->phi[i], 0, sizeof(double) * (size_t)N);
+    /* PsChargeDens::update: resetDensField (psphysf/PsChargeDens.cpp:180-190) */
+    for (int c = 0; c < s->nq; ++c) memset(s->rho[c], 0, sizeof(double) * (size_t)N);
     /* PsDomain::update: solvents, then polymers (pstrol/PsDomain.cpp:359-362) */
-    for (int is = 0; is < s->cfg.n_solvents; ++is) solvent_update(s, is);
+    for (int is = 0; is < s->cfg.n_solvents; ++is) {
+      if (s->cfg.solvents[is].kind == PS_SOLV_IONS) ions_update(s, is);
+      else solvent_update(s, is);
+    }
     for (int ip = 0; ip < s->npol; ++ip) {
       int rc = polymer_update(s, &s->pol[ip]);
       if (rc != PS_OK) return rc;
@@ -998,12 +1187,16 @@ int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
     }
     sc.max_incomp = mx;
     update_fields(s, &sc);
-    if (s->has_filter) {  /* PsUpdater::update schedule (psbase/PsUpdater.cpp:180-206) */
+    /* the other updaters of updaterSequence (pseffhamil/PsEffHamil.cpp:190-203), each on
+     * the PsUpdater::update schedule (psbase/PsUpdater.cpp:180-206) */
+    for (int k = 0; k < s->npost; ++k) {
       const long long t = s->iter;
-      const ps_filter_config* F = &s->fcfg;
-      if (t >= F->apply_start && (F->apply_end < 0 || t <= F->apply_end) &&
-          (t - F->apply_start) % F->apply_frequency == 0)
+      if (s->post[k] == 1 && s->has_filter &&
+          scheduled(t, s->fcfg.apply_start, s->fcfg.apply_frequency, s->fcfg.apply_end))
         filter_apply(s);
+      if (s->post[k] == 2 && s->has_poisson &&
+          scheduled(t, s->pcfg.apply_start, s->pcfg.apply_frequency, s->pcfg.apply_end))
+        poisson_apply(s);
     }
     s->t_total = now_s() - t_begin;
     s->iter++;

@@ -15,6 +15,7 @@ PS_MAX_POLYMERS = 4
 PS_MAX_FIELDS = 4
 PS_MAX_INTERACTIONS = 6
 PS_MAX_SOLVENTS = 2
+PS_MAX_CHARGES = 2
 
 PS_OK = 0
 PS_ATTRIB_ERR = 3
@@ -29,6 +30,10 @@ PS_UPD_ANDERSON = 1
 PS_FIELD_W = 0
 PS_FIELD_PHI = 1
 PS_FIELD_PRES = 2
+PS_FIELD_CHARGE = 3
+PS_FIELD_POTENTIAL = 4
+PS_SOLV_SIMPLE = 0
+PS_SOLV_IONS = 1
 PS_FROM_HEAD = 0
 PS_FROM_TAIL = 1
 
@@ -59,7 +64,14 @@ class ps_updater_config(C.Structure):
 
 
 class ps_solvent_config(C.Structure):
-    _fields_ = [("field", C.c_int), ("volfrac", C.c_double)]
+    _fields_ = [("field", C.c_int), ("volfrac", C.c_double), ("kind", C.c_int),
+                ("charge_field", C.c_int), ("has_block_field", C.c_int), ("block_field", C.c_int),
+                ("zc", C.c_double), ("neutral_factor", C.c_double)]
+
+
+class ps_block_charge(C.Structure):
+    _fields_ = [("charged", C.c_int), ("charge_field", C.c_int), ("za", C.c_double),
+                ("alpha", C.c_double)]
 
 
 class ps_config(C.Structure):
@@ -70,7 +82,9 @@ class ps_config(C.Structure):
                 ("interactions", ps_interaction_config * PS_MAX_INTERACTIONS),
                 ("updater", ps_updater_config), ("seed", C.c_ulonglong),
                 ("calc_disorder", C.c_int), ("device", C.c_int),
-                ("n_solvents", C.c_int), ("solvents", ps_solvent_config * PS_MAX_SOLVENTS)]
+                ("n_solvents", C.c_int), ("solvents", ps_solvent_config * PS_MAX_SOLVENTS),
+                ("n_charges", C.c_int),
+                ("block_charge", (ps_block_charge * PS_MAX_BLOCKS) * PS_MAX_POLYMERS)]
 
 
 class ps_filter_config(C.Structure):
@@ -78,6 +92,13 @@ class ps_filter_config(C.Structure):
                 ("cutoff_factor", C.c_double), ("filter_strength", C.c_double),
                 ("apply_start", C.c_longlong), ("apply_frequency", C.c_longlong),
                 ("apply_end", C.c_longlong), ("spec_cells", C.c_int * 3), ("pad", C.c_int)]
+
+
+class ps_poisson_config(C.Structure):
+    _fields_ = [("n_fields", C.c_int), ("fields", C.c_int * PS_MAX_CHARGES),
+                ("bjerrum_len", C.c_double), ("relaxlambda", C.c_double),
+                ("apply_start", C.c_longlong), ("apply_frequency", C.c_longlong),
+                ("apply_end", C.c_longlong)]
 
 
 class ps_scalars(C.Structure):
@@ -122,6 +143,8 @@ SIGNATURES = {
     "ps_gpu_set_precision": (C.c_int, [_vp, C.c_int]),
     "ps_gpu_set_spectral_filter": (C.c_int, [_vp, C.POINTER(ps_filter_config)]),
     "ps_gpu_apply_spectral_filter": (C.c_int, [_vp]),
+    "ps_gpu_set_poisson": (C.c_int, [_vp, C.POINTER(ps_poisson_config)]),
+    "ps_gpu_apply_poisson": (C.c_int, [_vp]),
     "ps_gpu_sweep_timing": (C.c_int, [_vp, _dbl_p, C.c_int, C.POINTER(C.c_int), _dbl_p,
                                       C.POINTER(C.c_longlong)]),
     "ps_gpu_batch_create": (C.c_int, [C.POINTER(ps_config), C.c_int, C.POINTER(_vp)]),

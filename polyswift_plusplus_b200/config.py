@@ -46,6 +46,10 @@ class Block:
     bseg_ratio: float = 1.0
     force_block_steps: bool = False
     kind: str = "flexPseudoSpec"
+    # chargeFlexPseudoSpec (pspolymer/PsChargeFlexPseudoSpec.cpp:42-75)
+    chargefield: str | None = None
+    za: float = 0.0
+    alpha: float = 0.0
 
 
 @dataclass
@@ -67,11 +71,44 @@ class Interaction:
 
 @dataclass
 class Solvent:
-    """<Solvent name> kind = simpleSolvent (psbase/PsSolvent.cpp:40-60)."""
+    """<Solvent name> kind = simpleSolvent | simpleIons (psbase/PsSolvent.cpp:40-60,
+    pssolvent/PsSimpleIons.cpp:30-60)."""
     name: str
     scfield: str
     volfrac: float
     kind: str = "simpleSolvent"
+    # simpleIons
+    chargefield: str | None = None
+    blockfield: str | None = None
+    zc: float = 0.0
+    neutral_factor: float = 0.0
+
+
+@dataclass
+class PoissonUpdater:
+    """<Updater name> kind = poissonUpdater (pseffhamil/PsPoissonUpdater.cpp:50-95,
+    psbase/PsUpdater.cpp:60-120)."""
+    name: str = "poisson"
+    updatefields: list = field(default_factory=list)   # chargeDens PhysFields
+    bjerrum_len: float = 1.0
+    relaxlambda: float = 1.0
+    apply_start: int = 0
+    apply_frequency: int = 1
+    apply_end: int = -1
+
+    def to_ps(self, cfg: "ScftConfig") -> A.ps_poisson_config:
+        p = A.ps_poisson_config()
+        if not 1 <= len(self.updatefields) <= A.PS_MAX_CHARGES:
+            raise ValueError("poissonUpdater: updatefields out of range")
+        p.n_fields = len(self.updatefields)
+        for i, name in enumerate(self.updatefields):
+            p.fields[i] = cfg.charge_index(name)
+        p.bjerrum_len = float(self.bjerrum_len)
+        p.relaxlambda = float(self.relaxlambda)
+        p.apply_start = int(self.apply_start)
+        p.apply_frequency = int(self.apply_frequency)
+        p.apply_end = int(self.apply_end)
+        return p
 
 
 @dataclass
@@ -131,6 +168,25 @@ class ScftConfig:
     device: int = 0
     solvents: list = field(default_factory=list)  # Solvent entries
     spec_filter: "SpecFilter | None" = None       # simpleSpecFilter updater
+    charge_fields: list = field(default_factory=list)  # chargeDens PhysFields in declaration order
+    poisson: "PoissonUpdater | None" = None
+    updater_sequence: list | None = None         # names; None: filter, then Poisson
+
+    def post_updaters(self) -> list:
+        """The updaters that run after the field updater, in updaterSequence order
+        (pseffhamil/PsEffHamil.cpp:190-203): ("filter", SpecFilter) / ("poisson", PoissonUpdater)."""
+        items = [(u.name, k, u) for k, u in (("filter", self.spec_filter), ("poisson", self.poisson))
+                 if u is not None]
+        if self.updater_sequence is not None:
+            seq = list(self.updater_sequence)
+            items = sorted((t for t in items if t[0] in seq), key=lambda t: seq.index(t[0]))
+        return [(k, u) for _, k, u in items]
+
+    def charge_index(self, name: str) -> int:
+        try:
+            return self.charge_fields.index(name)
+        except ValueError as e:
+            raise ValueError(f"unknown chargeDens PhysField {name!r}; declared: {self.charge_fields}") from e
 
     @property
     def n_total(self) -> int:
@@ -183,6 +239,12 @@ class ScftConfig:
                     cb.head_joined[k] = v
                 for k, v in enumerate(tails):
                     cb.tail_joined[k] = v
+                if B.chargefield is not None:
+                    z = c.block_charge[ip][ib]
+                    z.charged = 1
+                    z.charge_field = self.charge_index(B.chargefield)
+                    z.za = float(B.za)
+                    z.alpha = float(B.alpha)
         if len(self.interactions) > A.PS_MAX_INTERACTIONS:
             raise ValueError("too many interactions")
         c.n_interactions = len(self.interactions)
@@ -207,11 +269,25 @@ class ScftConfig:
         if len(self.solvents) > A.PS_MAX_SOLVENTS:
             raise ValueError("too many solvents")
         c.n_solvents = len(self.solvents)
+        if len(self.charge_fields) > A.PS_MAX_CHARGES:
+            raise ValueError("too many chargeDens PhysFields")
+        c.n_charges = len(self.charge_fields)
         for i_s, S in enumerate(self.solvents):
-            if S.kind not in ("simpleSolvent", "simpleSolventGPU"):
+            cs = c.solvents[i_s]
+            cs.field = self.field_index(S.scfield)
+            cs.volfrac = float(S.volfrac)
+            if S.kind in ("simpleSolvent", "simpleSolventGPU"):
+                cs.kind = A.PS_SOLV_SIMPLE
+            elif S.kind == "simpleIons":
+                cs.kind = A.PS_SOLV_IONS
+                cs.charge_field = self.charge_index(S.chargefield)
+                if S.blockfield is not None:
+                    cs.has_block_field = 1
+                    cs.block_field = self.charge_index(S.blockfield)
+                cs.zc = float(S.zc)
+                cs.neutral_factor = float(S.neutral_factor)
+            else:
                 raise ValueError(f"Solvent kind {S.kind!r} is not on the device path")
-            c.solvents[i_s].field = self.field_index(S.scfield)
-            c.solvents[i_s].volfrac = float(S.volfrac)
         c.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
         c.calc_disorder = 1
         c.device = int(self.device)
@@ -307,11 +383,13 @@ def config_from_text(text: str) -> ScftConfig:
     g = grids[0][1]["attrs"]
     n = tuple(int(v) for v in g["numCellsGlobal"])
     cell = tuple(float(v) for v in g["cellSizes"])
-    fields, has_pressure = [], False
+    fields, charge_fields, has_pressure = [], [], False
     for name, node in _find(root, "PhysField"):
         kind = node["attrs"].get("kind", "")
         if kind == "monomerDens":
             fields.append(name)
+        elif kind == "chargeDens":
+            charge_fields.append(name)
         elif kind == "constraint":
             has_pressure = True
         else:
@@ -326,8 +404,16 @@ def config_from_text(text: str) -> ScftConfig:
         blocks = []
         for bname, bnode in _find(pnode, "Block"):
             ba = bnode["attrs"]
-            if ba.get("kind", "flexPseudoSpec") not in ("flexPseudoSpec", "flexPseudoSpecGPU"):
+            bkind = str(ba.get("kind", "flexPseudoSpec"))
+            if bkind not in ("flexPseudoSpec", "flexPseudoSpecGPU", "chargeFlexPseudoSpec"):
                 raise InputError(f"Block kind {ba.get('kind')!r} is not on the device path")
+            charge = {}
+            if bkind == "chargeFlexPseudoSpec":
+                for key in ("za", "alpha", "chargefield"):
+                    if key not in ba:
+                        raise InputError(f"PsChargeFlexPseudoSpec::setAttrib: {key} not set in <Block {bname}>")
+                charge = dict(chargefield=str(ba["chargefield"]), za=float(ba["za"]),
+                              alpha=float(ba["alpha"]))
             if "ds" not in ba:
                 raise InputError(f"PsBlockBase::setAttrib: ds not set in <Block {bname}>")
             if "headjoined" not in ba or "tailjoined" not in ba:
@@ -339,18 +425,27 @@ def config_from_text(text: str) -> ScftConfig:
                                 lengthfrac=float(ba.get("lengthfrac", 0.0)),
                                 headjoined=[str(x) for x in hj], tailjoined=[str(x) for x in tj],
                                 bseg_ratio=float(ba.get("bSegRatio", 1.0)),
-                                force_block_steps=fbs in (1, "on", "true", "1")))
+                                force_block_steps=fbs in (1, "on", "true", "1"), kind=bkind,
+                                **charge))
         polymers.append(Polymer(name=pname, volfrac=float(pa.get("volfrac", 1.0)),
                                 length=int(pa.get("length", 1)), blocks=blocks))
     solvents = []
     for sname, snode in _find(root, "Solvent"):
         sa = snode["attrs"]
         kind = str(sa.get("kind", "simpleSolvent"))
-        if kind not in ("simpleSolvent", "simpleSolventGPU"):
+        if kind not in ("simpleSolvent", "simpleSolventGPU", "simpleIons"):
             raise InputError(f"Solvent kind {kind!r} is not on the device path")
+        ions = {}
+        if kind == "simpleIons":
+            for key in ("zc", "neutralFactor", "chargefield"):
+                if key not in sa:
+                    raise InputError(f"PsSimpleIons::setAttrib: {key} not set in <Solvent {sname}>")
+            ions = dict(chargefield=str(sa["chargefield"]), zc=float(sa["zc"]),
+                        neutral_factor=float(sa["neutralFactor"]),
+                        blockfield=str(sa["blockfield"]) if "blockfield" in sa else None)
         solvents.append(Solvent(name=sname, scfield=str(sa["scfield"]),
-                                volfrac=float(sa.get("volfrac", 0.0)), kind=kind))
-    interactions, updater, spec_filter = [], None, None
+                                volfrac=float(sa.get("volfrac", 0.0)), kind=kind, **ions))
+    interactions, updater, spec_filter, poisson, sequence = [], None, None, None, None
     for hname, hnode in _find(root, "EffHamil"):
         for iname, inode in _find(hnode, "Interaction"):
             ia = inode["attrs"]
@@ -361,18 +456,39 @@ def config_from_text(text: str) -> ScftConfig:
         ups = _find(hnode, "Updater")
         fkinds = ("simpleSpecFilter", "multiSpecFilter")
         filters = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) in fkinds]
-        ups = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) not in fkinds]
+        poissons = [(n, u) for n, u in ups if str(u["attrs"].get("kind", "")) == "poissonUpdater"]
+        ups = [(n, u) for n, u in ups
+               if str(u["attrs"].get("kind", "")) not in fkinds + ("poissonUpdater",)]
         # PsEffHamil::update runs the updaters named in updaterSequence, in its order
         # (pseffhamil/PsEffHamil.cpp:190-203)
         seq = hnode["attrs"].get("updaterSequence")
         seq = [str(x) for x in (seq if isinstance(seq, list) else [seq])] if seq is not None else None
         if seq is not None:
+            sequence = seq
             filters = [(n, u) for n, u in filters if n in seq]
-            if ups and filters and ups[0][0] in seq and seq.index(filters[0][0]) < seq.index(ups[0][0]):
-                raise InputError("a spectral filter before the field updater in updaterSequence "
-                                 "is not on the device path")
+            poissons = [(n, u) for n, u in poissons if n in seq]
+            if ups and ups[0][0] in seq:
+                for uname_, _u in filters + poissons:
+                    if seq.index(uname_) < seq.index(ups[0][0]):
+                        raise InputError(f"updater {uname_!r} before the field updater in updaterSequence "
+                                         "is not on the device path")
         if len(filters) > 1:
             raise InputError("one spectral filter per run is on the device path")
+        if len(poissons) > 1:
+            raise InputError("one poissonUpdater per run is on the device path")
+        if poissons:
+            pname, pnode = poissons[0]
+            pa = pnode["attrs"]
+            for key in ("relaxlambda", "bjerrumLen"):
+                if key not in pa:
+                    raise InputError(f"PsPoissonUpdater::setAttrib: {key} not set")
+            upf = pa.get("updatefields", [])
+            poisson = PoissonUpdater(name=pname, updatefields=[str(x) for x in (upf if isinstance(upf, list) else [upf])],
+                                     bjerrum_len=float(pa["bjerrumLen"]),
+                                     relaxlambda=float(pa["relaxlambda"]),
+                                     apply_start=int(pa.get("applyStart", 0)),
+                                     apply_frequency=int(pa.get("applyFrequency", 1)),
+                                     apply_end=int(pa.get("applyEnd", -1)))
         if filters:
             fname, fnode = filters[0]
             fa = fnode["attrs"]
@@ -410,7 +526,8 @@ def config_from_text(text: str) -> ScftConfig:
     return ScftConfig(n=n, cell=cell, fields=fields, polymers=polymers, interactions=interactions,
                       updater=updater, seed=int(ra.get("randomSeed", 0)),
                       precision=str(ra.get("precision", "fp64")), nsteps=int(ra.get("nsteps", 1)),
-                      device=int(ra.get("device", 0)), solvents=solvents, spec_filter=spec_filter)
+                      device=int(ra.get("device", 0)), solvents=solvents, spec_filter=spec_filter,
+                      charge_fields=charge_fields, poisson=poisson, updater_sequence=sequence)
 
 
 def config_from_file(path: str | Path) -> ScftConfig:

@@ -319,7 +319,7 @@ struct Builder {
   const double* wf(int b) const {
     const BlockMap& bm = h->blocks[0][b];
     for (size_t i = 0; i < h->wfac_keys.size(); ++i)
-      if (h->wfac_keys[i].first == bm.field && h->wfac_keys[i].second == bm.ds) return h->bd.wfac[i];
+      if (h->wfac_keys[i].field == bm.field && h->wfac_keys[i].ds == bm.ds) return h->bd.wfac[i];
     return nullptr;
   }
   int ktab(int b) const {
@@ -554,7 +554,7 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
     a->err = "the adjoint runs in FP64 (precision must be PS_PREC_FP64)";
     return PS_ATTRIB_ERR;
   }
-  if (cfg->n_polymers != 1 || cfg->n_solvents != 0) {
+  if (cfg->n_polymers != 1 || cfg->n_solvents != 0 || cfg->n_charges != 0) {
     a->err = "the adjoint takes one polymer (a linear block copolymer melt) and no solvent";
     return PS_INPUT_ERR;
   }

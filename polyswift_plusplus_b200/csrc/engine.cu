@@ -272,10 +272,18 @@ static int launch_pre(ps_handle* h, long long* nlaunch) {
   const long long N = h->N;
   PS_CUDA(h, launch_zero(h->d_phi, (long long)h->nf * N, h->st));
   ++*nlaunch;
+  if (h->nq > 0) {
+    // PsChargeDens::update: resetDensField (psphysf/PsChargeDens.cpp:180-190)
+    PS_CUDA(h, launch_zero(h->d_rho, (long long)h->nq * N, h->st));
+    ++*nlaunch;
+  }
   for (size_t i = 0; i < h->wfac_keys.size(); ++i) {
-    const int f = h->wfac_keys[i].first;
-    const double ds = h->wfac_keys[i].second;
-    PS_CUDA(h, launch_wfac<T>(h->d_w + (size_t)f * N, B.wfac[i], -0.5 * ds, N, h->st));
+    const WfacKey& k = h->wfac_keys[i];
+    if (k.charge_field < 0)
+      PS_CUDA(h, launch_wfac<T>(h->d_w + (size_t)k.field * N, B.wfac[i], -0.5 * k.ds, N, h->st));
+    else
+      PS_CUDA(h, launch_wfac_charged<T>(h->d_w + (size_t)k.field * N, h->d_psi + (size_t)k.charge_field * N,
+                                        B.wfac[i], -0.5 * k.ds, k.facz, N, h->st));
     ++*nlaunch;
   }
   return PS_OK;
@@ -308,8 +316,13 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
   // solvents before polymers (PsDomain::update, pstrol/PsDomain.cpp:359-362)
   for (int is = 0; is < h->cfg.n_solvents; ++is) {
     const ps_solvent_config& S = h->cfg.solvents[is];
-    PS_CUDA(h, launch_solvent(h->d_w + (size_t)S.field * N, -1.0 / h->fm.scale_len, S.volfrac, N, is,
-                              h->d_qpart, h->d_sc, h->d_phi + (size_t)S.field * N, h->st));
+    if (S.kind == PS_SOLV_IONS)
+      PS_CUDA(h, launch_ions(h->d_psi + (size_t)S.charge_field * N, S.zc, S.neutral_factor, N, is,
+                             h->d_qpart, h->d_sc, h->d_rho + (size_t)S.charge_field * N,
+                             S.has_block_field ? h->d_rho + (size_t)S.block_field * N : nullptr, h->st));
+    else
+      PS_CUDA(h, launch_solvent(h->d_w + (size_t)S.field * N, -1.0 / h->fm.scale_len, S.volfrac, N, is,
+                                h->d_qpart, h->d_sc, h->d_phi + (size_t)S.field * N, h->st));
     *nlaunch += 3;
   }
   for (int ip = 0; ip < h->cfg.n_polymers; ++ip) {
@@ -329,6 +342,13 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
                                       b.steps, N, b.ds, densfac, h->d_sc, ip,
                                       h->d_phi + (size_t)b.field * N, h->st));
       ++*nlaunch;
+      if (b.charge_field >= 0) {
+        // the charged block is the only density source of its field, so phi_f here
+        // is what PsChargeFlexPseudoSpec::setPhysFields reads
+        PS_CUDA(h, launch_charge_accum(h->d_phi + (size_t)b.field * N, b.qalpha, b.za, N,
+                                       h->d_rho + (size_t)b.charge_field * N, h->st));
+        ++*nlaunch;
+      }
     }
   }
   FieldPtrs fp;
@@ -449,10 +469,11 @@ template <typename T> static void free_buffers(Buffers<T>& B) {
 
 static void free_all(ps_handle* h) {
   filter_free(h);
+  poisson_free(h);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   auto f = [](void* p) { if (p) cudaFree(p); };
-  f(h->d_w); f(h->d_phi); f(h->d_p); f(h->d_noise);
+  f(h->d_w); f(h->d_phi); f(h->d_p); f(h->d_noise); f(h->d_rho); f(h->d_psi);
   if (h->h_noise) cudaFreeHost(h->h_noise);
   free_buffers(h->bf);
   free_buffers(h->bd);
@@ -556,6 +577,21 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
       bm.field = B.field;
       bm.ds = B.ds;
       bm.bseg = (B.bseg_ratio > 0.0) ? B.bseg_ratio : 1.0;
+      const ps_block_charge& Z = c.block_charge[ip][ib];
+      bm.charge_field = -1;
+      if (Z.charged) {
+        if (c.n_charges < 1 || c.n_charges > PS_MAX_CHARGES || Z.charge_field < 0 ||
+            Z.charge_field >= c.n_charges) {
+          h->err = "polymer " + std::to_string(ip) + " block " + std::to_string(ib) +
+                   ": chargefield out of range";
+          return PS_ATTRIB_ERR;
+        }
+        bm.charge_field = Z.charge_field;
+        bm.za = Z.za;
+        bm.qalpha = Z.alpha;
+        // facZ = za alpha N (pspolymer/PsChargeFlexPseudoSpec.cpp:104-106)
+        bm.facz = Z.za * Z.alpha * scale_len;
+      }
       h->blocks[ip].push_back(bm);
     }
   }
@@ -565,14 +601,49 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
     h->err = "n_solvents out of range";
     return PS_ATTRIB_ERR;
   }
+  if (c.n_charges < 0 || c.n_charges > PS_MAX_CHARGES) {
+    h->err = "n_charges out of range";
+    return PS_ATTRIB_ERR;
+  }
+  h->nq = c.n_charges;
   for (int is = 0; is < c.n_solvents; ++is) {
     const ps_solvent_config& S = c.solvents[is];
     if (S.field < 0 || S.field >= h->nf) {
       h->err = "solvent " + std::to_string(is) + ": scfield out of range";
       return PS_ATTRIB_ERR;
     }
-    dens_avg[S.field] = dens_avg[S.field] + S.volfrac;
+    if (S.kind == PS_SOLV_IONS) {
+      if (S.charge_field < 0 || S.charge_field >= h->nq ||
+          (S.has_block_field && (S.block_field < 0 || S.block_field >= h->nq)) || S.zc == 0.0) {
+        h->err = "solvent " + std::to_string(is) +
+                 ": simpleIons needs chargefield (and blockfield) and zc != 0";
+        return PS_ATTRIB_ERR;
+      }
+    } else if (S.kind == PS_SOLV_SIMPLE) {
+      dens_avg[S.field] = dens_avg[S.field] + S.volfrac;
+    } else {
+      h->err = "solvent " + std::to_string(is) + ": unknown kind";
+      return PS_ATTRIB_ERR;
+    }
   }
+  // A charged block must be the only density source of its scfield: its
+  // rho += za alpha phi_f then sees its own density, as the reference's does.
+  for (int ip = 0; ip < c.n_polymers; ++ip)
+    for (size_t ib = 0; ib < h->blocks[ip].size(); ++ib) {
+      const BlockMap& b = h->blocks[ip][ib];
+      if (b.charge_field < 0) continue;
+      int others = 0;
+      for (int jp = 0; jp < c.n_polymers; ++jp)
+        for (size_t jb = 0; jb < h->blocks[jp].size(); ++jb)
+          if ((jp != ip || jb != ib) && h->blocks[jp][jb].field == b.field) ++others;
+      for (int is = 0; is < c.n_solvents; ++is)
+        if (c.solvents[is].kind == PS_SOLV_SIMPLE && c.solvents[is].field == b.field) ++others;
+      if (others) {
+        h->err = "polymer " + std::to_string(ip) + " block " + std::to_string(ib) +
+                 ": a charged block must be the only density source of its scfield";
+        return PS_INPUT_ERR;
+      }
+    }
   double vsolv = 0.0;
   for (int is = 0; is < c.n_solvents; ++is) vsolv += c.solvents[is].volfrac;
   vtot = vsolv + vtot;
@@ -616,7 +687,8 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
     for (size_t i = 0; same && i < a.segs.size(); ++i) {
       const BlockMap& x = h->blocks[ip][a.segs[i].block];
       const BlockMap& y = h->blocks[ip][b.segs[i].block];
-      same = (x.field == y.field && x.steps == y.steps && x.ds == y.ds && x.bseg == y.bseg);
+      same = (x.field == y.field && x.steps == y.steps && x.ds == y.ds && x.bseg == y.bseg &&
+              x.charge_field == y.charge_field && x.facz == y.facz);
     }
     const int ia = (int)h->sweeps.size();
     a.storage = (int)h->exec.size();
@@ -642,7 +714,7 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   for (Sweep& sw : h->sweeps)
     for (Seg& g : sw.segs) {
       const BlockMap& bm = h->blocks[sw.polymer][g.block];
-      std::pair<int, double> wk(bm.field, bm.ds);
+      WfacKey wk{bm.field, bm.ds, bm.charge_field, bm.charge_field >= 0 ? bm.facz : 0.0};
       auto it = std::find(h->wfac_keys.begin(), h->wfac_keys.end(), wk);
       if (it == h->wfac_keys.end()) {
         g.wfac_id = (int)h->wfac_keys.size();
@@ -721,6 +793,13 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   PS_CUDA(h, cudaMemset(h->d_w, 0, sizeof(double) * nfN));
   PS_CUDA(h, cudaMemset(h->d_phi, 0, sizeof(double) * nfN));
   PS_CUDA(h, cudaMemset(h->d_p, 0, sizeof(double) * (size_t)h->N));
+  if (h->nq > 0) {
+    const size_t qN = (size_t)h->nq * h->N;
+    PS_CUDA(h, cudaMalloc((void**)&h->d_rho, sizeof(double) * qN));
+    PS_CUDA(h, cudaMalloc((void**)&h->d_psi, sizeof(double) * qN));
+    PS_CUDA(h, cudaMemset(h->d_rho, 0, sizeof(double) * qN));
+    PS_CUDA(h, cudaMemset(h->d_psi, 0, sizeof(double) * qN));
+  }
   if (c.updater.noise != 0.0) {
     PS_CUDA(h, cudaMalloc((void**)&h->d_noise, sizeof(double) * nfN));
     PS_CUDA(h, cudaMallocHost((void**)&h->h_noise, sizeof(double) * nfN));
@@ -836,9 +915,10 @@ static int iterate_impl(ps_handle* h, int n) {
       }
       PS_CUDA(h, cudaGraphLaunch(h->gexec, h->st));
     }
-    if (h->filter) {
-      // updaterSequence order: the filter runs after the field updater of the same step
-      int rc = filter_after_iteration(h, h->iterations);
+    // updaterSequence order: these run after the field updater of the same step
+    for (int code : h->post_order) {
+      int rc = (code == POST_FILTER) ? filter_after_iteration(h, h->iterations)
+                                     : poisson_after_iteration(h, h->iterations);
       if (rc) return rc;
     }
     h->iterations++;
@@ -847,6 +927,14 @@ static int iterate_impl(ps_handle* h, int n) {
 }
 
 int engine_create(ps_handle* h, const ps_config* cfg) { return create_impl(h, cfg); }
+
+void post_order_set(ps_handle* h, int code, bool on) {
+  std::vector<int> o;
+  for (int c : h->post_order)
+    if (c != code) o.push_back(c);
+  if (on) o.push_back(code);
+  h->post_order = o;
+}
 
 void engine_free(ps_handle* h) { free_all(h); }
 
@@ -900,6 +988,10 @@ int ps_gpu_block_steps(const ps_handle* h, int ip, int ib, int* steps) {
 
 static double* field_ptr(ps_handle* h, int which, int index) {
   if (which == PS_FIELD_PRES) return h->d_p;
+  if (which == PS_FIELD_CHARGE || which == PS_FIELD_POTENTIAL) {
+    if (index < 0 || index >= h->nq) return nullptr;
+    return (which == PS_FIELD_CHARGE ? h->d_rho : h->d_psi) + (size_t)index * h->N;
+  }
   if (index < 0 || index >= h->nf) return nullptr;
   if (which == PS_FIELD_W) return h->d_w + (size_t)index * h->N;
   if (which == PS_FIELD_PHI) return h->d_phi + (size_t)index * h->N;

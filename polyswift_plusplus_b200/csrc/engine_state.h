@@ -31,10 +31,24 @@ struct Sweep {
   int storage = -1;  // index of the executed sweep holding its slices
 };
 
+// Boltzmann-factor table key: one wfac array per distinct (field, ds, charge)
+// (charge_field -1: flexPseudoSpec; else chargeFlexPseudoSpec with facz = za alpha L).
+struct WfacKey {
+  int field;
+  double ds;
+  int charge_field;
+  double facz;
+  bool operator==(const WfacKey& o) const {
+    return field == o.field && ds == o.ds && charge_field == o.charge_field && facz == o.facz;
+  }
+};
+
 struct BlockMap {
   int steps;
   int field;
   double ds, bseg;
+  int charge_field;  // -1: not charged
+  double za, qalpha, facz;
   int sweep_head, off_head;  // qs[n]  = slices(sweep_head)[off_head + n]
   int sweep_tail, off_tail;  // qts[n] = slices(sweep_tail)[off_tail + n]
 };
@@ -73,12 +87,15 @@ struct ps_handle {
   double* d_p = nullptr;
   double* d_noise = nullptr;
   double* h_noise = nullptr;  // pinned
+  int nq = 0;                 // chargeDens PhysFields
+  double* d_rho = nullptr;    // nq*N charge densities
+  double* d_psi = nullptr;    // nq*N electric potentials
 
   std::vector<std::vector<psb::BlockMap>> blocks;
   std::vector<double> alpha;  // length ratios
   std::vector<psb::Sweep> sweeps;
   std::vector<int> exec;  // sweep indices that are executed (own storage)
-  std::vector<std::pair<int, double>> wfac_keys;
+  std::vector<psb::WfacKey> wfac_keys;
   std::vector<std::pair<double, double>> ktab_keys;
   int kmax = 0;
   std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
@@ -116,6 +133,8 @@ struct ps_handle {
   bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
   bool no_slices = false; // tables only, no slice storage (the adjoint keeps its own)
   void* filter = nullptr;  // spectral filter updater (filter.cu), or nullptr
+  void* poisson = nullptr; // Poisson updater (poisson.cu), or nullptr
+  std::vector<int> post_order;  // updaters after the field update, in run order (POST_*)
 
   psb::Mt19937 rng;
   long long pending_gauss = 0;  // Gaussian draws owed to the stream (noise = 0)
@@ -156,6 +175,12 @@ void engine_free(ps_handle* h);
 // when its schedule says so; freed with the handle.
 int filter_after_iteration(ps_handle* h, long long step);
 void filter_free(ps_handle* h);
+// Poisson updater (poisson.cu), the same way.
+int poisson_after_iteration(ps_handle* h, long long step);
+void poisson_free(ps_handle* h);
+// Updaters that run after the field update, in h->post_order.
+enum { POST_FILTER = 1, POST_POISSON = 2 };
+void post_order_set(ps_handle* h, int code, bool on);
 int engine_pre(ps_handle* h, long long* nlaunch);
 int engine_post(ps_handle* h, long long* nlaunch);
 // Host-side random-number bookkeeping owed before each iteration.

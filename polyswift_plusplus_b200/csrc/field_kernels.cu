@@ -189,6 +189,94 @@ cudaError_t launch_solvent(const double* w, double neg_inv_len, double volfrac, 
 }
 
 // ---------------------------------------------------------------------------
+// chargeFlexPseudoSpec Boltzmann factor (pspolymer/PsChargeFlexPseudoSpec.cpp:97-130):
+// wfac = exp(ds2 w) exp(facZ ds2 psi), facZ = za alpha L.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void wfac_charged_kernel(const double* __restrict__ w, const double* __restrict__ psi,
+                                    T* __restrict__ wfac, double ds2, double facz, long long N) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x)
+    wfac[i] = (T)(exp(ds2 * w[i]) * exp(facz * ds2 * psi[i]));
+}
+
+template <typename T>
+cudaError_t launch_wfac_charged(const double* w, const double* psi, T* wfac, double ds2, double facz,
+                                long long N, cudaStream_t st) {
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  wfac_charged_kernel<T><<<blocks, 256, 0, st>>>(w, psi, wfac, ds2, facz, N);
+  return cudaGetLastError();
+}
+template cudaError_t launch_wfac_charged<float>(const double*, const double*, float*, double, double,
+                                                long long, cudaStream_t);
+template cudaError_t launch_wfac_charged<double>(const double*, const double*, double*, double, double,
+                                                 long long, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// simpleIons (pssolvent/PsSimpleIons.cpp:90-160): e = exp(-zc psi),
+// Q = sum(e) / N, e *= -neutralFactor / (Q zc); blockfield = e; rho += zc e.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ion_factor(double psi, double negfac) {
+  double v = 0.0 + psi;
+  v = v * negfac;
+  return exp(v);
+}
+
+__global__ void ions_partials_kernel(const double* __restrict__ psi, double negfac, long long N,
+                                     double* __restrict__ partials) {
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < N;
+       i += (long long)kRedBlocks * kRedThreads)
+    v[0] += ion_factor(psi[i], negfac);
+  block_reduce_write<1>(v, 0u, partials + blockIdx.x);
+}
+
+__global__ void ions_density_kernel(const double* __restrict__ psi, double zc, double neutral_factor,
+                                    long long N, int is, const DevScalars* __restrict__ sc,
+                                    double* __restrict__ rho, double* __restrict__ block_rho) {
+  const double cfac = -neutral_factor / (sc->solv_q[is] * zc);
+  const double negfac = -1.0 * zc;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    const double e = ion_factor(psi[r], negfac) * cfac;
+    if (block_rho) block_rho[r] = 0.0 + e;
+    rho[r] = rho[r] + e * zc;
+  }
+}
+
+cudaError_t launch_ions(const double* psi, double zc, double neutral_factor, long long N, int is,
+                        double* partials, DevScalars* sc, double* rho, double* block_rho,
+                        cudaStream_t st) {
+  ions_partials_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(psi, -1.0 * zc, N, partials);
+  solvent_finalize_kernel<<<1, kRedThreads, 0, st>>>(partials, (double)N, is, sc);
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  ions_density_kernel<<<blocks, 256, 0, st>>>(psi, zc, neutral_factor, N, is, sc, rho, block_rho);
+  return cudaGetLastError();
+}
+
+// rho += (phi alpha) za   (pspolymer/PsChargeFlexPseudoSpec.cpp:136-165)
+__global__ void charge_accum_kernel(const double* __restrict__ phi, double alpha, double za, long long N,
+                                    double* __restrict__ rho) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    double t = 0.0 + phi[r];
+    t = t * alpha;
+    t = t * za;
+    rho[r] = rho[r] + t;
+  }
+}
+
+cudaError_t launch_charge_accum(const double* phi, double alpha, double za, long long N, double* rho,
+                                cudaStream_t st) {
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  charge_accum_kernel<<<blocks, 256, 0, st>>>(phi, alpha, za, N, rho);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Contour quadrature (pspolymer/PsBlock.cpp:255-380) and density update
 // (pspolymer/PsBlock.cpp:153-196): extended Simpson with the reference's
 // 0.33333 factor, trapezoid on the last interval for an even point count.

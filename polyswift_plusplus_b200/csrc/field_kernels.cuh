@@ -82,6 +82,22 @@ cudaError_t launch_zero(double* p, long long n, cudaStream_t st);
 cudaError_t launch_solvent(const double* w, double neg_inv_len, double volfrac, long long N, int is,
                            double* partials, DevScalars* sc, double* phi, cudaStream_t st);
 
+// chargeFlexPseudoSpec: wfac = exp(ds2 w) exp(facz ds2 psi) rounded to T.
+template <typename T>
+cudaError_t launch_wfac_charged(const double* w, const double* psi, T* wfac, double ds2, double facz,
+                                long long N, cudaStream_t st);
+
+// simpleIons (pssolvent/PsSimpleIons.cpp:90-160): Q = <exp(-zc psi)> into
+// sc->solv_q[is]; e = exp(-zc psi) (-neutral_factor / (Q zc)); block_rho = e
+// (when not null); rho += zc e.
+cudaError_t launch_ions(const double* psi, double zc, double neutral_factor, long long N, int is,
+                        double* partials, DevScalars* sc, double* rho, double* block_rho,
+                        cudaStream_t st);
+
+// rho += (phi alpha) za after a charged block's density.
+cudaError_t launch_charge_accum(const double* phi, double alpha, double za, long long N, double* rho,
+                                cudaStream_t st);
+
 // Steepest-descent update, pressure rebuild and free-energy partial sums.
 cudaError_t launch_sd_update(const FieldModel& fm, const FieldPtrs& fp, double* partials,
                              cudaStream_t st);

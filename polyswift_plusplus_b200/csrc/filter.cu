@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine_state.h"
+#include "spectral.cuh"
 
 namespace psb {
 
@@ -125,8 +126,6 @@ static Regions regions_of(const ps_handle* h, const ps_filter_config& c) {
   return g;
 }
 
-constexpr int kFT = 256;
-
 __global__ void filter_sum_partials(const double* __restrict__ w, long long N, double* __restrict__ part,
                                     int is_max, const double2* __restrict__ spec) {
   __shared__ double sh[kFT];
@@ -181,7 +180,7 @@ __global__ void filter_mask(double2* __restrict__ spec, long long n, const doubl
   }
 }
 
-static cudaError_t twiddles64(double2** dst, int L) {
+cudaError_t twiddles64(double2** dst, int L) {
   std::vector<double2> tw(L > 0 ? L : 1);
   const double twopi = 2.0 * acos(-1.0);
   for (int m = 0; m < L; ++m) tw[m] = make_double2(cos(twopi * m / L), -sin(twopi * m / L));
@@ -316,6 +315,7 @@ int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* c) {
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   filter_free(h);
+  post_order_set(h, POST_FILTER, false);
   if (!c) return PS_OK;
   if (c->n_fields < 1 || c->n_fields > h->nf) {
     h->err = "spectral filter: n_fields out of range";
@@ -349,6 +349,7 @@ int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* c) {
     filter_free(h);
     return rc;
   }
+  post_order_set(h, POST_FILTER, true);
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   return PS_OK;
 }

@@ -34,8 +34,13 @@ class ScftSolver:
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
         self.t = 0
-        if self._owned and getattr(cfg, "spec_filter", None) is not None:
-            self.set_spectral_filter(cfg.spec_filter)
+        if self._owned:
+            # updaters after the field updater, installed in updaterSequence order
+            for kind, u in cfg.post_updaters():
+                if kind == "filter":
+                    self.set_spectral_filter(u)
+                else:
+                    self.set_poisson(u)
 
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -113,6 +118,14 @@ class ScftSolver:
     def pressure(self) -> np.ndarray:
         return self.get_field(A.PS_FIELD_PRES, 0)
 
+    def rho(self, c: int) -> np.ndarray:
+        """Charge density of chargeDens field c."""
+        return self.get_field(A.PS_FIELD_CHARGE, c)
+
+    def psi(self, c: int) -> np.ndarray:
+        """Electric potential of chargeDens field c."""
+        return self.get_field(A.PS_FIELD_POTENTIAL, c)
+
     # -- iterations -------------------------------------------------------
     def update(self, n: int = 1) -> None:
         """Run n SCFT iterations (PsDomain::update order)."""
@@ -156,6 +169,17 @@ class ScftSolver:
 
     def apply_spectral_filter(self) -> None:
         self._check(self._lib.ps_gpu_apply_spectral_filter(self._h))
+
+    def set_poisson(self, poisson) -> None:
+        """Install a poissonUpdater (config.PoissonUpdater) or remove it (None)."""
+        if poisson is None:
+            self._check(self._lib.ps_gpu_set_poisson(self._h, None))
+            return
+        self._pcfg = poisson.to_ps(self.cfg)
+        self._check(self._lib.ps_gpu_set_poisson(self._h, C.byref(self._pcfg)))
+
+    def apply_poisson(self) -> None:
+        self._check(self._lib.ps_gpu_apply_poisson(self._h))
 
     def set_precision(self, precision: str) -> None:
         """Switch the sweeps to "fp64" or "mixed" between iterations; fields and

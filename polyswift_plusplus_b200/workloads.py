@@ -19,6 +19,12 @@ point in row-major order, plus the deterministic seeds described per workload.
 * ``triblock256`` 256^3, box 16 Rg, ABC (0.3, 0.4, 0.3), chiN AB 30, BC 30, AC 45,
                   Ns 400, Anderson depth 20, mixed precision; w = U(-0.05, 0.05).
 * ``blend_batch`` 64 diblock / A-homopolymer blend instances (see ``blend_instances``).
+* ``charged_diblock`` the charged-diblock test deck's model (chargeFlexPseudoSpec A block,
+                  za 1, alpha 0.01, length 1000, f_A 0.5, ds 0.05, chi = 1/(20 (3.1415) 1.4),
+                  bjerrumLen = 1/(4 (3.1415) 0.01 1.4), simpleIons counter-ions zc -1 with
+                  neutralFactor za alpha f_A, a poissonUpdater every 5 steps), on a chosen
+                  grid; w = U(-0.1, 0.1) +/- cos(2 pi x / L), and a small seeded potential
+                  psi (the reference starts from psi = 0, which its Poisson clamp keeps at 0).
 """
 from __future__ import annotations
 
@@ -160,3 +166,33 @@ def blend_instances(count=64, seed=2024, ns=100, sizes=(32, 48, 64, 96), precisi
         w = random_fields(cfg, 0.1)
         out.append((cfg, [w[0] + c, w[1] - c]))
     return out
+
+
+def charged_diblock(n=(16, 16, 16), cell=0.05, precision="fp64", poisson_every=5, seed=38383):
+    """(cfg, w, psi) for a charged diblock with counter-ions and a Poisson updater."""
+    from .config import PoissonUpdater, Solvent
+    za, alpha, f_a, length, ds, red_t = 1.0, 0.01, 0.5, 1000, 0.05, 1.4
+    blocks = [Block(name="blockA", scfield="A", ds=ds, lengthfrac=f_a, headjoined=["freeEnd"],
+                    tailjoined=["blockB"], kind="chargeFlexPseudoSpec", chargefield="charge",
+                    za=za, alpha=alpha),
+              Block(name="blockB", scfield="B", ds=ds, lengthfrac=1.0 - f_a, headjoined=["blockA"],
+                    tailjoined=["freeEnd"])]
+    cfg = ScftConfig(
+        n=tuple(n), cell=(cell, cell, cell), fields=["A", "B"],
+        polymers=[Polymer(name="diblock1", volfrac=1.0, length=length, blocks=blocks)],
+        interactions=[Interaction(name="AB", chi=1.0 / (20.0 * 3.1415 * red_t), scfields=["A", "B"])],
+        updater=Updater(kind="steepestDescent", relaxlambdas=(0.2, 0.1)), seed=seed,
+        precision=precision,
+        solvents=[Solvent(name="counterIons", scfield="A", volfrac=0.0, kind="simpleIons",
+                          chargefield="charge", blockfield="counterIon", zc=-1.0,
+                          neutral_factor=za * alpha * f_a)],
+        charge_fields=["charge", "counterIon"],
+        poisson=PoissonUpdater(name="ePotential", updatefields=["charge"],
+                               bjerrum_len=1.0 / (4.0 * 3.1415 * alpha * red_t), relaxlambda=1.0,
+                               apply_frequency=poisson_every))
+    x, _, _ = coords(cfg)
+    c = np.cos(2 * math.pi * x / cfg.box[0]).reshape(-1)
+    w = random_fields(cfg, 0.1)
+    u = mt_reals(seed + 1, cfg.n_total)
+    psi = 0.05 * c + 0.01 * (u - 0.5)
+    return cfg, [w[0] + 1.0 * c, w[1] - 1.0 * c], psi

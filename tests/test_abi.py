@@ -45,8 +45,8 @@ def test_version_string(native_lib):
 def test_struct_layout_matches_header(tmp_path):
     """Every ctypes field offset and struct size equals gcc's offsetof/sizeof."""
     structs = [A.ps_block_config, A.ps_polymer_config, A.ps_interaction_config,
-               A.ps_updater_config, A.ps_solvent_config, A.ps_config, A.ps_filter_config,
-               A.ps_scalars]
+               A.ps_updater_config, A.ps_solvent_config, A.ps_block_charge, A.ps_config,
+               A.ps_filter_config, A.ps_poisson_config, A.ps_scalars]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pswift.h"', 'int main(void){']
     for s in structs:
         n = s.__name__
@@ -313,3 +313,95 @@ def test_config_parser_multi_spec_filter_and_updater_sequence():
         config_from_text(deck.replace("<EffHamil h>", "<EffHamil h>\n  updaterSequence = [filt u]"))
     with pytest.raises(InputError):
         config_from_text(base.replace("kind = simpleSpecFilter", "kind = multiSpecFilter"))
+
+
+def test_config_parser_reads_charged_deck():
+    """chargeDens PhysFields, a chargeFlexPseudoSpec block, simpleIons and a
+    poissonUpdater after the field updater, as in the reference's charged test deck."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+setupPS(16, 16, 1, 0.05, 0.05, 0.05, "'off'")
+<EffHamil mainHamil>
+  updaterSequence = [wAwB ePotential]
+  <Updater ePotential>
+    kind = poissonUpdater
+    fftKind = fftWObj
+    applyFrequency = 5
+    relaxlambda = 1.0
+    bjerrumLen = 5.68
+    updatefields = [ totChargeDens ]
+  </Updater>
+  <Updater wAwB>
+    kind = steepestDescent
+    relaxlambdas = [0.20 0.10]
+    updatefields = [totStyrDens totEthyDens]
+  </Updater>
+  <Interaction StyrEthy>
+     kind = flory
+     chi = 0.0114
+     scfields = [totStyrDens totEthyDens]
+  </Interaction>
+</EffHamil>
+<PhysField totStyrDens>
+   kind = monomerDens
+</PhysField>
+<PhysField totEthyDens>
+   kind = monomerDens
+</PhysField>
+<PhysField totChargeDens>
+   kind = chargeDens
+</PhysField>
+<PhysField counterIonDens>
+   kind = chargeDens
+</PhysField>
+<PhysField defaultPressure>
+   kind = constraint
+</PhysField>
+<Solvent counterIons>
+  kind = simpleIons
+  volfrac = 0.0
+  zc = -1.0
+  neutralFactor = 0.005
+  scfield = totStyrDens
+  chargefield = totChargeDens
+  blockfield = counterIonDens
+</Solvent>
+<Polymer diblock1>
+  kind = blockCopolymer
+  volfrac = 1.0
+  length = 1000
+  <Block blockA>
+    kind = chargeFlexPseudoSpec
+    scfield = totStyrDens
+    chargefield = totChargeDens
+    za = 1.0
+    alpha = 0.01
+    ds = 0.05
+    lengthfrac = 0.5
+    headjoined = [freeEnd]
+    tailjoined = [blockB]
+  </Block>
+  <Block blockB>
+    kind = flexPseudoSpec
+    scfield = totEthyDens
+    ds = 0.05
+    lengthfrac = 0.50
+    headjoined = [blockA]
+    tailjoined = [freeEnd]
+  </Block>
+</Polymer>
+"""
+    cfg = config_from_text(text)
+    assert cfg.charge_fields == ["totChargeDens", "counterIonDens"]
+    assert cfg.poisson.updatefields == ["totChargeDens"] and cfg.poisson.apply_frequency == 5
+    assert [k for k, _ in cfg.post_updaters()] == ["poisson"]
+    pc = cfg.to_ps_config()
+    assert pc.n_charges == 2
+    z = pc.block_charge[0][0]
+    assert (z.charged, z.charge_field, z.za, z.alpha) == (1, 0, 1.0, 0.01)
+    assert pc.block_charge[0][1].charged == 0
+    s = pc.solvents[0]
+    assert (s.kind, s.charge_field, s.has_block_field, s.block_field) == (A.PS_SOLV_IONS, 0, 1, 1)
+    assert (s.zc, s.neutral_factor) == (-1.0, 0.005)
+    pp = cfg.poisson.to_ps(cfg)
+    assert pp.n_fields == 1 and pp.fields[0] == 0 and pp.bjerrum_len == 5.68

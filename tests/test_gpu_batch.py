@@ -142,3 +142,33 @@ def test_batch_instance_precision_is_fixed(gpu):
         with pytest.raises(A.PsError) as e:
             b.instance(0).set_precision("fp64")
         assert e.value.code == A.PS_ATTRIB_ERR
+
+
+def test_batch_with_charged_instances_bit_identical(gpu):
+    """Charged diblocks (ions + charged block, no Poisson updater: a batch takes no
+    post-update updaters) batched with a plain diblock: bit-identical to single runs."""
+    items = []
+    for i, n in enumerate(((16, 16, 16), (16, 16, 16))):
+        cfg, w, psi = W.charged_diblock(n=n, seed=300 + i)
+        cfg.poisson = None
+        items.append((cfg, w, psi))
+    plain, wp = W.diblock32(n=16)
+    with ScftBatch([c for c, _, _ in items] + [plain]) as b:
+        b.set_variant(0)
+        for i, (_, w, psi) in enumerate(items):
+            b.instance(i).restore(w)
+            b.instance(i).set_field(A.PS_FIELD_POTENTIAL, 0, psi)
+        b.instance(2).restore(wp)
+        b.update(4)
+        for i, (cfg, w, psi) in enumerate(items):
+            s = ScftSolver(cfg)
+            s.set_variant(0)
+            s.restore(w)
+            s.set_field(A.PS_FIELD_POTENTIAL, 0, psi)
+            s.update(4)
+            v = b.instance(i)
+            assert v.scalars()["free_energy"] == s.scalars()["free_energy"]
+            for c in range(2):
+                assert np.array_equal(v.rho(c), s.rho(c))
+            assert np.array_equal(v.w(0), s.w(0))
+            s.close()

@@ -601,3 +601,97 @@ def test_multi_spectral_filter_scheduled_parity(gpu, oracle_lib):
     cfg = dataclasses.replace(cfg, spec_filter=f)
     g, o, hg, ho = run_both(cfg, w, 12)
     assert_parity(cfg, g, o, hg, ho)
+
+
+# ---------------------------------------------------------------------------
+# Charged systems
+
+def _charged_both(n, every=2, precision="fp64"):
+    cfg, w, psi = W.charged_diblock(n=n, poisson_every=every, precision=precision)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.set_field(A.PS_FIELD_POTENTIAL, 0, psi)
+    import dataclasses
+    o = O.Oracle(dataclasses.replace(cfg, precision="fp64"))
+    o.restore(w)
+    o.set_field(A.PS_FIELD_POTENTIAL, 0, psi)
+    return cfg, g, o
+
+
+@pytest.mark.parametrize("n", [(16, 16, 16), (32, 32, 32), (16, 12, 1), (8, 4, 256)])
+def test_fp64_charged_diblock_parity(gpu, oracle_lib, n):
+    """chargeFlexPseudoSpec block, simpleIons counter-ions and the Poisson updater every
+    2 steps on the device against the oracle: F, Q, w, phi at 1e-10; rho and psi at 1e-10
+    of their magnitude."""
+    cfg, g, o = _charged_both(n)
+    ho = o.update(7)
+    hg = []
+    for _ in range(7):
+        g.update(1)
+        hg.append(g.scalars())
+    assert_parity(cfg, g, o, hg, ho)
+    for c in range(2):
+        assert rel(g.rho(c), o.rho(c)) < TOL64
+        assert np.abs(g.psi(c) - o.psi(c)).max() <= TOL64 * max(np.abs(o.psi(c)).max(), 1e-300)
+
+
+def test_poisson_single_apply_matches_oracle(gpu, oracle_lib):
+    """One Poisson application on a random charge density with the old potential near the
+    answer (no clamping) and far from it (clamping), device vs oracle at 1e-12."""
+    from polyswift_plusplus_b200.config import PoissonUpdater
+    cfg, w, _ = W.charged_diblock(n=(32, 32, 32))
+    cfg.poisson = None
+    rng = np.random.default_rng(4)
+    rho = rng.standard_normal(cfg.n_total) + 0.2
+    pu = PoissonUpdater(updatefields=["charge"], bjerrum_len=3.0)
+    o = O.Oracle(cfg)
+    o.set_field(A.PS_FIELD_CHARGE, 0, rho)
+    o.set_poisson(pu)
+    o.apply_poisson()
+    exact = o.psi(0)  # psi = 0 before: every changed point clamps to 0
+    assert not np.any(exact)
+    for psi0 in (1.05 * rng.standard_normal(cfg.n_total), None):
+        o.set_field(A.PS_FIELD_CHARGE, 0, rho)
+        g = ScftSolver(cfg)
+        g.set_field(A.PS_FIELD_CHARGE, 0, rho)
+        if psi0 is None:  # start near the answer: take the unclamped result as the old potential
+            from oracle.np_scft import coulomb_operator
+            r = (rho - rho.mean()).reshape(cfg.n)
+            psi0 = 1.1 * np.fft.ifftn(np.fft.fftn(r) * coulomb_operator(cfg, 3.0)).real.reshape(-1)
+        o.set_field(A.PS_FIELD_POTENTIAL, 0, psi0)
+        g.set_field(A.PS_FIELD_POTENTIAL, 0, psi0)
+        g.set_poisson(pu)
+        g.apply_poisson()
+        o.apply_poisson()
+        assert rel(g.psi(0), o.psi(0)) < 1e-12
+        assert rel(g.rho(0), o.rho(0)) < 1e-12
+
+
+def test_mixed_charged_diblock_close_to_fp64(gpu):
+    out = []
+    for prec in ("fp64", "mixed"):
+        cfg, g, _ = _charged_both((16, 16, 16), precision=prec)
+        g.update(12)
+        out.append(g.scalars()["free_energy"])
+    assert abs(out[1] - out[0]) < 1e-5 * max(abs(out[0]), 1.0)
+
+
+def test_charged_errors(gpu):
+    import dataclasses
+    from polyswift_plusplus_b200.config import PoissonUpdater, Solvent
+    cfg, _, _ = W.charged_diblock(n=(16, 16, 16))
+    cfg.polymers[0].volfrac = 0.9
+    bad = dataclasses.replace(cfg, solvents=cfg.solvents + [Solvent("s", "A", 0.1)])
+    with pytest.raises(A.PsError):
+        ScftSolver(bad)
+    cfg, _, _ = W.charged_diblock(n=(16, 16, 16))
+    g = ScftSolver(cfg)
+    with pytest.raises(A.PsError):
+        g.set_poisson(PoissonUpdater(updatefields=["charge"], apply_start=4, apply_end=4))
+    g.set_poisson(None)
+    with pytest.raises(A.PsError):
+        g.apply_poisson()
+    with pytest.raises(ValueError):
+        g.set_poisson(PoissonUpdater(updatefields=["nope"]))
+    with pytest.raises(A.PsError):
+        g.get_field(A.PS_FIELD_POTENTIAL, 2)

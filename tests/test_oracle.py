@@ -372,3 +372,92 @@ def test_multi_spec_filter_rejects_cells_not_dividing_the_grid(oracle_lib):
     o = O.Oracle(cfg)
     with pytest.raises(A.PsError):
         o.set_spectral_filter(_multi(["A"], (3, 4, 1), 0.5, 0.0))
+
+
+# ---------------------------------------------------------------------------
+# Charged systems: chargeDens fields, simpleIons, chargeFlexPseudoSpec, poissonUpdater
+
+def _charged_pair(n, every, psi_scale=1.0):
+    cfg, w, psi = W.charged_diblock(n=n, poisson_every=every)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.set_field(A.PS_FIELD_POTENTIAL, 0, psi * psi_scale)
+    m = NpScft(cfg)
+    m.restore(w)
+    m.psi[0] = (psi * psi_scale).reshape(cfg.n).copy()
+    return cfg, o, m
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (16, 12, 1)])
+def test_charged_diblock_oracle_matches_numpy(oracle_lib, n):
+    """Charged A block (Boltzmann factor with psi, rho += za alpha phi_A), counter-ions
+    (rho += zc e, blockfield = e) and the Poisson updater every 2 steps: the C oracle
+    against the numpy restatement over 7 iterations."""
+    cfg, o, m = _charged_pair(n, 2)
+    ho = o.update(7)
+    for t in range(7):
+        hm = m.iterate()
+        assert ho[t]["free_energy"] == pytest.approx(hm["free_energy"], rel=1e-11, abs=1e-13)
+        assert ho[t]["q"][0] == pytest.approx(hm["q"][0], rel=1e-12)
+    for i in range(2):
+        np.testing.assert_allclose(o.w(i), m.w[i].reshape(-1), rtol=0, atol=1e-12)
+        np.testing.assert_allclose(o.phi(i), m.phi[i].reshape(-1), rtol=0, atol=1e-12)
+    for c in range(2):
+        np.testing.assert_allclose(o.rho(c), m.rho[c].reshape(-1), rtol=0, atol=1e-15)
+        np.testing.assert_allclose(o.psi(c), m.psi[c].reshape(-1), rtol=0, atol=1e-15)
+
+
+def test_poisson_known_answer(oracle_lib):
+    """rho = A cos(2 pi x / L): psi = 4 (3.1415) lB A cos / k^2 when the old psi is within
+    the 20% clamp; psi = 0 stays 0 (every changed point is clamped to 1.2 * 0)."""
+    from polyswift_plusplus_b200.config import PoissonUpdater
+    cfg, w, _ = W.charged_diblock(n=(16, 8, 4))
+    cfg.poisson = None
+    x, _, _ = W.coords(cfg)
+    L = cfg.box[0]
+    k = 2 * math.pi / L
+    rho = (0.3 * np.cos(k * x)).reshape(-1)
+    lb = 2.5
+    want = 4.0 * 3.1415 * lb * rho / (k * k)
+    o = O.Oracle(cfg)
+    o.set_field(A.PS_FIELD_CHARGE, 0, rho + 0.7)  # the mean is removed first
+    o.set_field(A.PS_FIELD_POTENTIAL, 0, 1.1 * want)
+    o.set_poisson(PoissonUpdater(updatefields=["charge"], bjerrum_len=lb))
+    o.apply_poisson()
+    np.testing.assert_allclose(o.psi(0), want, rtol=0, atol=1e-12 * np.abs(want).max())
+    np.testing.assert_allclose(o.rho(0), rho, rtol=0, atol=1e-14)
+    # the clamp: an old potential 2x off keeps 1.2 psi_old / N
+    o.set_field(A.PS_FIELD_CHARGE, 0, rho)
+    o.set_field(A.PS_FIELD_POTENTIAL, 0, 2.0 * want)
+    o.apply_poisson()
+    np.testing.assert_allclose(o.psi(0), 2.0 * want * 1.2 / cfg.n_total, rtol=1e-14, atol=1e-300)
+    o.set_field(A.PS_FIELD_POTENTIAL, 0, np.zeros(cfg.n_total))
+    o.set_field(A.PS_FIELD_CHARGE, 0, rho)
+    o.apply_poisson()
+    assert not np.any(o.psi(0))
+
+
+def test_counter_ions_known_answer(oracle_lib):
+    """psi = 0: the ions' Q is 1, blockfield = -neutralFactor / zc and they add
+    -neutralFactor to rho; the charged block adds za alpha phi_A."""
+    cfg, w, _ = W.charged_diblock(n=(8, 8, 8))
+    cfg.poisson = None
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.update(1)
+    S = cfg.solvents[0]
+    nf = S.neutral_factor
+    np.testing.assert_allclose(o.rho(1), np.full(cfg.n_total, -nf / S.zc), rtol=1e-15)
+    blk = cfg.polymers[0].blocks[0]
+    np.testing.assert_allclose(o.rho(0), (o.phi(0) * blk.alpha) * blk.za + (-nf / S.zc) * S.zc,
+                               rtol=0, atol=1e-16)
+
+
+def test_charged_block_must_own_its_field(oracle_lib):
+    import dataclasses
+    from polyswift_plusplus_b200.config import Solvent
+    cfg, _, _ = W.charged_diblock(n=(8, 8, 8))
+    cfg.polymers[0].volfrac = 0.9
+    bad = dataclasses.replace(cfg, solvents=cfg.solvents + [Solvent("s", "A", 0.1)])
+    with pytest.raises(A.PsError):
+        O.Oracle(bad)
