@@ -31,7 +31,8 @@ extern "C" {
 
 #define PS_MAX_BLOCKS 8
 #define PS_MAX_JOINS 4
-#define PS_MAX_POLYMERS 4
+#define PS_MAX_POLYMERS 16 /* polymers, counting each quadrature chain of a
+                              polyDisperseBCP as one */
 #define PS_MAX_FIELDS 4
 #define PS_MAX_INTERACTIONS 6
 #define PS_MAX_SOLVENTS 2
@@ -89,6 +90,24 @@ typedef struct ps_polymer_config {
   int n_blocks;
   ps_block_config blocks[PS_MAX_BLOCKS];
 } ps_polymer_config;
+
+/* <Polymer name> kind = polyDisperseBCP (pspolymer/PsPolyDisperseBCP.cpp:41-455):
+ * block poly_block (polyblock) has a Schulz length distribution of exponent
+ * alpha, integrated by n_g-point generalized Gauss-Laguerre quadrature
+ * (x^(alpha-1) e^-x).  The polymer becomes n_g chains; chain k copies the
+ * blocks with the polydisperse block's lengthfrac
+ *   f_k = (x_k n_b + N_c) / N - (1 - f_poly),  N_c = (1 - f_poly) N,
+ *   n_b = (N - N_c) / alpha,
+ * densities weighted by w_k / Gamma(alpha), and ln Q = sum_k w_k ln Q_k / Gamma(alpha).
+ * At most two blocks (as in the reference); the chains count towards
+ * PS_MAX_POLYMERS.  Block index b of such a polymer in the ABI is the
+ * reference's quadrature block b: seed block b / n_g of chain b % n_g. */
+typedef struct ps_polydisperse_config {
+  int enabled;
+  int poly_block;          /* polyblock: index of the polydisperse block    */
+  int n_g;                 /* n_g                                           */
+  double alpha;            /* alpha (Schulz exponent, > 0)                  */
+} ps_polydisperse_config;
 
 /* <Interaction name> kind = flory (pseffhamil/PsFloryInteraction.cpp:65-89). */
 typedef struct ps_interaction_config {
@@ -156,7 +175,15 @@ typedef struct ps_config {
    * through ps_gpu_set_fields and the Poisson updater.  Appended at the end. */
   int n_charges;
   ps_block_charge block_charge[PS_MAX_POLYMERS][PS_MAX_BLOCKS];
+  ps_polydisperse_config polydisperse[PS_MAX_POLYMERS];
 } ps_config;
+
+/* n-point generalized Gauss-Laguerre rule for the weight x^a e^-x on [0, inf):
+ * nodes ascending into x[n], weights into w[n] (sum w = Gamma(a + 1)); the
+ * rule PsGaussLagQuad(n, a) computes (pspolymer/PsGaussLagQuad.cpp), found
+ * here as the eigen-decomposition of the Jacobi matrix (Golub-Welsch).
+ * 1 <= n <= 64, a > -1. */
+int ps_gauss_laguerre(int n, double a, double* x, double* w);
 
 typedef struct ps_scalars {
   double free_energy;        /* sumFe, disorder term subtracted            */

@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
         L.oracle_set_poisson.restype = C.c_int
         L.oracle_set_poisson.argtypes = [vp, C.POINTER(A.ps_poisson_config)]
         L.oracle_apply_poisson.argtypes = [vp]
+        L.oracle_gauss_laguerre.restype = C.c_int
+        L.oracle_gauss_laguerre.argtypes = [C.c_int, C.c_double, vp, vp]
         L.oracle_get_field.argtypes = [vp, C.c_int, C.c_int, vp]
         L.oracle_iterate.restype = C.c_int
         L.oracle_iterate.argtypes = [vp, C.c_int, C.POINTER(A.ps_scalars)]
@@ -99,6 +101,16 @@ def scaled_fft_pair(data: np.ndarray, kdata: np.ndarray) -> np.ndarray:
     res = np.empty_like(d)
     lib().oracle_scaled_fft_pair(n, _ptr(d), _ptr(k), _ptr(res))
     return res
+
+
+def gauss_laguerre(n: int, a: float):
+    """The oracle's generalized Gauss-Laguerre rule (root bracketing + bisection)."""
+    x = np.zeros(n)
+    w = np.zeros(n)
+    rc = lib().oracle_gauss_laguerre(int(n), float(a), _ptr(x), _ptr(w))
+    if rc != A.PS_OK:
+        raise A.PsError(rc, "bad Gauss-Laguerre arguments")
+    return x, w
 
 
 class Oracle:

@@ -104,7 +104,11 @@ class NpScft:
                    for it in cfg.interactions]
         self.avg = [0.0] * self.nf
         self.steps = []
+        self.pd = {}
         for ip, P in enumerate(cfg.polymers):
+            if P.kind == "polyDisperseBCP":
+                self.pd[ip] = self._polydisperse(ip, P)
+                continue
             st = []
             for B in P.blocks:
                 f = cfg.field_index(B.scfield)
@@ -127,6 +131,34 @@ class NpScft:
         self.phi = [np.zeros(self.shape) for _ in range(self.nf)]
         self.k2 = {}
 
+    def _polydisperse(self, ip, P):
+        """PsPolyDisperseBCP (pspolymer/PsPolyDisperseBCP.cpp:41-455): quadrature chains of the
+        seed blocks with the Schulz-distributed block's lengthfrac at the Gauss-Laguerre nodes
+        (scipy's generalized Gauss-Laguerre rule for x^(alpha-1) e^-x)."""
+        from scipy.special import gamma, roots_genlaguerre
+        x, wq = roots_genlaguerre(P.n_g, P.schulz_alpha - 1.0)
+        galpha = float(gamma(P.schulz_alpha))
+        names = [b.name for b in P.blocks]
+        pb = names.index(P.polyblock)
+        nlen = float(P.length)
+        const_frac = 1.0 - P.blocks[pb].lengthfrac
+        ncl = const_frac * nlen
+        n_b = (nlen - ncl) / P.schulz_alpha
+        fmk = [((xk * n_b + ncl) / nlen) - const_frac for xk in x]
+        chains = []
+        for k in range(P.n_g):
+            fr = [fmk[k] if b == pb else B.lengthfrac for b, B in enumerate(P.blocks)]
+            st = [block_steps(self.alpha[ip] * fr[b] / B.ds, B.force_block_steps)
+                  for b, B in enumerate(P.blocks)]
+            lwt = [wq[k] / galpha if b == pb else 1.0 / P.n_g for b in range(len(P.blocks))]
+            chains.append({"frac": fr, "steps": st, "lwt": lwt, "dwt": wq[k] / galpha, "w": wq[k]})
+        for b, B in enumerate(P.blocks):  # seed-major block order
+            f = self.cfg.field_index(B.scfield)
+            for ch in chains:
+                self.avg[f] = self.avg[f] + ch["lwt"][b] * ch["frac"][b] * P.volfrac
+        self.steps.append(None)
+        return {"chains": chains, "galpha": galpha}
+
     def restore(self, w, p=None):
         self.w = [np.asarray(x, dtype=np.float64).reshape(self.shape).copy() for x in w]
         self.p = np.zeros(self.shape) if p is None else np.asarray(p).reshape(self.shape).copy()
@@ -140,6 +172,59 @@ class NpScft:
             q = (1.0 / self.N) * (res * wfac)
             out.append(q)
         return out
+
+    def _chain(self, P, steps_of):
+        order = chain_order(P)
+        qs = {}
+        for direction in (order, [(b, 1 - e) for b, e in reversed(order)]):
+            q = np.ones(self.shape)
+            for b, e in direction:
+                B = P.blocks[b]
+                f = self.cfg.field_index(B.scfield)
+                wfac = np.exp(-0.5 * B.ds * self.w[f])
+                key = (B.ds, B.bseg_ratio)
+                if key not in self.k2:
+                    self.k2[key] = k2_operator(self.cfg, B.ds, B.bseg_ratio)
+                sl = self._solve(q, wfac, self.k2[key], steps_of[b])
+                qs[(b, e)] = sl
+                q = sl[-1]
+        return qs
+
+    def _qqt(self, a, t, ds):
+        num = len(a)
+        even = num % 2 == 0
+        tail = num - 1 - (3 if even else 2)
+        acc = np.zeros(self.shape)
+        for n in range(0, tail + 1, 2):
+            acc = acc + a[n] * t[num - n - 1]
+            acc = acc + (a[n + 1] * t[num - n - 2]) * 4.0
+            acc = acc + a[n + 2] * t[num - n - 3]
+        acc = acc * (0.33333 * ds)
+        if even:
+            acc = acc + (a[num - 2] * t[1] + a[num - 1] * t[0]) * (ds * 0.5)
+        return acc
+
+    def polymer_pd(self, ip):
+        """PsPolyDisperseBCP::update and getLogBigQ (pspolymer/PsPolyDisperseBCP.cpp:282-377):
+        per-block Q normalisation, densities weighted by w_k / Gamma(alpha)."""
+        P = self.cfg.polymers[ip]
+        pdm = self.pd[ip]
+        res = []
+        for ch in pdm["chains"]:
+            qs = self._chain(P, ch["steps"])
+            res.append(qs)
+        logq = 0.0
+        for k, ch in enumerate(pdm["chains"]):
+            Q0 = float(np.sum(res[k][(0, 0)][0] * res[k][(0, 1)][-1])) / self.N
+            logq = logq + (math.log(Q0) * ch["w"]) / pdm["galpha"]
+        for b, B in enumerate(P.blocks):
+            f = self.cfg.field_index(B.scfield)
+            for k, ch in enumerate(pdm["chains"]):
+                a, t = res[k][(b, 0)], res[k][(b, 1)]
+                Qb = float(np.sum(a[0] * t[-1])) / self.N
+                acc = self._qqt(a, t, B.ds)
+                self.phi[f] = self.phi[f] + (ch["dwt"] * P.volfrac / self.alpha[ip]) * ((1.0 / Qb) * acc)
+        return math.exp(logq), logq
 
     def polymer(self, ip):
         P = self.cfg.polymers[ip]
@@ -219,7 +304,15 @@ class NpScft:
         self.rho = [np.zeros(self.shape) for _ in range(self.nq)]
         solvents = list(getattr(self.cfg, "solvents", []))
         Qsol = [self.ions(S) if S.kind == "simpleIons" else self.solvent(S) for S in solvents]
-        Qs = [self.polymer(ip)[0] for ip in range(len(self.cfg.polymers))]
+        Qs, logQs = [], []
+        for ip in range(len(self.cfg.polymers)):
+            if ip in self.pd:
+                q, lq = self.polymer_pd(ip)
+            else:
+                q = self.polymer(ip)[0]
+                lq = math.log(q)
+            Qs.append(q)
+            logQs.append(lq)
         nf = self.nf
         dh = []
         for i in range(nf):
@@ -245,7 +338,7 @@ class NpScft:
                         pr = pr + (self.phi[n] - self.avg[n]) * self.chin[it]
             pr = (1.0 / 3.0) * pr
         self.p = pr - np.sum(pr) / self.N
-        fe = -sum(P.volfrac * math.log(Q) / a for P, Q, a in zip(self.cfg.polymers, Qs, self.alpha))
+        fe = -sum(P.volfrac * lq / a for P, lq, a in zip(self.cfg.polymers, logQs, self.alpha))
         fe -= sum(S.volfrac * math.log(Q) * self.L0 for S, Q in zip(solvents, Qsol))
         dens = -sum(self.phi[i] * self.w[i] for i in range(nf))
         for it, (a, b) in enumerate(self.ia):

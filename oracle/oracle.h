@@ -44,6 +44,7 @@ void oracle_destroy(oracle_state* s);
 int oracle_set_filter(oracle_state* s, const ps_filter_config* f);
 void oracle_apply_filter(oracle_state* s);
 int oracle_set_poisson(oracle_state* s, const ps_poisson_config* p);
+int oracle_gauss_laguerre(int n, double a, double* x, double* w);
 void oracle_apply_poisson(oracle_state* s);
 int oracle_block_steps(const oracle_state* s, int polymer, int block);
 void oracle_init_random(oracle_state* s);

@@ -46,6 +46,9 @@ void oracle_scaled_pair_buf(const int n[3], const double* data, const double* kd
 
 enum { HEAD = 0, TAIL = 1 };
 
+/* blocks per polymer here: a polyDisperseBCP has n_g quadrature copies of each seed block */
+#define OMAX_BLOCKS 64
+
 typedef struct oblock {
   ps_block_config cfg;
   int steps;
@@ -73,9 +76,67 @@ typedef struct opolymer {
   ps_polymer_config cfg;
   double length_ratio;
   int nb;
-  oblock b[PS_MAX_BLOCKS];
+  oblock b[OMAX_BLOCKS];
   double bigq;
+  double logq;                 /* getLogBigQ */
+  /* polyDisperseBCP (pspolymer/PsPolyDisperseBCP.cpp): quadrature blocks seed-major */
+  int pd, n_g, n_seed, poly_block;
+  double galpha;               /* Gamma(alpha) */
+  double gw[OMAX_BLOCKS];      /* Gauss-Laguerre weights w_k */
+  double lwt[OMAX_BLOCKS];     /* lengthWeight of each block */
+  double dwt[OMAX_BLOCKS];     /* densityWeight of each block */
+  double bq[OMAX_BLOCKS];      /* per-block calcBigQ */
 } opolymer;
+
+/* n-point generalized Gauss-Laguerre rule (weight x^a e^-x): the roots of
+ * L_n^(a) are bracketed on a grid quadratic in x, bisected, and the weights
+ * are Gamma(n + a + 1) / (n! x_i L_n^(a)'(x_i)^2).  L by the three-term
+ * recurrence, x L_n' = n L_n - (n + a) L_{n-1}. */
+static double laguerre(int n, double a, double x, double* dl) {
+  double p0 = 1.0, p1 = 1.0 + a - x;
+  if (n == 0) { *dl = 0.0; return 1.0; }
+  for (int j = 1; j < n; ++j) {
+    const double p2 = ((2.0 * j + 1.0 + a - x) * p1 - (j + a) * p0) / (j + 1.0);
+    p0 = p1;
+    p1 = p2;
+  }
+  *dl = (n * p1 - (n + a) * p0) / x;
+  return p1;
+}
+
+int oracle_gauss_laguerre(int n, double a, double* x, double* w);
+static int gauss_laguerre(int n, double a, double* x, double* w) { return oracle_gauss_laguerre(n, a, x, w); }
+int oracle_gauss_laguerre(int n, double a, double* x, double* w) {
+  if (n < 1 || n > 64 || !(a > -1.0)) return PS_ATTRIB_ERR;
+  const double X = 4.0 * n + 2.0 * a + 10.0;
+  const long M = 200000;
+  double dl, xa = 0.0, fa = 1.0;  /* L_n^(a)(0) > 0 */
+  int found = 0;
+  for (long i = 1; i <= M && found < n; ++i) {
+    const double t = (double)i / (double)M;
+    const double xb = X * t * t;
+    const double fb = laguerre(n, a, xb, &dl);
+    if ((fa > 0.0) != (fb > 0.0)) {
+      double lo = xa, hi = xb, flo = fa;
+      for (int it = 0; it < 200 && hi - lo > 0.0; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        const double fm = laguerre(n, a, mid, &dl);
+        if ((fm > 0.0) == (flo > 0.0)) { lo = mid; flo = fm; } else { hi = mid; }
+      }
+      x[found++] = 0.5 * (lo + hi);
+    }
+    xa = xb;
+    fa = fb;
+  }
+  if (found != n) return PS_ATTRIB_ERR;
+  const double c = exp(lgamma(n + a + 1.0) - lgamma(n + 1.0));
+  for (int i = 0; i < n; ++i) {
+    laguerre(n, a, x[i], &dl);
+    w[i] = c / (x[i] * dl * dl);
+  }
+  return PS_OK;
+}
 
 struct oracle_state {
   ps_config cfg;
@@ -162,6 +223,13 @@ static int set_block_steps(double bs, int force, int* out, char* err, int errlen
   return PS_OK;
 }
 
+/* Charge attributes of block ib of polymer ip (a quadrature block copies its seed's). */
+static const ps_block_charge* block_charge_of(const oracle_state* s, int ip, int ib) {
+  const opolymer* P = &s->pol[ip];
+  const int seed = P->pd ? ib / P->n_g : ib;
+  return &s->cfg.block_charge[ip][seed];
+}
+
 /* PsGridField::calck2 (psbase/PsGridField.cpp:66-104): |k|^2 at grid index (i, j, k). */
 static double calck2(const oracle_state* s, int i, int j, int k) {
   const double twopi = 2.0 * acos(-1.0);
@@ -231,17 +299,69 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
       rc = PS_ATTRIB_ERR;
       break;
     }
-    /* |sum f - 1| <= 1e-5 (pspolymer/PsBlockCopolymer.cpp:113-127) */
-    double tot = 0.0;
-    for (int ib = 0; ib < P->nb; ++ib) tot = tot + P->cfg.blocks[ib].lengthfrac;
-    if (fabs(tot - 1.0) > 0.00001) {
-      snprintf(err, errlen, "polymer %d: |totalFrac - 1.0| = %g > tolerance", ip, fabs(tot - 1.0));
-      rc = PS_INPUT_ERR;
-      break;
+    const ps_polydisperse_config* D = &cfg->polydisperse[ip];
+    for (int ib = 0; ib < OMAX_BLOCKS; ++ib) P->lwt[ib] = P->dwt[ib] = 1.0;
+    if (D->enabled) {
+      /* PsPolyDisperseBCP::setAttrib / calcPolyParams / makeQuadAttrib
+       * (pspolymer/PsPolyDisperseBCP.cpp:41-145, 384-455, 495-600) */
+      if (P->nb > 2 || D->poly_block < 0 || D->poly_block >= P->nb || D->n_g < 1 ||
+          D->n_g * P->nb > OMAX_BLOCKS || !(D->alpha > 0.0)) {
+        snprintf(err, errlen, "polymer %d: bad polyDisperseBCP (at most 2 blocks)", ip);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+      double xg[64];
+      if (gauss_laguerre(D->n_g, D->alpha - 1.0, xg, P->gw) != PS_OK) {
+        snprintf(err, errlen, "polymer %d: Gauss-Laguerre rule failed", ip);
+        rc = PS_ATTRIB_ERR;
+        break;
+      }
+      P->pd = 1;
+      P->n_g = D->n_g;
+      P->n_seed = P->nb;
+      P->poly_block = D->poly_block;
+      P->galpha = tgamma(D->alpha);
+      const double nlen = (double)P->cfg.length;
+      const double poly_frac = P->cfg.blocks[D->poly_block].lengthfrac;
+      const double const_frac = 1.0 - poly_frac;
+      const double ncl = const_frac * nlen;
+      const double n_b = (nlen - ncl) / D->alpha;
+      for (int sb = 0; sb < P->n_seed; ++sb)
+        for (int k = 0; k < P->n_g; ++k) {
+          const int q = sb * P->n_g + k;
+          ps_block_config bc = P->cfg.blocks[sb];
+          for (int j = 0; j < bc.n_head; ++j) bc.head_joined[j] = bc.head_joined[j] * P->n_g + k;
+          for (int j = 0; j < bc.n_tail; ++j) bc.tail_joined[j] = bc.tail_joined[j] * P->n_g + k;
+          if (sb == D->poly_block) {
+            bc.lengthfrac = ((xg[k] * n_b + ncl) / nlen) - const_frac;
+            P->lwt[q] = P->gw[k] / P->galpha;
+          } else {
+            P->lwt[q] = 1.0 / (double)P->n_g;
+          }
+          P->dwt[q] = P->gw[k] / P->galpha;
+          P->b[q].cfg = bc;
+        }
+      P->nb = P->n_seed * P->n_g;
+      double tot = 0.0;
+      for (int ib = 0; ib < P->nb; ++ib) tot = tot + (P->b[ib].cfg.lengthfrac * P->lwt[ib]);
+      if (fabs(tot - 1.0) > 0.00001) {
+        snprintf(err, errlen, "polymer %d: PsPolyDisperseBCP |totalFrac - 1.0| > tolerance", ip);
+        rc = PS_INPUT_ERR;
+        break;
+      }
+    } else {
+      /* |sum f - 1| <= 1e-5 (pspolymer/PsBlockCopolymer.cpp:113-127) */
+      double tot = 0.0;
+      for (int ib = 0; ib < P->nb; ++ib) tot = tot + P->cfg.blocks[ib].lengthfrac;
+      if (fabs(tot - 1.0) > 0.00001) {
+        snprintf(err, errlen, "polymer %d: |totalFrac - 1.0| = %g > tolerance", ip, fabs(tot - 1.0));
+        rc = PS_INPUT_ERR;
+        break;
+      }
+      for (int ib = 0; ib < P->nb; ++ib) P->b[ib].cfg = P->cfg.blocks[ib];
     }
     for (int ib = 0; ib < P->nb && rc == PS_OK; ++ib) {
       oblock* B = &P->b[ib];
-      B->cfg = P->cfg.blocks[ib];
       if (B->cfg.field < 0 || B->cfg.field >= s->nf) {
         snprintf(err, errlen, "polymer %d block %d: field index out of range", ip, ib);
         rc = PS_ATTRIB_ERR;
@@ -253,7 +373,7 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
         break;
       }
       /* psbase/PsBlockBase.cpp:187-198 */
-      s->dens_avg[B->cfg.field] = s->dens_avg[B->cfg.field] + 1.0 * B->cfg.lengthfrac * P->cfg.volfrac;
+      s->dens_avg[B->cfg.field] = s->dens_avg[B->cfg.field] + P->lwt[ib] * B->cfg.lengthfrac * P->cfg.volfrac;
       double bstmp = P->length_ratio * B->cfg.lengthfrac / B->cfg.ds;
       char e2[200];
       rc = set_block_steps(bstmp, B->cfg.force_block_steps, &B->steps, e2, sizeof(e2));
@@ -273,7 +393,7 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
     }
     if (rc != PS_OK) break;
     /* setCntToLists (psbase/PsBlockBase.cpp:214-245) */
-    for (int ib = 0; ib < P->nb; ++ib) {
+    for (int ib = 0; ib < P->nb && rc == PS_OK; ++ib) {
       oblock* B = &P->b[ib];
       B->ncnt[HEAD] = B->cfg.n_head;
       B->ncnt[TAIL] = B->cfg.n_tail;
@@ -362,7 +482,7 @@ int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errle
    * that rho += za alpha phi_f sees the block's own density as the reference does */
   for (int ip = 0; ip < s->npol && rc == PS_OK; ++ip)
     for (int ib = 0; ib < s->pol[ip].nb && rc == PS_OK; ++ib) {
-      const ps_block_charge* Z = &cfg->block_charge[ip][ib];
+      const ps_block_charge* Z = block_charge_of(s, ip, ib);
       if (!Z->charged) continue;
       if (Z->charge_field < 0 || Z->charge_field >= s->nq) {
         snprintf(err, errlen, "polymer %d block %d: chargefield out of range", ip, ib);
@@ -432,7 +552,7 @@ void oracle_destroy(oracle_state* s) {
   free(s->fcut); free(s->fregion); free(s->kcoul);
   for (int c = 0; c < PS_MAX_CHARGES; ++c) { free(s->rho[c]); free(s->psi[c]); }
   for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip)
-    for (int ib = 0; ib < PS_MAX_BLOCKS; ++ib) {
+    for (int ib = 0; ib < OMAX_BLOCKS; ++ib) {
       oblock* B = &s->pol[ip].b[ib];
       free(B->qs); free(B->qts); free(B->wfac); free(B->k2); free(B->qqt);
       for (int e = 0; e < 2; ++e) {
@@ -627,7 +747,7 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     for (long n = 0; n < N; ++n) B->wfac[n] = exp(ds2 * w[n]);
     /* PsChargeFlexPseudoSpec::reset (pspolymer/PsChargeFlexPseudoSpec.cpp:97-130):
      * wfac *= exp(facZ ds2 psi), facZ = za alpha L */
-    const ps_block_charge* Z = &s->cfg.block_charge[P - s->pol][ib];
+    const ps_block_charge* Z = block_charge_of(s, (int)(P - s->pol), ib);
     if (Z->charged) {
       const double facz = Z->za * Z->alpha * s->scale_length;
       const double* psi = s->psi[Z->charge_field];
@@ -641,7 +761,7 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     for (int ib = 0; ib < P->nb; ++ib)
       if (!(P->b[ib].final_set[HEAD] && P->b[ib].final_set[TAIL])) all = 0;
     if (all) break;
-    if (++guard > 4 * PS_MAX_BLOCKS + 4) return PS_INPUT_ERR; /* unreachable blocks */
+    if (++guard > 4 * OMAX_BLOCKS + 4) return PS_INPUT_ERR; /* unreachable blocks */
     for (int ib = 0; ib < P->nb; ++ib) {
       update_block_q(s, P, ib, HEAD);
       update_block_q(s, P, ib, TAIL);
@@ -658,13 +778,35 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     }
     double q = tot / ((double)(1 * (double)N));
     P->bigq = q;
+    P->logq = log(q);
     if (q != q) return PS_RUN_ERR;
   }
-  for (int ib = 0; ib < P->nb; ++ib) calc_qqt(s, &P->b[ib], P->bigq);
+  if (P->pd) {
+    /* PsPolyDisperseBCP::update / getLogBigQ (pspolymer/PsPolyDisperseBCP.cpp:282-377):
+     * every quadrature block normalises with its own calcBigQ; ln Q sums the first
+     * seed block's copies with weights w_k / Gamma(alpha) */
+    for (int ib = 0; ib < P->nb; ++ib) {
+      oblock* B = &P->b[ib];
+      double tot = 0.0;
+      for (long r = 0; r < N; ++r) {
+        double v = (0.0 + B->q_init[HEAD][r]) * B->q_final[HEAD][r];
+        tot = tot + v;
+      }
+      P->bq[ib] = tot / ((double)(1 * (double)N));
+      if (P->bq[ib] != P->bq[ib]) return PS_RUN_ERR;
+    }
+    double sum = 0.0;
+    for (int k = 0; k < P->n_g; ++k) sum = sum + ((log(P->bq[k]) * P->gw[k]) / P->galpha);
+    P->logq = sum;
+    P->bigq = exp(sum);
+    for (int ib = 0; ib < P->nb; ++ib) calc_qqt(s, &P->b[ib], P->bq[ib]);
+  } else {
+    for (int ib = 0; ib < P->nb; ++ib) calc_qqt(s, &P->b[ib], P->bigq);
+  }
   /* PsBlock::setPhysFields (pspolymer/PsBlock.cpp:153-196) */
   for (int ib = 0; ib < P->nb; ++ib) {
     oblock* B = &P->b[ib];
-    double densfac = 1.0 * P->cfg.volfrac / P->length_ratio;
+    double densfac = P->dwt[ib] * P->cfg.volfrac / P->length_ratio;
     double* phi = s->phi[B->cfg.field];
 #pragma omp parallel for schedule(static)
     for (long r = 0; r < N; ++r) {
@@ -673,7 +815,7 @@ static int polymer_update(oracle_state* s, opolymer* P) {
     }
     /* PsChargeFlexPseudoSpec::setPhysFields (pspolymer/PsChargeFlexPseudoSpec.cpp:136-165):
      * rho += (phi_f alpha) za */
-    const ps_block_charge* Z = &s->cfg.block_charge[P - s->pol][ib];
+    const ps_block_charge* Z = block_charge_of(s, (int)(P - s->pol), ib);
     if (Z->charged) {
       double* rho = s->rho[Z->charge_field];
       for (long r = 0; r < N; ++r) {
@@ -971,7 +1113,7 @@ static void calc_fe(oracle_state* s, double* fe_out, double* fe_nodis_out) {
   const double inv_vol = 1.0 / (double)N;
   double sum_tmp = 0.0;
   for (int ip = 0; ip < s->npol; ++ip) {
-    double logq = log(s->pol[ip].bigq);
+    double logq = s->pol[ip].logq;
     double vf = s->pol[ip].cfg.volfrac;
     double lr = s->pol[ip].length_ratio;
     sum_tmp = sum_tmp - ((vf * logq) / lr);
@@ -1176,7 +1318,7 @@ int oracle_iterate(oracle_state* s, int niter, ps_scalars* hist) {
       int rc = polymer_update(s, &s->pol[ip]);
       if (rc != PS_OK) return rc;
       sc.q[ip] = s->pol[ip].bigq;
-      sc.log_q[ip] = log(s->pol[ip].bigq);
+      sc.log_q[ip] = s->pol[ip].logq;
     }
     double mx = 0.0;
     for (long r = 0; r < N; ++r) {

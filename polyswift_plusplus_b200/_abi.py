@@ -11,7 +11,7 @@ from pathlib import Path
 
 PS_MAX_BLOCKS = 8
 PS_MAX_JOINS = 4
-PS_MAX_POLYMERS = 4
+PS_MAX_POLYMERS = 16
 PS_MAX_FIELDS = 4
 PS_MAX_INTERACTIONS = 6
 PS_MAX_SOLVENTS = 2
@@ -53,6 +53,11 @@ class ps_polymer_config(C.Structure):
                 ("blocks", ps_block_config * PS_MAX_BLOCKS)]
 
 
+class ps_polydisperse_config(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("poly_block", C.c_int), ("n_g", C.c_int),
+                ("alpha", C.c_double)]
+
+
 class ps_interaction_config(C.Structure):
     _fields_ = [("field_a", C.c_int), ("field_b", C.c_int), ("chi", C.c_double)]
 
@@ -84,7 +89,8 @@ class ps_config(C.Structure):
                 ("calc_disorder", C.c_int), ("device", C.c_int),
                 ("n_solvents", C.c_int), ("solvents", ps_solvent_config * PS_MAX_SOLVENTS),
                 ("n_charges", C.c_int),
-                ("block_charge", (ps_block_charge * PS_MAX_BLOCKS) * PS_MAX_POLYMERS)]
+                ("block_charge", (ps_block_charge * PS_MAX_BLOCKS) * PS_MAX_POLYMERS),
+                ("polydisperse", ps_polydisperse_config * PS_MAX_POLYMERS)]
 
 
 class ps_filter_config(C.Structure):
@@ -169,6 +175,7 @@ SIGNATURES = {
     "ps_fft_destroy": (C.c_int, [_vp]),
     "ps_fft_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "ps_fft_scaled_pair": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ps_gauss_laguerre": (C.c_int, [C.c_int, C.c_double, _vp, _vp]),
     "ps_fft_last_error": (C.c_char_p, []),
     "ps_fft_scaled_pair_noalloc": (C.c_int, [C.POINTER(C.c_int), _vp, _vp, _vp, _vp]),
     "ps_fft_noalloc_scratch_bytes": (C.c_size_t, []),

@@ -59,6 +59,15 @@ class Polymer:
     length: int
     blocks: list[Block]
     kind: str = "blockCopolymer"
+    # polyDisperseBCP (pspolymer/PsPolyDisperseBCP.cpp:41-100): Schulz exponent alpha,
+    # n_g Gauss-Laguerre points, the polydisperse block's name
+    n_g: int = 0
+    schulz_alpha: float = 0.0
+    polyblock: str | None = None
+
+    @property
+    def n_chains(self) -> int:
+        return self.n_g if self.kind == "polyDisperseBCP" else 1
 
 
 @dataclass
@@ -211,8 +220,8 @@ class ScftConfig:
             raise ValueError("precision must be 'fp64' or 'mixed'")
         c.precision = A.PS_PREC_FP64 if self.precision == "fp64" else A.PS_PREC_MIXED
         c.n_fields = len(self.fields)
-        if not 1 <= len(self.polymers) <= A.PS_MAX_POLYMERS:
-            raise ValueError("number of polymers out of range")
+        if not 1 <= sum(P.n_chains for P in self.polymers) <= A.PS_MAX_POLYMERS:
+            raise ValueError("number of polymers (counting polydisperse quadrature chains) out of range")
         c.n_polymers = len(self.polymers)
         for ip, P in enumerate(self.polymers):
             cp = c.polymers[ip]
@@ -222,6 +231,12 @@ class ScftConfig:
                 raise ValueError(f"polymer {P.name}: number of blocks out of range")
             cp.n_blocks = len(P.blocks)
             names = [b.name for b in P.blocks]
+            if P.kind == "polyDisperseBCP":
+                d = c.polydisperse[ip]
+                d.enabled = 1
+                d.poly_block = names.index(P.polyblock)
+                d.n_g = int(P.n_g)
+                d.alpha = float(P.schulz_alpha)
             for ib, B in enumerate(P.blocks):
                 cb = cp.blocks[ib]
                 cb.field = self.field_index(B.scfield)
@@ -399,8 +414,16 @@ def config_from_text(text: str) -> ScftConfig:
     polymers = []
     for pname, pnode in _find(root, "Polymer"):
         pa = pnode["attrs"]
-        if pa.get("kind", "blockCopolymer") not in ("blockCopolymer", "blockCopolymerGPU"):
+        pkind = str(pa.get("kind", "blockCopolymer"))
+        if pkind not in ("blockCopolymer", "blockCopolymerGPU", "polyDisperseBCP"):
             raise InputError(f"Polymer kind {pa.get('kind')!r} is not on the device path")
+        pd = {}
+        if pkind == "polyDisperseBCP":
+            for key in ("alpha", "n_g", "polyblock"):
+                if key not in pa:
+                    raise InputError(f"PsPolyDisperseBCP::setAttrib: {key} not set in <Polymer {pname}>")
+            pd = dict(kind=pkind, n_g=int(pa["n_g"]), schulz_alpha=float(pa["alpha"]),
+                      polyblock=str(pa["polyblock"]))
         blocks = []
         for bname, bnode in _find(pnode, "Block"):
             ba = bnode["attrs"]
@@ -428,7 +451,7 @@ def config_from_text(text: str) -> ScftConfig:
                                 force_block_steps=fbs in (1, "on", "true", "1"), kind=bkind,
                                 **charge))
         polymers.append(Polymer(name=pname, volfrac=float(pa.get("volfrac", 1.0)),
-                                length=int(pa.get("length", 1)), blocks=blocks))
+                                length=int(pa.get("length", 1)), blocks=blocks, **pd))
     solvents = []
     for sname, snode in _find(root, "Solvent"):
         sa = snode["attrs"]

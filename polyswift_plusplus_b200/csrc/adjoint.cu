@@ -554,7 +554,8 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
     a->err = "the adjoint runs in FP64 (precision must be PS_PREC_FP64)";
     return PS_ATTRIB_ERR;
   }
-  if (cfg->n_polymers != 1 || cfg->n_solvents != 0 || cfg->n_charges != 0) {
+  if (cfg->n_polymers != 1 || cfg->n_solvents != 0 || cfg->n_charges != 0 ||
+      cfg->polydisperse[0].enabled) {
     a->err = "the adjoint takes one polymer (a linear block copolymer melt) and no solvent";
     return PS_INPUT_ERR;
   }

@@ -334,8 +334,8 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
     *nlaunch += 2;
   }
   for (int ip = 0; ip < h->cfg.n_polymers; ++ip) {
-    const double vf = h->cfg.polymers[ip].volfrac;
-    const double densfac = 1.0 * vf / h->alpha[ip];
+    // densWt vf / lengthRatio (pspolymer/PsBlock.cpp:164-172); densWt = 1 or w_k / Gamma(alpha)
+    const double densfac = h->chain_dwt[ip] * h->chain_vf[ip] / h->alpha[ip];
     for (size_t ib = 0; ib < h->blocks[ip].size(); ++ib) {
       const BlockMap& b = h->blocks[ip][ib];
       PS_CUDA(h, launch_quadrature<T>(slice(b.sweep_head, b.off_head), slice(b.sweep_tail, b.off_tail),
@@ -490,9 +490,13 @@ static void free_all(ps_handle* h) {
   if (h->st) cudaStreamDestroy(h->st);
 }
 
-static int create_impl(ps_handle* h, const ps_config* cfg) {
-  h->cfg = *cfg;
-  const ps_config& c = *cfg;
+static int create_impl(ps_handle* h, const ps_config* ucfg) {
+  h->ucfg = *ucfg;
+  {
+    int rc = expand_polydisperse(h, *ucfg, &h->cfg);
+    if (rc) return rc;
+  }
+  const ps_config& c = h->cfg;
   for (int d = 0; d < 3; ++d) {
     h->n[d] = c.n[d];
     if (!extent_supported(c.n[d])) {
@@ -548,10 +552,11 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
     }
     const double alpha = (double)P.length / scale_len;
     h->alpha.push_back(alpha);
-    vtot += P.volfrac;
+    const ps_polydisperse_config& D = c.polydisperse[ip];
+    if (h->chain_k[ip] == 0) vtot += h->chain_vf[ip];
     double ftot = 0.0;
     for (int ib = 0; ib < P.n_blocks; ++ib) ftot = ftot + P.blocks[ib].lengthfrac;
-    if (fabs(ftot - 1.0) > 0.00001) {
+    if (!D.enabled && fabs(ftot - 1.0) > 0.00001) {
       h->err = "polymer " + std::to_string(ip) + ": |totalFrac - 1.0| > tolerance";
       return PS_INPUT_ERR;
     }
@@ -565,7 +570,10 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
         h->err = "ds not set";
         return PS_ATTRIB_ERR;
       }
-      dens_avg[B.field] = dens_avg[B.field] + 1.0 * B.lengthfrac * P.volfrac;
+      // lengthWeight: 1; for a polydisperse chain w_k / Gamma(alpha) on the polydisperse
+      // block and 1 / n_g on the other (pspolymer/PsPolyDisperseBCP.cpp:458-480)
+      const double lwt = !D.enabled ? 1.0 : (ib == D.poly_block ? h->chain_dwt[ip] : 1.0 / (double)D.n_g);
+      dens_avg[B.field] = dens_avg[B.field] + lwt * B.lengthfrac * h->chain_vf[ip];
       BlockMap bm;
       memset(&bm, 0, sizeof(bm));
       std::string e2;
@@ -593,6 +601,23 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
         bm.facz = Z.za * Z.alpha * scale_len;
       }
       h->blocks[ip].push_back(bm);
+    }
+  }
+  // polyDisperseBCP length-fraction check over all quadrature blocks
+  // (pspolymer/PsPolyDisperseBCP.cpp:246-274)
+  for (int up = 0; up < h->ucfg.n_polymers; ++up) {
+    const ps_polydisperse_config& D = h->ucfg.polydisperse[up];
+    if (!D.enabled) continue;
+    double tot = 0.0;
+    for (int ib = 0; ib < h->ucfg.polymers[up].n_blocks; ++ib)
+      for (int k = 0; k < D.n_g; ++k) {
+        const int ch = h->user_first[up] + k;
+        const double lwt = (ib == D.poly_block) ? h->chain_dwt[ch] : 1.0 / (double)D.n_g;
+        tot = tot + c.polymers[ch].blocks[ib].lengthfrac * lwt;
+      }
+    if (fabs(tot - 1.0) > 0.00001) {
+      h->err = "PsPolyDisperseBCP::buildData: |totalFrac - 1.0| > tolerance";
+      return PS_INPUT_ERR;
     }
   }
   // simpleSolvent: density average and volume fraction (pssolvent/PsSimpleSolvent.cpp:56-80,
@@ -754,7 +779,8 @@ static int create_impl(ps_handle* h, const ps_config* cfg) {
   fm.lambda1 = c.updater.lambda1;
   fm.npol = c.n_polymers;
   for (int ip = 0; ip < c.n_polymers; ++ip) {
-    fm.vf[ip] = c.polymers[ip].volfrac;
+    // -vf ln Q / alpha; a polydisperse chain carries its weight: -vf (w_k / Gamma) ln Q_k / alpha
+    fm.vf[ip] = h->chain_dwt[ip] * h->chain_vf[ip];
     fm.alpha[ip] = h->alpha[ip];
   }
   fm.nsolv = c.n_solvents;
@@ -978,11 +1004,28 @@ int ps_gpu_destroy(ps_handle* h) {
   return PS_OK;
 }
 
+// The caller's (polymer, block) -> (chain, block of the chain).  A polyDisperseBCP
+// numbers its quadrature blocks seed-major, as the reference's block list does
+// (pspolymer/PsPolyDisperseBCP.cpp:155-208): block b is seed b / n_g of chain b % n_g.
+static bool user_block(const ps_handle* h, int up, int ub, int* ch, int* b) {
+  if (up < 0 || up >= (int)h->user_first.size() || ub < 0) return false;
+  const int ng = h->user_ng[up];
+  const int nseed = h->ucfg.polymers[up].n_blocks;
+  if (ub >= nseed * ng) return false;
+  if (h->ucfg.polydisperse[up].enabled) {
+    *ch = h->user_first[up] + ub % ng;
+    *b = ub / ng;
+  } else {
+    *ch = h->user_first[up];
+    *b = ub;
+  }
+  return *ch < (int)h->blocks.size() && *b < (int)h->blocks[*ch].size();
+}
+
 int ps_gpu_block_steps(const ps_handle* h, int ip, int ib, int* steps) {
-  if (!h || !steps || ip < 0 || ip >= (int)h->blocks.size() || ib < 0 ||
-      ib >= (int)h->blocks[ip].size())
-    return PS_ATTRIB_ERR;
-  *steps = h->blocks[ip][ib].steps;
+  int ch = 0, b = 0;
+  if (!h || !steps || !user_block(h, ip, ib, &ch, &b)) return PS_ATTRIB_ERR;
+  *steps = h->blocks[ch][b].steps;
   return PS_OK;
 }
 
@@ -1061,9 +1104,18 @@ int ps_gpu_get_scalars(ps_handle* h, ps_scalars* out) {
   memset(out, 0, sizeof(*out));
   out->free_energy = s.free_energy;
   out->free_energy_nodis = s.free_energy_nodis;
-  for (int ip = 0; ip < PS_MAX_POLYMERS; ++ip) {
-    out->q[ip] = s.q[ip];
-    out->log_q[ip] = s.log_q[ip];
+  for (int up = 0; up < h->ucfg.n_polymers && up < (int)h->user_first.size(); ++up) {
+    const int c0 = h->user_first[up];
+    if (h->user_ng[up] == 1 && !h->ucfg.polydisperse[up].enabled) {
+      out->q[up] = s.q[c0];
+      out->log_q[up] = s.log_q[c0];
+      continue;
+    }
+    // PsPolyDisperseBCP::getLogBigQ (pspolymer/PsPolyDisperseBCP.cpp:282-305)
+    double sum = 0.0;
+    for (int k = 0; k < h->user_ng[up]; ++k) sum = sum + (log(s.q[c0 + k]) * h->chain_dwt[c0 + k]);
+    out->log_q[up] = sum;
+    out->q[up] = exp(sum);
   }
   out->max_incomp = s.max_incomp;
   out->dh_norm = s.dh_norm;
@@ -1073,10 +1125,9 @@ int ps_gpu_get_scalars(ps_handle* h, ps_scalars* out) {
   return PS_OK;
 }
 
-int ps_gpu_get_propagator(ps_handle* h, int ip, int ib, int end, int n, double* out) {
-  if (!h || !out || ip < 0 || ip >= (int)h->blocks.size() || ib < 0 ||
-      ib >= (int)h->blocks[ip].size())
-    return PS_ATTRIB_ERR;
+int ps_gpu_get_propagator(ps_handle* h, int uip, int uib, int end, int n, double* out) {
+  int ip = 0, ib = 0;
+  if (!h || !out || !user_block(h, uip, uib, &ip, &ib)) return PS_ATTRIB_ERR;
   const BlockMap& b = h->blocks[ip][ib];
   if (n < 0 || n > b.steps) {
     h->err = "slice index out of range";

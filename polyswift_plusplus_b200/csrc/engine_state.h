@@ -71,7 +71,14 @@ template <typename T> struct Buffers {
 }  // namespace psb
 
 struct ps_handle {
-  ps_config cfg;
+  ps_config cfg;   // with every polyDisperseBCP expanded into its quadrature chains
+  ps_config ucfg;  // as the caller gave it
+  // polymer ("chain") index of cfg -> the caller's polymer, its quadrature index,
+  // density weight (1, or w_k / Gamma(alpha)) and the caller's volfrac
+  std::vector<int> chain_user, chain_k;
+  std::vector<double> chain_dwt, chain_vf;
+  // caller's polymer -> first chain and number of chains (1 unless polydisperse)
+  std::vector<int> user_first, user_ng;
   int n[3];
   long long N = 0;
   int nzh = 0;
@@ -175,6 +182,9 @@ void engine_free(ps_handle* h);
 // when its schedule says so; freed with the handle.
 int filter_after_iteration(ps_handle* h, long long step);
 void filter_free(ps_handle* h);
+// polyDisperseBCP (polydisperse.cu): `out` = `in` with each polydisperse polymer
+// replaced by its n_g quadrature chains; fills the chain tables of h.
+int expand_polydisperse(ps_handle* h, const ps_config& in, ps_config* out);
 // Poisson updater (poisson.cu), the same way.
 int poisson_after_iteration(ps_handle* h, long long step);
 void poisson_free(ps_handle* h);

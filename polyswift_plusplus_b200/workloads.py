@@ -19,6 +19,11 @@ point in row-major order, plus the deterministic seeds described per workload.
 * ``triblock256`` 256^3, box 16 Rg, ABC (0.3, 0.4, 0.3), chiN AB 30, BC 30, AC 45,
                   Ns 400, Anderson depth 20, mixed precision; w = U(-0.05, 0.05).
 * ``blend_batch`` 64 diblock / A-homopolymer blend instances (see ``blend_instances``).
+* ``polydisperse_diblock`` the polydisperse example's model: A block (f 0.7, ds 0.02) and
+                  a Schulz-distributed B block (average f 0.3, ds 0.01, alpha 1.5, n_g 4
+                  Gauss-Laguerre points, forceBlockSteps), length 100, chiN 12 (the example
+                  ramps chi with an STFunc; a constant chi stands in), steepest descent
+                  lambda (0.2, 0.1); w = U(-0.1, 0.1) +/- cos(2 pi x / L).
 * ``charged_diblock`` the charged-diblock test deck's model (chargeFlexPseudoSpec A block,
                   za 1, alpha 0.01, length 1000, f_A 0.5, ds 0.05, chi = 1/(20 (3.1415) 1.4),
                   bjerrumLen = 1/(4 (3.1415) 0.01 1.4), simpleIons counter-ions zc -1 with
@@ -196,3 +201,24 @@ def charged_diblock(n=(16, 16, 16), cell=0.05, precision="fp64", poisson_every=5
     u = mt_reals(seed + 1, cfg.n_total)
     psi = 0.05 * c + 0.01 * (u - 0.5)
     return cfg, [w[0] + 1.0 * c, w[1] - 1.0 * c], psi
+
+
+def polydisperse_diblock(n=(16, 16, 16), cell=0.2, n_g=4, schulz_alpha=1.5, precision="fp64",
+                         seed=38383):
+    """(cfg, w) for a diblock whose B block follows a Schulz length distribution."""
+    blocks = [Block(name="blockA", scfield="A", ds=0.02, lengthfrac=0.7, headjoined=["freeEnd"],
+                    tailjoined=["blockB"], force_block_steps=True),
+              Block(name="blockB", scfield="B", ds=0.01, lengthfrac=0.3, headjoined=["blockA"],
+                    tailjoined=["freeEnd"], force_block_steps=True)]
+    cfg = ScftConfig(
+        n=tuple(n), cell=(cell, cell, cell), fields=["A", "B"],
+        polymers=[Polymer(name="diblock1", volfrac=1.0, length=100, blocks=blocks,
+                          kind="polyDisperseBCP", n_g=n_g, schulz_alpha=schulz_alpha,
+                          polyblock="blockB")],
+        interactions=[Interaction(name="AB", chi=0.12, scfields=["A", "B"])],
+        updater=Updater(kind="steepestDescent", relaxlambdas=(0.2, 0.1)), seed=seed,
+        precision=precision)
+    x, _, _ = coords(cfg)
+    c = np.cos(2 * math.pi * x / cfg.box[0]).reshape(-1)
+    w = random_fields(cfg, 0.1)
+    return cfg, [w[0] + 1.0 * c, w[1] - 1.0 * c]

@@ -405,3 +405,66 @@ setupPS(16, 16, 1, 0.05, 0.05, 0.05, "'off'")
     assert (s.zc, s.neutral_factor) == (-1.0, 0.005)
     pp = cfg.poisson.to_ps(cfg)
     assert pp.n_fields == 1 and pp.fields[0] == 0 and pp.bjerrum_len == 5.68
+
+
+def test_config_parser_reads_polydisperse_polymer():
+    """<Polymer> kind = polyDisperseBCP with alpha, n_g and polyblock
+    (pspolymer/PsPolyDisperseBCP.cpp:41-100)."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+setupPS(16, 16, 1, 0.2, 0.2, 0.2, "'off'")
+<EffHamil mainHamil>
+  updaterSequence = [wAwB]
+  <Updater wAwB>
+    kind = steepestDescent
+    relaxlambdas = [0.20 0.10]
+    updatefields = [totStyrDens totEthyDens]
+  </Updater>
+  <Interaction StyrEthy>
+    kind = flory
+    chi = 0.12
+    scfields = [totStyrDens totEthyDens]
+  </Interaction>
+</EffHamil>
+<PhysField totStyrDens>
+  kind = monomerDens
+</PhysField>
+<PhysField totEthyDens>
+  kind = monomerDens
+</PhysField>
+<PhysField defaultPressure>
+  kind = constraint
+</PhysField>
+<Polymer diblock1>
+  kind = polyDisperseBCP
+  n_g = 4
+  alpha = 1.5
+  polyblock = blockB
+  volfrac = 1.0
+  length = 100
+  <Block blockA>
+    kind = flexPseudoSpec
+    scfield = totStyrDens
+    forceBlockSteps = true
+    ds = 0.02
+    lengthfrac = 0.7
+    headjoined = [freeEnd]
+    tailjoined = [blockB]
+  </Block>
+  <Block blockB>
+    kind = flexPseudoSpec
+    scfield = totEthyDens
+    ds = 0.01
+    forceBlockSteps = true
+    lengthfrac = 0.3
+    headjoined = [blockA]
+    tailjoined = [freeEnd]
+  </Block>
+</Polymer>
+"""
+    cfg = config_from_text(text)
+    P = cfg.polymers[0]
+    assert (P.kind, P.n_g, P.schulz_alpha, P.polyblock) == ("polyDisperseBCP", 4, 1.5, "blockB")
+    pc = cfg.to_ps_config()
+    d = pc.polydisperse[0]
+    assert (d.enabled, d.poly_block, d.n_g, d.alpha) == (1, 1, 4, 1.5)

@@ -695,3 +695,48 @@ def test_charged_errors(gpu):
         g.set_poisson(PoissonUpdater(updatefields=["nope"]))
     with pytest.raises(A.PsError):
         g.get_field(A.PS_FIELD_POTENTIAL, 2)
+
+
+# ---------------------------------------------------------------------------
+# polyDisperseBCP
+
+@pytest.mark.parametrize("n", [(16, 16, 16), (16, 12, 1), (8, 4, 256)])
+def test_fp64_polydisperse_parity(gpu, oracle_lib, n):
+    """n_g = 4 quadrature chains on the device (the library's Golub-Welsch nodes) against
+    the oracle (its own root-bracketing nodes, per-block Q): 1e-10; block steps and
+    propagators indexed the reference's way (seed-major quadrature blocks)."""
+    cfg, w = W.polydisperse_diblock(n=n)
+    g, o, hg, ho = run_both(cfg, w, 6)
+    assert_parity(cfg, g, o, hg, ho)
+    for b in range(8):
+        assert g.block_steps(0, b) == o.block_steps(0, b)
+    for b in (0, 3, 5, 7):
+        steps = o.block_steps(0, b)
+        for end in (A.PS_FROM_HEAD, A.PS_FROM_TAIL):
+            for s in (0, steps // 2, steps):
+                assert rel(g.propagator(0, b, end, s), o.propagator(0, b, end, s)) < TOL64
+
+
+def test_mixed_polydisperse_close_to_fp64(gpu):
+    out = []
+    for prec in ("fp64", "mixed"):
+        cfg, w = W.polydisperse_diblock(n=(16, 16, 16), precision=prec)
+        g = ScftSolver(cfg)
+        g.restore(w)
+        g.update(15)
+        out.append(g.scalars()["free_energy"])
+    assert abs(out[1] - out[0]) < 1e-5 * max(abs(out[0]), 1.0)
+
+
+def test_polydisperse_blend_with_homopolymer(gpu, oracle_lib):
+    """A polydisperse diblock (n_g 3) blended with an A homopolymer: chains of both
+    polymers in one graph, F and fields at 1e-10."""
+    import dataclasses
+    from polyswift_plusplus_b200.config import Block, Polymer
+    cfg, w = W.polydisperse_diblock(n=(16, 16, 16), n_g=3)
+    pd = dataclasses.replace(cfg.polymers[0], volfrac=0.85)
+    homo = Polymer(name="homoA", volfrac=0.15, length=50,
+                   blocks=[Block(name="hA", scfield="A", ds=0.02, lengthfrac=1.0)])
+    cfg = dataclasses.replace(cfg, polymers=[pd, homo])
+    g, o, hg, ho = run_both(cfg, w, 5)
+    assert_parity(cfg, g, o, hg, ho)

@@ -461,3 +461,61 @@ def test_charged_block_must_own_its_field(oracle_lib):
     bad = dataclasses.replace(cfg, solvents=cfg.solvents + [Solvent("s", "A", 0.1)])
     with pytest.raises(A.PsError):
         O.Oracle(bad)
+
+
+# ---------------------------------------------------------------------------
+# polyDisperseBCP
+
+@pytest.mark.parametrize("n", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("a", [-0.5, 0.0, 0.5, 2.0])
+def test_gauss_laguerre_rules_match_scipy(oracle_lib, n, a):
+    """The oracle's rule (root bracketing) and the library's (Golub-Welsch, host code, no
+    GPU call) against scipy.special.roots_genlaguerre."""
+    import ctypes as C
+    from scipy.special import roots_genlaguerre
+    xs, ws = roots_genlaguerre(n, a)
+    xo, wo = O.gauss_laguerre(n, a)
+    lib = A.load_library()
+    xl, wl = np.zeros(n), np.zeros(n)
+    assert lib.ps_gauss_laguerre(n, a, xl.ctypes.data_as(C.c_void_p), wl.ctypes.data_as(C.c_void_p)) == 0
+    for x, w in ((xo, wo), (xl, wl)):
+        np.testing.assert_allclose(x, xs, rtol=1e-12)
+        np.testing.assert_allclose(w, ws, rtol=1e-11, atol=1e-14 * ws.max())
+        assert w.sum() == pytest.approx(math.gamma(a + 1.0), rel=1e-13)
+
+
+@pytest.mark.parametrize("n", [(8, 8, 4), (16, 12, 1)])
+def test_polydisperse_oracle_matches_numpy(oracle_lib, n):
+    """Quadrature blocks seed-major, per-block Q, w_k / Gamma(alpha) density and ln Q
+    weights, the 1/n_g length weight of the monodisperse block: the C oracle against the
+    numpy restatement (scipy's nodes) over 5 iterations."""
+    cfg, w = W.polydisperse_diblock(n=n)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    m = NpScft(cfg)
+    m.restore(w)
+    ho = o.update(5)
+    for t in range(5):
+        hm = m.iterate()
+        assert ho[t]["free_energy"] == pytest.approx(hm["free_energy"], rel=1e-11)
+        assert ho[t]["log_q"][0] == pytest.approx(math.log(hm["q"][0]), rel=1e-11, abs=1e-14)
+    for i in range(2):
+        np.testing.assert_allclose(o.w(i), m.w[i].reshape(-1), rtol=0, atol=1e-12)
+        np.testing.assert_allclose(o.phi(i), m.phi[i].reshape(-1), rtol=0, atol=1e-12)
+    steps = [o.block_steps(0, b) for b in range(8)]
+    assert steps[:4] == [35] * 4 and steps[4:] == sorted(steps[4:])
+
+
+def test_polydisperse_one_point_is_monodisperse(oracle_lib):
+    """n_g = 1: the node is alpha (the distribution's mean), the weight Gamma(alpha): one
+    chain with the average length, i.e. the monodisperse diblock."""
+    import dataclasses
+    cfg, w = W.polydisperse_diblock(n=(8, 8, 8), n_g=1, schulz_alpha=2.5)
+    mono = dataclasses.replace(cfg, polymers=[dataclasses.replace(cfg.polymers[0], kind="blockCopolymer")])
+    o1 = O.Oracle(cfg)
+    o1.restore(w)
+    o2 = O.Oracle(mono)
+    o2.restore(w)
+    h1, h2 = o1.update(3), o2.update(3)
+    assert h1[-1]["free_energy"] == pytest.approx(h2[-1]["free_energy"], rel=1e-13)
+    np.testing.assert_allclose(o1.phi(1), o2.phi(1), rtol=0, atol=1e-13)
