@@ -60,4 +60,14 @@ __device__ __forceinline__ C mul_mi(C a) {
   return {a.y, -a.x};
 }
 
+// Programmatic dependent launch (sm_90+).  A sweep kernel launched with the
+// programmatic-serialisation attribute may be launched before the kernel ahead
+// of it on the stream has finished: it does its independent prologue (twiddle
+// tables, work descriptors), then pdl_wait() blocks until that kernel has
+// completed and its writes are visible; without the attribute pdl_wait() is a
+// no-op.  No kernel triggers its dependents early: blocks of the next sweep
+// kernel parked on pdl_wait() would hold shared memory that the concurrent
+// sweep's kernels need (measured 4% slower at 128^3).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace psb

@@ -15,6 +15,7 @@
 // (z only) plus y pencil passes.  Real <-> half-spectrum transforms use the
 // half-length complex FFT of the even/odd samples with an in-place pairwise
 // post-/pre-processing step (k with h-k of the same row).
+#include <stdlib.h>
 #include <cstdio>
 
 #include "fft_smem.cuh"
@@ -457,6 +458,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
   const bool load_spec = (w.mode != MODE_FIRST);
 
   if (BULK && load_spec && tid == 0) {
+    pdl_wait();
     mbar_init(bar, 1);
     fence_mbar_init();
     mbar_arrive_expect_tx(bar, SPEC_BYTES);
@@ -469,6 +471,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
   if constexpr (DO_Y) {
     for (int i = tid; i < ROWS; i += TH) s_tw_y[i] = tw_y[i];
   }
+  pdl_wait();  // before any read of the spectrum, src or wfac, and any write
 
   if (load_spec) {
     if constexpr (BULK) {
@@ -644,6 +647,8 @@ __global__ void __launch_bounds__(TH)
   const int c0 = (blockIdx.x - o * tiles) * TK;
   C* base = w.spec + (size_t)o * L * inner;
   const bool full = (c0 + TK <= inner) && (inner % CPV == 0);
+  for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
+  pdl_wait();  // before any read or write of the spectrum
   if (full) {
     V v[UV];
 #pragma unroll
@@ -668,7 +673,6 @@ __global__ void __launch_bounds__(TH)
       buf[e] = (c < inner) ? base[(size_t)i * inner + c] : C{T(0), T(0)};
     }
   }
-  for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
   __syncthreads();
   if constexpr (MODE == PENCIL_KINV && L > 1 && FK) {
     // forward FFT, k2 multiply and inverse FFT with the last forward pass, the
@@ -757,6 +761,33 @@ static cudaError_t ensure_smem_attr(K kern, size_t smem, unsigned* done_mask) {
   return e;
 }
 
+// Sweep kernels are launched with programmatic stream serialisation (they call
+// pdl_wait() before touching data another kernel wrote), unless PSB_PDL=0.
+static bool pdl_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("PSB_PDL");
+    on = (e && e[0] == '0') ? 0 : 1;
+  }
+  return on != 0;
+}
+
+template <typename... K, typename... Args>
+static cudaError_t launch_sweep_kernel(void (*kern)(K...), dim3 grid, dim3 block, size_t smem,
+                                       cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 static const int kExtents[] = {1, 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 256};
 
 bool extent_supported(int n) {
@@ -780,8 +811,8 @@ static cudaError_t launch_plane_t(const PlaneWork<T>* d_works, int nworks, int n
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
   if (ea != cudaSuccess) return ea;
   dim3 grid(ntiles, nworks);
-  kern<<<grid, TH, smem, st>>>(d_works, nrows_total, tw_y, tw_zh, tw_z, lt_nx, lt_ny);
-  return cudaGetLastError();
+  return launch_sweep_kernel(kern, grid, dim3(TH), smem, st, d_works, nrows_total, tw_y, tw_zh, tw_z,
+                             lt_nx, lt_ny);
 }
 
 // (ny, nz) planes with a fused y-z kernel instantiation.
@@ -913,6 +944,8 @@ __global__ void __launch_bounds__(TH)
   const int kz = blockIdx.x;
   const int tid = threadIdx.x;
   C* base = w.spec + (size_t)kz * NE;
+  for (int i = tid; i < NXY; i += TH) s_tw[i] = tw[i];
+  pdl_wait();  // before any read or write of the spectrum
   {
     V v[UV];
 #pragma unroll
@@ -920,7 +953,6 @@ __global__ void __launch_bounds__(TH)
       const int e = tid + u * TH;
       if (NV % TH == 0 || e < NV) v[u] = reinterpret_cast<const V*>(base)[e];
     }
-    for (int i = tid; i < NXY; i += TH) s_tw[i] = tw[i];
 #pragma unroll
     for (int u = 0; u < UV; ++u) {
       const int e = tid + u * TH;
@@ -986,8 +1018,7 @@ static cudaError_t launch_xy_t(const PencilWork<T>* d_works, int nworks, int nzh
   cudaError_t ea = ensure_smem_attr(kern, smem, &attr_mask);
   if (ea != cudaSuccess) return ea;
   dim3 grid(nzh, nworks);
-  kern<<<grid, TH, smem, st>>>(d_works, nzh, tw);
-  return cudaGetLastError();
+  return launch_sweep_kernel(kern, grid, dim3(TH), smem, st, d_works, nzh, tw);
 }
 
 static const int kXYShapes[] = {8, 16, 32, 64, 96, 128};
@@ -1029,8 +1060,7 @@ static cudaError_t launch_pencil_t(const PencilWork<T>* d_works, int nworks, int
   if (ea != cudaSuccess) return ea;
   const int tiles = (inner + TK - 1) / TK;
   dim3 grid(outer * tiles, nworks);
-  kern<<<grid, TH, smem, st>>>(d_works, inner, tiles, tw, nx, ny, nz);
-  return cudaGetLastError();
+  return launch_sweep_kernel(kern, grid, dim3(TH), smem, st, d_works, inner, tiles, tw, nx, ny, nz);
 }
 
 template <typename T, int L, int TK, int TH>
