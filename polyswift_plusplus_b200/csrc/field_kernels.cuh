@@ -8,7 +8,7 @@
 
 namespace psb {
 
-constexpr int kRedBlocks = 296;  // 2 x 148 SMs; fixed so every reduction is deterministic
+constexpr int kRedBlocks = 1184;  // 8 x 148 SMs; fixed so every reduction is deterministic
 constexpr int kRedThreads = 256;
 
 // Device-resident scalars of the current iteration.
