@@ -66,6 +66,9 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched blend workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="pin the propagator kernel variant (0..15) instead of autotuning, e.g. "
+                         "so that a profiler run uses the variant the plain run chose")
     ap.add_argument("--workload", choices=["diblock128", "triblock256"], default="diblock128",
                     help="triblock256: the 256^3 ABC scale case (about 75 GB on the device; "
                          "reports the variable-cell stress step instead of the 128^3 extras)")
@@ -372,6 +375,8 @@ def run_ours(args, world, rank, local):
         wl, grid, ns, upd = WORKLOAD, args.n, 200, "anderson10"
     cfg.device = local
     solver = ScftSolver(cfg)
+    if args.variant >= 0:
+        solver.set_variant(args.variant)
     solver.restore(w)
     stream = torch.cuda.ExternalStream(solver.stream_ptr, device=torch.device("cuda", local))
 
