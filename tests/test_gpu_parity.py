@@ -740,3 +740,18 @@ def test_polydisperse_blend_with_homopolymer(gpu, oracle_lib):
     cfg = dataclasses.replace(cfg, polymers=[pd, homo])
     g, o, hg, ho = run_both(cfg, w, 5)
     assert_parity(cfg, g, o, hg, ho)
+
+
+@pytest.mark.parametrize("axis", [0, 2])
+def test_kat7_debye_response_gpu(gpu, axis):
+    """The device's weak-segregation response against the Debye functions (see the
+    oracle's KAT7), FP64: 1e-4."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_oracle import mode_amplitude, rpa_case
+    cfg, w, k, eps, (gaa, gab) = rpa_case(axis)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(1)
+    assert mode_amplitude(g.phi(0), cfg, axis) == pytest.approx(-eps * gaa, rel=1e-4)
+    assert mode_amplitude(g.phi(1), cfg, axis) == pytest.approx(-eps * gab, rel=1e-4)

@@ -519,3 +519,45 @@ def test_polydisperse_one_point_is_monodisperse(oracle_lib):
     h1, h2 = o1.update(3), o2.update(3)
     assert h1[-1]["free_energy"] == pytest.approx(h2[-1]["free_energy"], rel=1e-13)
     np.testing.assert_allclose(o1.phi(1), o2.phi(1), rtol=0, atol=1e-13)
+
+
+def debye(f, x):
+    """Debye function of a block of contour fraction f at x = k^2 Rg^2."""
+    return 2.0 * (f * x + math.exp(-f * x) - 1.0) / (x * x)
+
+
+def rpa_case(axis, ns=100):
+    """A weak single-mode w_A along `axis` on an AB diblock (f = 0.3): its linear response."""
+    cfg = W.diblock_config(32, 4.0, 0.30, 20.0, ns, Updater(kind="steepestDescent", relaxlambdas=(0.1, 0.05)))
+    n = [4, 4, 4]
+    n[axis] = 32
+    cell = [0.1, 0.1, 0.1]
+    cell[axis] = 4.0 / 32
+    cfg.n, cfg.cell = tuple(n), tuple(cell)
+    coords = W.coords(cfg)
+    k = 2 * math.pi / cfg.box[axis]
+    eps = 1e-4
+    wa = (eps * np.cos(k * coords[axis])).reshape(-1)
+    x = k * k
+    gaa, gbb = debye(0.3, x), debye(0.7, x)
+    gab = 0.5 * (debye(1.0, x) - gaa - gbb)
+    return cfg, [wa, np.zeros_like(wa)], k, eps, (gaa, gab)
+
+
+def mode_amplitude(phi, cfg, axis):
+    line = np.moveaxis(phi.reshape(cfg.n), axis, 0)[:, 0, 0]
+    return 2.0 * np.fft.fft(line)[1].real / cfg.n[axis]
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_kat7_weak_segregation_debye_response(oracle_lib, axis):
+    """KAT7: for w_A = eps cos(k r) the densities respond as -eps g_AA(k) and -eps g_AB(k),
+    the random-phase (Debye-function) correlations of an ideal diblock, with lengths in Rg
+    and the contour in units of N.  Pins the k^2 convention along every axis, the step and
+    the quadrature: 1e-4 at Ns = 100 (the 0.33333 Simpson factor alone is 1e-5)."""
+    cfg, w, k, eps, (gaa, gab) = rpa_case(axis)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    o.update(1)  # densities of the given fields (the update changes w afterwards)
+    assert mode_amplitude(o.phi(0), cfg, axis) == pytest.approx(-eps * gaa, rel=1e-4)
+    assert mode_amplitude(o.phi(1), cfg, axis) == pytest.approx(-eps * gab, rel=1e-4)
