@@ -567,6 +567,10 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
     return rc;
   }
   ps_handle* h = a->h;
+  if (h->branched) {
+    a->err = "the adjoint takes a linear chain (this polymer is branched)";
+    return PS_INPUT_ERR;
+  }
   if (h->exec.size() != 2) {
     a->err = "the adjoint needs two distinct sweeps (mirror-symmetric chains are not supported)";
     return PS_INPUT_ERR;

@@ -275,6 +275,11 @@ static int batch_create(ps_batch* b, const ps_config* cfgs, int count) {
     }
     h->in_batch = true;
     b->inst.push_back(h);
+    if (h->branched) {
+      b->err = "instance " + std::to_string(i) +
+               ": a branched polymer runs as its own handle (its sweeps depend on one another)";
+      return PS_INPUT_ERR;
+    }
     auto key = std::make_tuple(h->n[0], h->n[1], h->n[2], h->prec);
     auto it = cls.find(key);
     int ci;

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <map>
 #include <string>
 #include <vector>
@@ -107,6 +108,114 @@ static bool chain_sweeps(const ps_polymer_config& P, std::vector<std::pair<int, 
   return true;
 }
 
+// Sweeps of a branched (tree-shaped) polymer, following the reference's
+// dependency-driven solve order (pspolymer/PsBlockCopolymer.cpp:189-313,
+// pspolymer/PsBlock.cpp:387-472).  Each directed propagation "block b solved
+// from end e" appears in exactly one sweep.  A sweep starts at a free end (q = 1)
+// or at a junction of three or more block ends (q = product of the final q of
+// the other blocks there), runs through simple block-to-block joins, and stops
+// at the next free end or junction.  Sweeps are appended in dependency order.
+// Returns an empty string, or why the architecture is not supported.
+static std::string tree_sweeps(ps_handle* h, int ip, const ps_polymer_config& P) {
+  const int nb = P.n_blocks;
+  auto conns = [&](int b, int e) -> std::vector<int> {
+    const ps_block_config& B = P.blocks[b];
+    std::vector<int> v;
+    if (e == HEAD) v.assign(B.head_joined, B.head_joined + B.n_head);
+    else v.assign(B.tail_joined, B.tail_joined + B.n_tail);
+    std::sort(v.begin(), v.end());  // junction products in ascending block order
+    return v;
+  };
+  for (int b = 0; b < nb; ++b)
+    for (int e = 0; e < 2; ++e)
+      for (int c : conns(b, e)) {
+        if (c < 0 || c >= nb || c == b) return "joined block index out of range";
+        const auto back = conns(c, joined_end(P, b, c));
+        if (std::find(back.begin(), back.end(), b) == back.end()) return "inconsistent head/tail joins";
+      }
+  // a simple join: the end meets exactly one other block end, which meets only it
+  auto simple = [&](int b, int e) -> bool {
+    const auto c = conns(b, e);
+    return c.size() == 1 && conns(c[0], joined_end(P, b, c[0])).size() == 1;
+  };
+  // sweep_of[b][e]: sweep holding "b solved from e"
+  std::vector<std::array<int, 2>> sweep_of(nb, {-1, -1});
+  std::vector<Sweep> made;
+  std::vector<std::vector<std::pair<int, int>>> need;  // (block, end) of each input: solved from that end's far side
+  for (int b = 0; b < nb; ++b)
+    for (int e = 0; e < 2; ++e) {
+      const auto c0 = conns(b, e);
+      if (simple(b, e)) continue;  // reached by continuing another sweep
+      Sweep sw;
+      sw.polymer = ip;
+      std::vector<std::pair<int, int>> in;
+      for (int c : c0) in.push_back({c, joined_end(P, b, c)});
+      int cb = b, ce = e;
+      for (int guard = 0; guard <= 2 * nb; ++guard) {
+        if (sweep_of[cb][ce] >= 0) return "a block graph with a cycle";
+        sweep_of[cb][ce] = (int)made.size();
+        Seg g;
+        g.block = cb;
+        g.from = ce;
+        g.off = sw.total;
+        g.steps = h->blocks[ip][cb].steps;
+        g.wfac_id = g.ktab_id = -1;
+        sw.segs.push_back(g);
+        sw.total += g.steps;
+        const int o = (ce == HEAD) ? TAIL : HEAD;
+        if (!simple(cb, o)) break;
+        const int nbk = conns(cb, o)[0];
+        ce = joined_end(P, cb, nbk);
+        cb = nbk;
+      }
+      made.push_back(sw);
+      need.push_back(in);
+    }
+  for (int b = 0; b < nb; ++b)
+    if (sweep_of[b][0] < 0 || sweep_of[b][1] < 0) return "a block graph with a cycle";
+  // inputs: the sweep arriving at each joined end (it ends there: a junction stops a sweep)
+  std::vector<std::vector<int>> in_sweeps(made.size());
+  for (size_t i = 0; i < made.size(); ++i)
+    for (auto& ce : need[i]) {
+      const int far = (ce.second == HEAD) ? TAIL : HEAD;
+      in_sweeps[i].push_back(sweep_of[ce.first][far]);
+    }
+  // dependency order
+  std::vector<int> order, placed(made.size(), 0);
+  for (size_t round = 0; round < made.size() && order.size() < made.size(); ++round)
+    for (size_t i = 0; i < made.size(); ++i) {
+      if (placed[i]) continue;
+      bool ready = true;
+      for (int j : in_sweeps[i]) ready = ready && placed[j];
+      if (ready) {
+        placed[i] = 1;
+        order.push_back((int)i);
+      }
+    }
+  if (order.size() != made.size()) return "a block graph with a cycle";
+  std::vector<int> index_of(made.size());
+  const int base = (int)h->sweeps.size();
+  for (size_t r = 0; r < order.size(); ++r) index_of[order[r]] = base + (int)r;
+  for (int i : order) {
+    Sweep sw = made[i];
+    for (int j : in_sweeps[i]) sw.jin.push_back({index_of[j], made[j].total});
+    if (!sw.jin.empty()) {
+      if ((int)sw.jin.size() > PS_MAX_JOINS) return "too many blocks at one junction";
+      sw.jbuf = h->n_jbuf++;
+      h->branched = true;
+    }
+    sw.storage = (int)h->exec.size();
+    h->exec.push_back((int)h->sweeps.size());
+    for (const Seg& g : sw.segs) {
+      BlockMap& bm = h->blocks[ip][g.block];
+      if (g.from == HEAD) { bm.sweep_head = (int)h->sweeps.size(); bm.off_head = g.off; }
+      else { bm.sweep_tail = (int)h->sweeps.size(); bm.off_tail = g.off; }
+    }
+    h->sweeps.push_back(sw);
+  }
+  return "";
+}
+
 template <typename T>
 static int alloc_copy(ps_handle* h, T** dst, const std::vector<T>& src) {
   PS_CUDA(h, cudaMalloc((void**)dst, sizeof(T) * std::max<size_t>(src.size(), 1)));
@@ -154,6 +263,11 @@ static int build_device_tables(ps_handle* h) {
     T* wf = nullptr;
     PS_CUDA(h, cudaMalloc((void**)&wf, sizeof(T) * (size_t)N));
     B.wfac.push_back(wf);
+  }
+  for (int i = 0; i < h->n_jbuf; ++i) {
+    T* jb = nullptr;
+    PS_CUDA(h, cudaMalloc((void**)&jb, sizeof(T) * (size_t)N));
+    B.jbuf.push_back(jb);
   }
   for (auto& kk : h->ktab_keys) {
     const double ds = kk.first, b = kk.second;
@@ -217,7 +331,7 @@ static int build_device_tables(ps_handle* h) {
       PlaneWork<T> w;
       memset(&w, 0, sizeof(w));
       w.mode = (k == 0) ? MODE_FIRST : (k == sw.total ? MODE_LAST : MODE_MID);
-      w.src = nullptr;
+      w.src = (k == 0 && sw.jbuf >= 0) ? B.jbuf[sw.jbuf] : nullptr;
       w.spec = B.spec[e];
       w.wfac_in = (k > 0) ? B.wfac[seg_of(sw, k - 1).wfac_id] : nullptr;
       w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
@@ -247,6 +361,10 @@ static int build_device_tables(ps_handle* h) {
 template <typename T>
 static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
   if (!(variant & VARIANT_SPLIT) || h->sw_st.empty()) {
+    if (h->branched) {
+      h->err = "a branched polymer's sweeps run as dependent launch chains (variant bit 8) only";
+      return PS_ATTRIB_ERR;
+    }
     PS_CUDA(h, launch_sweep_set<T>(handle_sweep_set<T>(h), variant, h->st, nlaunch));
     return PS_OK;
   }
@@ -259,6 +377,21 @@ static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
     s.pencil_off = h->sw_pencil_off[e].data();
     s.pencil_cnt = h->sw_pencil_cnt[e].data();
     PS_CUDA(h, cudaStreamWaitEvent(h->sw_st[e], h->ev_split, 0));
+    const Sweep& sw = h->sweeps[h->exec[e]];
+    if (sw.jbuf >= 0) {
+      // junction start (PsBlock::combineSetJnt): after the arriving sweeps
+      Buffers<T>& B = bufs<T>(h);
+      JunctionIn<T> in;
+      memset(&in, 0, sizeof(in));
+      in.n = (int)sw.jin.size();
+      for (int i = 0; i < in.n; ++i) {
+        const int es = h->sweeps[sw.jin[i].first].storage;
+        PS_CUDA(h, cudaStreamWaitEvent(h->sw_st[e], h->sw_ev[es], 0));
+        in.q[i] = B.slices[es] + (size_t)sw.jin[i].second * h->N;
+      }
+      PS_CUDA(h, launch_junction<T>(in, h->N, B.jbuf[sw.jbuf], h->sw_st[e]));
+      ++*nlaunch;
+    }
     PS_CUDA(h, launch_sweep_set<T>(s, variant & ~VARIANT_SPLIT, h->sw_st[e], nlaunch));
     PS_CUDA(h, cudaEventRecord(h->sw_ev[e], h->sw_st[e]));
     PS_CUDA(h, cudaStreamWaitEvent(h->st, h->sw_ev[e], 0));
@@ -299,7 +432,7 @@ static int launch_iteration(ps_handle* h, long long* nlaunch) {
   // node of the graph (a plain record would only order the capture).
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_start, h->st, cudaEventRecordExternal));
-  rc = launch_sweeps<T>(h, nlaunch, h->variant < 0 ? 0 : h->variant);
+  rc = launch_sweeps<T>(h, nlaunch, h->variant < 0 ? (h->branched ? VARIANT_SPLIT : 0) : h->variant);
   if (rc) return rc;
   if (h->timing_cap > 0)
     PS_CUDA(h, cudaEventRecordWithFlags(h->ev_cap_end, h->st, cudaEventRecordExternal));
@@ -392,6 +525,7 @@ static int autotune_t(ps_handle* h) {
     h->tune_ms[v] = -1.f;
     if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
     if ((v & VARIANT_SPLIT) && h->sw_st.empty()) continue;                 // one sweep only
+    if (!(v & VARIANT_SPLIT) && h->branched) continue;                     // chains only
     long long nl = 0;
     rc = launch_sweeps<T>(h, &nl, v);  // warm-up
     if (rc == PS_OK) e = cudaEventRecord(a, h->st);
@@ -461,6 +595,7 @@ template <typename T> static void free_buffers(Buffers<T>& B) {
   for (auto p : B.slices) f(p);
   for (auto p : B.spec) f(p);
   for (auto p : B.wfac) f(p);
+  for (auto p : B.jbuf) f(p);
   for (auto p : B.kx) f(p);
   for (auto p : B.kyz) f(p);
   f(B.tw_x); f(B.tw_y); f(B.tw_z); f(B.tw_zh); f(B.d_plane); f(B.d_pencil);
@@ -681,9 +816,12 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
     const ps_polymer_config& P = c.polymers[ip];
     std::vector<std::pair<int, int>> order;
     if (!chain_sweeps(P, order)) {
-      h->err = "polymer " + std::to_string(ip) +
-               ": only linear block sequences run on the device path";
-      return PS_INPUT_ERR;
+      const std::string why = tree_sweeps(h, ip, P);
+      if (!why.empty()) {
+        h->err = "polymer " + std::to_string(ip) + ": " + why;
+        return PS_INPUT_ERR;
+      }
+      continue;
     }
     Sweep a, b;
     a.polymer = b.polymer = ip;
@@ -1167,6 +1305,10 @@ int ps_gpu_set_variant(ps_handle* h, int variant) {
   if (!h || variant < -1 || variant >= VARIANT_COUNT) return PS_ATTRIB_ERR;
   if (variant >= 0 && (variant & VARIANT_XY) && !h->xy_ok) {
     h->err = "the row + x-y plane design does not exist for this grid";
+    return PS_ATTRIB_ERR;
+  }
+  if (variant >= 0 && !(variant & VARIANT_SPLIT) && h->branched) {
+    h->err = "a branched polymer's sweeps run as dependent launch chains: set variant bit 8";
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));

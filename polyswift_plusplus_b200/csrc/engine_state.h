@@ -29,6 +29,11 @@ struct Sweep {
   std::vector<Seg> segs;
   int total = 0;
   int storage = -1;  // index of the executed sweep holding its slices
+  // Branched polymers: a sweep that starts at a junction of three or more block
+  // ends starts from the product of the final slices (sweep, slice) of the
+  // sweeps arriving there, written into junction buffer jbuf before it runs.
+  std::vector<std::pair<int, int>> jin;
+  int jbuf = -1;
 };
 
 // Boltzmann-factor table key: one wfac array per distinct (field, ds, charge)
@@ -57,6 +62,7 @@ template <typename T> struct Buffers {
   std::vector<T*> slices;        // per executed sweep: (total+1)*N
   std::vector<c2_t<T>*> spec;    // per executed sweep
   std::vector<T*> wfac;          // per (field, ds) key
+  std::vector<T*> jbuf;          // junction start buffers of branched polymers (N each)
   std::vector<T*> kx, kyz;       // per (ds, bseg) key
   c2_t<T>* tw_x = nullptr;
   c2_t<T>* tw_y = nullptr;
@@ -138,6 +144,8 @@ struct ps_handle {
   float tune_ms[psb::VARIANT_COUNT] = {};
   bool xy_ok = false;  // the row + x-y plane design exists for this grid
   bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
+  bool branched = false;  // a branched polymer: its sweeps run as dependent launch chains only
+  int n_jbuf = 0;
   bool no_slices = false; // tables only, no slice storage (the adjoint keeps its own)
   void* filter = nullptr;  // spectral filter updater (filter.cu), or nullptr
   void* poisson = nullptr; // Poisson updater (poisson.cu), or nullptr

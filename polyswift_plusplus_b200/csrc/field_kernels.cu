@@ -87,6 +87,26 @@ cudaError_t launch_wfac(const double* w, T* wfac, double ds2, long long N, cudaS
 template cudaError_t launch_wfac<float>(const double*, float*, double, long long, cudaStream_t);
 template cudaError_t launch_wfac<double>(const double*, double*, double, long long, cudaStream_t);
 
+template <typename T>
+__global__ void junction_kernel(JunctionIn<T> in, long long N, T* __restrict__ out) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    T p = T(1);
+    for (int i = 0; i < in.n; ++i) p = p * in.q[i][r];
+    out[r] = p;
+  }
+}
+
+template <typename T>
+cudaError_t launch_junction(const JunctionIn<T>& in, long long N, T* out, cudaStream_t st) {
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  junction_kernel<T><<<blocks, 256, 0, st>>>(in, N, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_junction<float>(const JunctionIn<float>&, long long, float*, cudaStream_t);
+template cudaError_t launch_junction<double>(const JunctionIn<double>&, long long, double*, cudaStream_t);
+
 __global__ void zero_kernel(double* p, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)

@@ -77,6 +77,15 @@ cudaError_t launch_quadrature(const T* qs, const T* qts, int steps, long long N,
 
 cudaError_t launch_zero(double* p, long long n, cudaStream_t st);
 
+// Junction of a branched polymer (PsBlock::combineSetJnt): out = 1 * q_0 * q_1 * ...
+// over the final slices of the blocks joined there, in ascending block order.
+template <typename T> struct JunctionIn {
+  const T* q[PS_MAX_JOINS];
+  int n;
+};
+template <typename T>
+cudaError_t launch_junction(const JunctionIn<T>& in, long long N, T* out, cudaStream_t st);
+
 // simpleSolvent (pssolvent/PsSimpleSolvent.cpp:86-140): Q = <exp(-w/L)> into
 // sc->solv_q[is], then phi += (volfrac / Q) exp(-w/L).
 cudaError_t launch_solvent(const double* w, double neg_inv_len, double volfrac, long long N, int is,

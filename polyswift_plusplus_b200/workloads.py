@@ -24,6 +24,9 @@ point in row-major order, plus the deterministic seeds described per workload.
                   Gauss-Laguerre points, forceBlockSteps), length 100, chiN 12 (the example
                   ramps chi with an STFunc; a constant chi stands in), steepest descent
                   lambda (0.2, 0.1); w = U(-0.1, 0.1) +/- cos(2 pi x / L).
+* ``star_abc``    a three-arm ABC star (the reference's star example: every arm's head free,
+                  the tails joined at one junction), chiN 15 for each pair, ds 0.01;
+                  w = U(-0.2, 0.2).
 * ``charged_diblock`` the charged-diblock test deck's model (chargeFlexPseudoSpec A block,
                   za 1, alpha 0.01, length 1000, f_A 0.5, ds 0.05, chi = 1/(20 (3.1415) 1.4),
                   bjerrumLen = 1/(4 (3.1415) 0.01 1.4), simpleIons counter-ions zc -1 with
@@ -222,3 +225,22 @@ def polydisperse_diblock(n=(16, 16, 16), cell=0.2, n_g=4, schulz_alpha=1.5, prec
     c = np.cos(2 * math.pi * x / cfg.box[0]).reshape(-1)
     w = random_fields(cfg, 0.1)
     return cfg, [w[0] + 1.0 * c, w[1] - 1.0 * c]
+
+
+def star(fracs=(0.3, 0.3, 0.4), fields=("A", "B", "C"), ds=0.01, length=100, name="star"):
+    """An arm-star: arm i has a free head and its tail at the one junction."""
+    arms = [f"{name}_{k}" for k in range(len(fracs))]
+    blocks = [Block(name=arms[k], scfield=fields[k], ds=ds, lengthfrac=fracs[k], headjoined=["freeEnd"],
+                    tailjoined=[a for a in arms if a != arms[k]]) for k in range(len(fracs))]
+    return Polymer(name=name, volfrac=1.0, length=length, blocks=blocks)
+
+
+def star_abc(n=16, box=3.2, precision="fp64", fracs=(0.3, 0.3, 0.4), seed=515):
+    """(cfg, w) for a three-arm ABC star melt."""
+    cfg = ScftConfig(
+        n=(n, n, n), cell=(box / n,) * 3, fields=["A", "B", "C"], polymers=[star(fracs)],
+        interactions=[Interaction("AB", 0.15, ["A", "B"]), Interaction("BC", 0.15, ["B", "C"]),
+                      Interaction("AC", 0.15, ["A", "C"])],
+        updater=Updater(kind="steepestDescent", relaxlambdas=(0.05, 0.025)), seed=seed,
+        precision=precision)
+    return cfg, random_fields(cfg, 0.2)

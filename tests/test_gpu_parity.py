@@ -755,3 +755,100 @@ def test_kat7_debye_response_gpu(gpu, axis):
     g.update(1)
     assert mode_amplitude(g.phi(0), cfg, axis) == pytest.approx(-eps * gaa, rel=1e-4)
     assert mode_amplitude(g.phi(1), cfg, axis) == pytest.approx(-eps * gab, rel=1e-4)
+
+
+# ---------------------------------------------------------------------------
+# Branched polymers
+
+def _tree_h(n=16):
+    """Two junctions: arms A, B and the backbone C meet at one, C, D, E at the other."""
+    ds = 0.01
+    blocks = [Block("a", "A", ds, 0.15, ["freeEnd"], ["b", "c"]),
+              Block("b", "B", ds, 0.15, ["freeEnd"], ["a", "c"]),
+              Block("c", "C", ds, 0.40, ["a", "b"], ["d", "e"]),
+              Block("d", "A", ds, 0.15, ["freeEnd"], ["c", "e"]),
+              Block("e", "B", ds, 0.15, ["freeEnd"], ["c", "d"])]
+    cfg = ScftConfig(n=(n, n, n), cell=(0.2,) * 3, fields=["A", "B", "C"],
+                     polymers=[Polymer("h", 1.0, 100, blocks)],
+                     interactions=[Interaction("AB", 0.12, ["A", "B"]), Interaction("BC", 0.12, ["B", "C"]),
+                                   Interaction("AC", 0.15, ["A", "C"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)), seed=77)
+    return cfg, W.random_fields(cfg, 0.2)
+
+
+def _star4(n=16):
+    from polyswift_plusplus_b200.workloads import star
+    cfg = ScftConfig(n=(n, n, n), cell=(0.2,) * 3, fields=["A", "B", "C"],
+                     polymers=[star((0.2, 0.3, 0.25, 0.25), fields=("A", "B", "C", "A"))],
+                     interactions=[Interaction("AB", 0.15, ["A", "B"]), Interaction("BC", 0.15, ["B", "C"]),
+                                   Interaction("AC", 0.15, ["A", "C"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)), seed=78)
+    return cfg, W.random_fields(cfg, 0.2)
+
+
+@pytest.mark.parametrize("case", ["star3", "star3_split_plane", "star4", "tree_h"])
+def test_fp64_branched_polymer_parity(gpu, oracle_lib, case):
+    """Branched polymers (PsBlockCopolymer's dependency-driven solve order) on the device:
+    sweeps from free ends, junction products, sweeps from junctions, against the oracle's
+    general block scheduler at 1e-10, with every block's propagators from both ends."""
+    if case.startswith("star3"):
+        cfg, w = W.star_abc(n=16)
+        if case == "star3_split_plane":
+            cfg.n, cfg.cell = (8, 4, 256), (0.4, 0.4, 0.0125)
+            w = W.random_fields(cfg, 0.2)
+    elif case == "star4":
+        cfg, w = _star4()
+    else:
+        cfg, w = _tree_h()
+    g, o, hg, ho = run_both(cfg, w, 6)
+    assert_parity(cfg, g, o, hg, ho)
+    assert g.variant()[0] & 8  # dependent launch chains
+    for b in range(len(cfg.polymers[0].blocks)):
+        steps = o.block_steps(0, b)
+        assert g.block_steps(0, b) == steps
+        for end in (A.PS_FROM_HEAD, A.PS_FROM_TAIL):
+            for s in (0, steps):
+                assert rel(g.propagator(0, b, end, s), o.propagator(0, b, end, s)) < TOL64
+
+
+def test_kat7_star_debye_response_gpu(gpu):
+    """The star's weak-segregation response on the device (see the oracle's KAT7)."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_oracle import debye, mode_amplitude
+    fr = (0.3, 0.3, 0.4)
+    cfg = ScftConfig(n=(32, 4, 4), cell=(4.0 / 32, 0.1, 0.1), fields=["A", "B", "C"],
+                     polymers=[W.star(fr)], interactions=[Interaction("AB", 0.15, ["A", "B"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)))
+    x = W.coords(cfg)[0]
+    k = 2 * math.pi / cfg.box[0]
+    eps = 1e-4
+    wa = (eps * np.cos(k * x)).reshape(-1)
+    g = ScftSolver(cfg)
+    g.restore([wa, np.zeros_like(wa), np.zeros_like(wa)])
+    g.update(1)
+    kk = k * k
+    want = [debye(fr[0], kk)] + [0.5 * (debye(fr[0] + f, kk) - debye(fr[0], kk) - debye(f, kk)) for f in fr[1:]]
+    for i in range(3):
+        assert mode_amplitude(g.phi(i), cfg, 0) == pytest.approx(-eps * want[i], rel=1e-4)
+
+
+def test_branched_polymer_mixed_and_errors(gpu):
+    """Mixed-precision star within 1e-5 of FP64; a star takes only dependent-chain variants
+    and no batch."""
+    from polyswift_plusplus_b200.scft import ScftBatch
+    out = []
+    for prec in ("fp64", "mixed"):
+        cfg, w = W.star_abc(n=16, precision=prec)
+        g = ScftSolver(cfg)
+        g.restore(w)
+        g.update(10)
+        out.append(g.scalars()["free_energy"])
+        with pytest.raises(A.PsError):
+            g.set_variant(1)
+        g.set_variant(9)
+        g.update(1)
+    assert abs(out[1] - out[0]) < 1e-5 * max(abs(out[0]), 1.0)
+    cfg, _ = W.star_abc(n=16)
+    with pytest.raises(A.PsError):
+        ScftBatch([cfg])

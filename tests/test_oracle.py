@@ -561,3 +561,25 @@ def test_kat7_weak_segregation_debye_response(oracle_lib, axis):
     o.update(1)  # densities of the given fields (the update changes w afterwards)
     assert mode_amplitude(o.phi(0), cfg, axis) == pytest.approx(-eps * gaa, rel=1e-4)
     assert mode_amplitude(o.phi(1), cfg, axis) == pytest.approx(-eps * gab, rel=1e-4)
+
+
+def test_kat7_star_debye_response(oracle_lib):
+    """KAT7 on a three-arm star: arm A responds as -eps g(f_A); arm X joined to A at the
+    junction as -eps (g(f_A + f_X) - g(f_A) - g(f_X)) / 2, the correlation along the path
+    through the junction.  Pins the oracle's junction products: 1e-4."""
+    from polyswift_plusplus_b200.config import Interaction, ScftConfig
+    fr = (0.3, 0.3, 0.4)
+    cfg = ScftConfig(n=(32, 4, 4), cell=(4.0 / 32, 0.1, 0.1), fields=["A", "B", "C"],
+                     polymers=[W.star(fr)], interactions=[Interaction("AB", 0.15, ["A", "B"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)))
+    x = W.coords(cfg)[0]
+    k = 2 * math.pi / cfg.box[0]
+    eps = 1e-4
+    wa = (eps * np.cos(k * x)).reshape(-1)
+    o = O.Oracle(cfg)
+    o.restore([wa, np.zeros_like(wa), np.zeros_like(wa)])
+    o.update(1)
+    kk = k * k
+    want = [debye(fr[0], kk)] + [0.5 * (debye(fr[0] + f, kk) - debye(fr[0], kk) - debye(f, kk)) for f in fr[1:]]
+    for i in range(3):
+        assert mode_amplitude(o.phi(i), cfg, 0) == pytest.approx(-eps * want[i], rel=1e-4)
