@@ -209,7 +209,10 @@ const char* ps_gpu_last_error(const ps_handle* h);
 
 /* Build the device state for one SCFT instance.  Performs the reference's
  * setAttrib/buildData/buildSolvers checks: block-step rounding, sum of length
- * fractions, sum of volume fractions, supported grid extents. */
+ * fractions, sum of volume fractions, supported grid extents.  Polymers may be
+ * linear or branched (trees of blocks joined at their ends, as head_joined /
+ * tail_joined describe; a junction joins at most PS_MAX_JOINS + 1 block ends);
+ * cyclic block graphs are PS_INPUT_ERR (pspolymer/PsBlockCopolymer.cpp:189-313). */
 int ps_gpu_create(const ps_config* cfg, ps_handle** out);
 int ps_gpu_destroy(ps_handle* h);
 
@@ -262,7 +265,10 @@ void* ps_gpu_stream(const ps_handle* h);
  * whether an instance's sweeps share launches or run as concurrent launch
  * chains (bit 3).  variant = -1 (the default) times all variants on the
  * handle's own sweeps before its first captured iteration and keeps the
- * fastest; 0..15 forces one.
+ * fastest; 0..15 forces one.  A handle with a branched polymer runs its sweeps
+ * as dependent launch chains (a sweep that starts at a junction waits for the
+ * sweeps arriving there), so it takes only variants with bit 3 (PS_ATTRIB_ERR
+ * otherwise).
  * ps_gpu_get_variant also returns the measured sweep time of each variant (ms). */
 int ps_gpu_set_variant(ps_handle* h, int variant);
 int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune);

@@ -468,3 +468,68 @@ setupPS(16, 16, 1, 0.2, 0.2, 0.2, "'off'")
     pc = cfg.to_ps_config()
     d = pc.polydisperse[0]
     assert (d.enabled, d.poly_block, d.n_g, d.alpha) == (1, 1, 4, 1.5)
+
+
+def test_config_parser_reads_star_polymer():
+    """The reference's three-arm star: every arm's tail lists the two others."""
+    from polyswift_plusplus_b200.config import config_from_text
+    text = """
+setupPS(8, 8, 8, 0.25, 0.25, 0.25, "'off'")
+<EffHamil h>
+  <Updater u>
+    kind = steepestDescent
+    relaxlambdas = [0.1 0.05]
+  </Updater>
+  <Interaction AB>
+    kind = flory
+    chi = 0.15
+    scfields = [A B]
+  </Interaction>
+</EffHamil>
+<PhysField A>
+  kind = monomerDens
+</PhysField>
+<PhysField B>
+  kind = monomerDens
+</PhysField>
+<PhysField C>
+  kind = monomerDens
+</PhysField>
+<PhysField defaultPressure>
+  kind = constraint
+</PhysField>
+<Polymer threeArmABC>
+  kind = blockCopolymer
+  volfrac = 1.0
+  length = 100
+  <Block blockA>
+    kind = flexPseudoSpec
+    scfield = A
+    ds = 0.01
+    lengthfrac = 0.3
+    headjoined = [freeEnd]
+    tailjoined = [blockB blockC]
+  </Block>
+  <Block blockB>
+    kind = flexPseudoSpec
+    scfield = B
+    ds = 0.01
+    lengthfrac = 0.3
+    headjoined = [freeEnd]
+    tailjoined = [blockA blockC]
+  </Block>
+  <Block blockC>
+    kind = flexPseudoSpec
+    scfield = C
+    ds = 0.01
+    lengthfrac = 0.4
+    headjoined = [freeEnd]
+    tailjoined = [blockA blockB]
+  </Block>
+</Polymer>
+"""
+    cfg = config_from_text(text)
+    pc = cfg.to_ps_config()
+    blocks = pc.polymers[0].blocks
+    assert [(b.n_head, b.n_tail) for b in list(blocks)[:3]] == [(0, 2), (0, 2), (0, 2)]
+    assert list(blocks[0].tail_joined[:2]) == [1, 2] and list(blocks[2].tail_joined[:2]) == [0, 1]
