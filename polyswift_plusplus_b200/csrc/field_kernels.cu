@@ -739,11 +739,28 @@ __global__ void __launch_bounds__(kRedThreads)
       const double wk = hist_w[(size_t)cur * nfN + off];
       const double dk = hist_d[(size_t)cur * nfN + off];
       double wh = wk, dhh = dk;
-      for (int a = 1; a <= nh; ++a) {
-        const size_t sa = (size_t)((k - a) % slots);
-        const double ca = sc->am_c[a - 1];
-        wh = wh + ca * (hist_w[sa * nfN + off] - wk);
-        dhh = dhh + ca * (hist_d[sa * nfN + off] - dk);
+      // history terms four at a time: all eight loads in flight before the
+      // (unchanged, sequential) accumulation
+      for (int a0 = 1; a0 <= nh; a0 += 4) {
+        double hw[4], hd[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int a = a0 + j;
+          if (a <= nh) {
+            const size_t sa = (size_t)((k - a) % slots);
+            hw[j] = hist_w[sa * nfN + off];
+            hd[j] = hist_d[sa * nfN + off];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int a = a0 + j;
+          if (a <= nh) {
+            const double ca = sc->am_c[a - 1];
+            wh = wh + ca * (hw[j] - wk);
+            dhh = dhh + ca * (hd[j] - dk);
+          }
+        }
       }
       wn[i] = wh + mix * dhh;
     }
