@@ -611,6 +611,9 @@ cudaError_t launch_am_residual(const FieldModel& fm, const FieldPtrs& fp, double
 
 constexpr int kAmMax = 33;  // depth <= 32
 
+// MAXJ >= m + 1 accumulators: a small depth keeps them in few registers (more
+// blocks per SM); each Gram entry's sum and reduction tree do not depend on MAXJ.
+template <int MAXJ>
 __global__ void __launch_bounds__(kRedThreads)
     am_gram_kernel(long long nfN, const double* __restrict__ hist_d, int slots, int m,
                    const DevScalars* __restrict__ sc, double* __restrict__ gram_partials) {
@@ -618,29 +621,36 @@ __global__ void __launch_bounds__(kRedThreads)
   const int nh = (int)(k < m ? k : m);
   const int cur = (int)(k % slots);
   const double* Dc = hist_d + (size_t)cur * nfN;
-  __shared__ const double* Dj[kAmMax];
-  if (threadIdx.x < kAmMax) {
+  __shared__ const double* Dj[MAXJ];
+  if (threadIdx.x < MAXJ) {
     const int j = threadIdx.x;
     Dj[j] = hist_d + (size_t)((k - (j <= nh ? j : 0)) % slots) * nfN;
   }
   __syncthreads();
-  double acc[kAmMax];
+  double acc[MAXJ];
 #pragma unroll
-  for (int j = 0; j < kAmMax; ++j) acc[j] = 0.0;
+  for (int j = 0; j < MAXJ; ++j) acc[j] = 0.0;
   for (long long t = blockIdx.x * (long long)kRedThreads + threadIdx.x; t < nfN;
        t += (long long)kRedBlocks * kRedThreads) {
     const double d = Dc[t];
 #pragma unroll
-    for (int j = 0; j < kAmMax; ++j)
+    for (int j = 0; j < MAXJ; ++j)
       if (j <= nh) acc[j] += d * Dj[j][t];
   }
-  block_reduce_write<kAmMax>(acc, 0u, gram_partials + (size_t)blockIdx.x * kAmMax);
+  block_reduce_write<MAXJ>(acc, 0u, gram_partials + (size_t)blockIdx.x * kAmMax);
 }
 
 cudaError_t launch_am_gram(long long nfN, const double* hist_d, int slots, int m, DevScalars* sc,
                            double* gram_partials, cudaStream_t st) {
   if (m + 1 > kAmMax) return cudaErrorInvalidValue;
-  am_gram_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(nfN, hist_d, slots, m, sc, gram_partials);
+  if (m + 1 <= 8)
+    am_gram_kernel<8><<<kRedBlocks, kRedThreads, 0, st>>>(nfN, hist_d, slots, m, sc, gram_partials);
+  else if (m + 1 <= 12)
+    am_gram_kernel<12><<<kRedBlocks, kRedThreads, 0, st>>>(nfN, hist_d, slots, m, sc, gram_partials);
+  else if (m + 1 <= 16)
+    am_gram_kernel<16><<<kRedBlocks, kRedThreads, 0, st>>>(nfN, hist_d, slots, m, sc, gram_partials);
+  else
+    am_gram_kernel<kAmMax><<<kRedBlocks, kRedThreads, 0, st>>>(nfN, hist_d, slots, m, sc, gram_partials);
   return cudaGetLastError();
 }
 
