@@ -437,13 +437,28 @@ __device__ __forceinline__ bool int_has(const FieldModel& fm, int it, int f) {
   return fm.int_a[it] == f || fm.int_b[it] == f;
 }
 
+// Per-point field arrays of NF (2 or 3) entries stay in registers: loops over
+// fields are unrolled, and an entry picked by a runtime field index goes
+// through pick().  The arithmetic and its order are those of the reference.
+template <int NF>
+__device__ __forceinline__ double pick(const double (&a)[NF], int i) {
+  double v = a[0];
+#pragma unroll
+  for (int q = 1; q < NF; ++q)
+    if (i == q) v = a[q];
+  return v;
+}
+
 // dH_i = p - w_i + sum_{int ∋ i} chiN (phi_other - avg_other)
 // (pseffhamil/PsSteepDUpdater.cpp:174-184, :208-236; pseffhamil/PsFloryInteraction.cpp:204-269)
+template <int NF>
 __device__ __forceinline__ void compute_dh(const FieldModel& fm, const FieldPtrs& fp, long long r,
-                                           double* dh, double* phi_r) {
+                                           double (&dh)[NF], double (&phi_r)[NF]) {
   const double pr = fp.p[r];
-  for (int i = 0; i < fm.nf; ++i) phi_r[i] = fp.phi[i][r];
-  for (int i = 0; i < fm.nf; ++i) {
+#pragma unroll
+  for (int i = 0; i < NF; ++i) phi_r[i] = fp.phi[i][r];
+#pragma unroll
+  for (int i = 0; i < NF; ++i) {
     double d = 0.0;
     d = d + pr;
     d = d - fp.w[i][r];
@@ -452,7 +467,7 @@ __device__ __forceinline__ void compute_dh(const FieldModel& fm, const FieldPtrs
       const int other = (i == fm.int_a[it]) ? fm.int_b[it] : fm.int_a[it];
       const double mask = -1.0 * fm.dens_avg[other];
       double x = 0.0;
-      x = x + phi_r[other];
+      x = x + pick(phi_r, other);
       x = x + mask;
       x = x * fm.chin[it];
       d = d + x;
@@ -462,10 +477,13 @@ __device__ __forceinline__ void compute_dh(const FieldModel& fm, const FieldPtrs
 }
 
 // SD direction: dH_i - lambda1 * sum_{j != i} dH_j (pseffhamil/PsSteepDUpdater.cpp:264-278, :368-393)
-__device__ __forceinline__ void sd_direction(const FieldModel& fm, const double* dh, double* dir) {
-  for (int i = 0; i < fm.nf; ++i) {
+template <int NF>
+__device__ __forceinline__ void sd_direction(const FieldModel& fm, const double (&dh)[NF], double (&dir)[NF]) {
+#pragma unroll
+  for (int i = 0; i < NF; ++i) {
     double x = 0.0;
-    for (int j = 0; j < fm.nf; ++j)
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
       if (j != i) x = x + dh[j];
     x = x * (-1.0 * fm.lambda1);
     x = x + dh[i];
@@ -476,20 +494,24 @@ __device__ __forceinline__ void sd_direction(const FieldModel& fm, const double*
 // Noise, pressure rebuild (pseffhamil/PsSteepDUpdater.cpp:283-332, :398-452) and
 // the free-energy density (pseffhamil/PsPolymerUpdater.cpp:172-226, 302-341;
 // pseffhamil/PsFloryInteraction.cpp:274-321) at one point, given the new w.
+template <int NF>
 __device__ __forceinline__ void finish_point(const FieldModel& fm, const FieldPtrs& fp,
-                                             long long r, double* wn, const double* phi_r,
+                                             long long r, double (&wn)[NF], const double (&phi_r)[NF],
                                              double& psum, double& fe, double& fe_nd) {
   if (fp.noise) {
-    for (int i = 0; i < fm.nf; ++i) {
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
       double v = 0.0 + fp.noise[(size_t)i * fm.N + r];
       v = v * 1.0;
       wn[i] = wn[i] + v;
     }
   }
-  for (int i = 0; i < fm.nf; ++i) fp.w[i][r] = wn[i];
+#pragma unroll
+  for (int i = 0; i < NF; ++i) fp.w[i][r] = wn[i];
   double pr = 0.0;
-  for (int i = 0; i < fm.nf; ++i) pr = pr + wn[i];
-  if (fm.nf == 2) {
+#pragma unroll
+  for (int i = 0; i < NF; ++i) pr = pr + wn[i];
+  if (NF == 2) {
     for (int it = 0; it < fm.n_int; ++it) {
       if (int_has(fm, it, 0) && int_has(fm, it, 1)) {
         double x = 0.0;
@@ -500,7 +522,8 @@ __device__ __forceinline__ void finish_point(const FieldModel& fm, const FieldPt
     pr = 0.5 * pr;
   } else {
     for (int it = 0; it < fm.n_int; ++it) {
-      for (int n = 0; n < fm.nf; ++n) {
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
         if (int_has(fm, it, n)) continue;
         double x = 0.0;
         x = x + (phi_r[n] - fm.dens_avg[n]);
@@ -516,7 +539,8 @@ __device__ __forceinline__ void finish_point(const FieldModel& fm, const FieldPt
   psum += pr;
   const double inv_vol = 1.0 / (double)fm.N;
   double f = 0.0;
-  for (int i = 0; i < fm.nf; ++i) {
+#pragma unroll
+  for (int i = 0; i < NF; ++i) {
     double prod = (0.0 + phi_r[i]) * wn[i];
     prod = -1.0 * prod;
     f = f + prod;
@@ -528,7 +552,7 @@ __device__ __forceinline__ void finish_point(const FieldModel& fm, const FieldPt
     const double a0 = fm.dens_avg[fm.int_a[it]], a1 = fm.dens_avg[fm.int_b[it]];
     double dis = (((0.0 + 1.0) * 1.0) * a0) * a1;
     dis = dis * fm.chin[it];
-    double v = (0.0 + phi_r[fm.int_a[it]]) * phi_r[fm.int_b[it]];
+    double v = (0.0 + pick(phi_r, fm.int_a[it])) * pick(phi_r, fm.int_b[it]);
     v = v * fm.chin[it];
     const double vd = v - dis;
     ft = ft + inv_vol * vd;
@@ -538,34 +562,42 @@ __device__ __forceinline__ void finish_point(const FieldModel& fm, const FieldPt
   fe_nd += ftn;
 }
 
-__device__ __forceinline__ double incomp(const FieldModel& fm, const double* phi_r) {
+template <int NF>
+__device__ __forceinline__ double incomp(const double (&phi_r)[NF]) {
   double t = 0.0;
-  for (int i = 0; i < fm.nf; ++i) t += phi_r[i];
+#pragma unroll
+  for (int i = 0; i < NF; ++i) t += phi_r[i];
   return fabs(t - 1.0);
 }
 
+template <int NF>
 __global__ void __launch_bounds__(kRedThreads)
     sd_update_kernel(FieldModel fm, FieldPtrs fp, double* __restrict__ partials) {
   double acc[kUpdQ] = {0, 0, 0, 0, 0, 0};
   for (long long r = blockIdx.x * (long long)kRedThreads + threadIdx.x; r < fm.N;
        r += (long long)kRedBlocks * kRedThreads) {
-    double dh[PS_MAX_FIELDS], phi_r[PS_MAX_FIELDS], dir[PS_MAX_FIELDS], wn[PS_MAX_FIELDS];
-    compute_dh(fm, fp, r, dh, phi_r);
-    for (int i = 0; i < fm.nf; ++i) acc[3] += dh[i] * dh[i];
-    acc[4] = fmax(acc[4], incomp(fm, phi_r));
-    sd_direction(fm, dh, dir);
-    for (int i = 0; i < fm.nf; ++i) {
+    double dh[NF], phi_r[NF], dir[NF], wn[NF];
+    compute_dh<NF>(fm, fp, r, dh, phi_r);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) acc[3] += dh[i] * dh[i];
+    acc[4] = fmax(acc[4], incomp<NF>(phi_r));
+    sd_direction<NF>(fm, dh, dir);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
       const double x = dir[i] * fm.lambda0;
       wn[i] = fp.w[i][r] + x;
     }
-    finish_point(fm, fp, r, wn, phi_r, acc[0], acc[1], acc[2]);
+    finish_point<NF>(fm, fp, r, wn, phi_r, acc[0], acc[1], acc[2]);
   }
   block_reduce_write<kUpdQ>(acc, 1u << 4, partials + (size_t)blockIdx.x * kUpdQ);
 }
 
 cudaError_t launch_sd_update(const FieldModel& fm, const FieldPtrs& fp, double* partials,
                              cudaStream_t st) {
-  sd_update_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, partials);
+  if (fm.nf == 3)
+    sd_update_kernel<3><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, partials);
+  else
+    sd_update_kernel<2><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, partials);
   return cudaGetLastError();
 }
 
@@ -573,6 +605,7 @@ cudaError_t launch_sd_update(const FieldModel& fm, const FieldPtrs& fp, double* 
 // Anderson mixing (no reference counterpart): history of (w, D) with
 // D = steepest-descent direction; Gram-matrix normal equations in FP64.
 // ---------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kRedThreads)
     am_residual_kernel(FieldModel fm, FieldPtrs fp, double* __restrict__ hist_w,
                        double* __restrict__ hist_d, int slots, const DevScalars* __restrict__ sc,
@@ -584,12 +617,14 @@ __global__ void __launch_bounds__(kRedThreads)
   double acc[2] = {0.0, 0.0};
   for (long long r = blockIdx.x * (long long)kRedThreads + threadIdx.x; r < fm.N;
        r += (long long)kRedBlocks * kRedThreads) {
-    double dh[PS_MAX_FIELDS], phi_r[PS_MAX_FIELDS], dir[PS_MAX_FIELDS];
-    compute_dh(fm, fp, r, dh, phi_r);
-    for (int i = 0; i < fm.nf; ++i) acc[0] += dh[i] * dh[i];
-    acc[1] = fmax(acc[1], incomp(fm, phi_r));
-    sd_direction(fm, dh, dir);
-    for (int i = 0; i < fm.nf; ++i) {
+    double dh[NF], phi_r[NF], dir[NF];
+    compute_dh<NF>(fm, fp, r, dh, phi_r);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) acc[0] += dh[i] * dh[i];
+    acc[1] = fmax(acc[1], incomp<NF>(phi_r));
+    sd_direction<NF>(fm, dh, dir);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
       Wc[(size_t)i * fm.N + r] = fp.w[i][r];
       Dc[(size_t)i * fm.N + r] = dir[i];
     }
@@ -605,7 +640,10 @@ __global__ void __launch_bounds__(kRedThreads)
 cudaError_t launch_am_residual(const FieldModel& fm, const FieldPtrs& fp, double* hist_w,
                                double* hist_d, int slots, DevScalars* sc, double* partials,
                                cudaStream_t st) {
-  am_residual_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
+  if (fm.nf == 3)
+    am_residual_kernel<3><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
+  else
+    am_residual_kernel<2><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
   return cudaGetLastError();
 }
 
@@ -730,6 +768,7 @@ cudaError_t launch_am_solve(const double* gram_partials, double* gram, int slots
   return cudaGetLastError();
 }
 
+template <int NF>
 __global__ void __launch_bounds__(kRedThreads)
     am_mix_kernel(FieldModel fm, FieldPtrs fp, const double* __restrict__ hist_w,
                   const double* __restrict__ hist_d, int slots, const DevScalars* __restrict__ sc,
@@ -742,9 +781,11 @@ __global__ void __launch_bounds__(kRedThreads)
   double acc[3] = {0.0, 0.0, 0.0};
   for (long long r = blockIdx.x * (long long)kRedThreads + threadIdx.x; r < fm.N;
        r += (long long)kRedBlocks * kRedThreads) {
-    double wn[PS_MAX_FIELDS], phi_r[PS_MAX_FIELDS];
-    for (int i = 0; i < fm.nf; ++i) phi_r[i] = fp.phi[i][r];
-    for (int i = 0; i < fm.nf; ++i) {
+    double wn[NF], phi_r[NF];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) phi_r[i] = fp.phi[i][r];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
       const size_t off = (size_t)i * fm.N + r;
       const double wk = hist_w[(size_t)cur * nfN + off];
       const double dk = hist_d[(size_t)cur * nfN + off];
@@ -774,7 +815,7 @@ __global__ void __launch_bounds__(kRedThreads)
       }
       wn[i] = wh + mix * dhh;
     }
-    finish_point(fm, fp, r, wn, phi_r, acc[0], acc[1], acc[2]);
+    finish_point<NF>(fm, fp, r, wn, phi_r, acc[0], acc[1], acc[2]);
   }
   double out[3];
   block_reduce_write<3>(acc, 0u, out);
@@ -786,7 +827,10 @@ __global__ void __launch_bounds__(kRedThreads)
 cudaError_t launch_am_mix(const FieldModel& fm, const FieldPtrs& fp, const double* hist_w,
                           const double* hist_d, int slots, DevScalars* sc, double* partials,
                           cudaStream_t st) {
-  am_mix_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
+  if (fm.nf == 3)
+    am_mix_kernel<3><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
+  else
+    am_mix_kernel<2><<<kRedBlocks, kRedThreads, 0, st>>>(fm, fp, hist_w, hist_d, slots, sc, partials);
   return cudaGetLastError();
 }
 
