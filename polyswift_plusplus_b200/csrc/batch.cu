@@ -256,7 +256,7 @@ static int batch_create(ps_batch* b, const ps_config* cfgs, int count) {
   for (int i = 0; i < count; ++i) {
     if (cfgs[i].updater.noise != 0.0) {
       b->err = "instance " + std::to_string(i) +
-               ": noise must be 0 in a batch (its draws are made on the host every iteration)";
+               ": noise must be 0 in a batch";
       return PS_ATTRIB_ERR;
     }
     if (cfgs[i].device != cfgs[0].device) {

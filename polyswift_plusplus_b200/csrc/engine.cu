@@ -426,7 +426,10 @@ template <typename T> static int launch_post(ps_handle* h, long long* nlaunch);
 
 template <typename T>
 static int launch_iteration(ps_handle* h, long long* nlaunch) {
-  int rc = launch_pre<T>(h, nlaunch);
+  // this iteration's updater noise, drawn beside the sweeps
+  int rc = noise_launch(h, nlaunch);
+  if (rc) return rc;
+  rc = launch_pre<T>(h, nlaunch);
   if (rc) return rc;
   // cudaEventRecordExternal: inside stream capture this becomes an event-record
   // node of the graph (a plain record would only order the capture).
@@ -492,6 +495,10 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
   }
   fp.p = h->d_p;
   fp.noise = (h->cfg.updater.noise != 0.0) ? h->d_noise : nullptr;
+  if (fp.noise) {
+    int rc = noise_join(h);
+    if (rc) return rc;
+  }
   if (h->cfg.updater.kind == PS_UPD_ANDERSON) {
     const int m = h->cfg.updater.anderson_depth;
     PS_CUDA(h, launch_am_residual(h->fm, fp, h->d_hw, h->d_hd, h->am_slots, h->d_sc, h->d_upart, h->st));
@@ -566,28 +573,29 @@ int engine_post(ps_handle* h, long long* nlaunch) {
   return (h->prec == PS_PREC_MIXED) ? launch_post<float>(h, nlaunch) : launch_post<double>(h, nlaunch);
 }
 
-// Gaussian draws the reference makes every iteration even at noise = 0
-// (pseffhamil/PsPolymerUpdater.cpp:263-295); they are owed to the stream and
-// drawn lazily before anything else reads it.
-static void settle_rng(ps_handle* h) {
+// Bring the host generator up to date before the host reads it: take back the
+// state of device draws, then make the Gaussian draws the reference makes every
+// iteration even at noise = 0 (pseffhamil/PsPolymerUpdater.cpp:263-295), which
+// are owed to the stream and drawn lazily.
+static int settle_rng(ps_handle* h) {
+  int rc = noise_download(h);
+  if (rc) return rc;
   while (h->pending_gauss > 0) {
     (void)h->rng.gauss();
     --h->pending_gauss;
   }
+  return PS_OK;
 }
 
 int engine_prepare_noise(ps_handle* h) {
-  const double s = h->cfg.updater.noise;
-  if (s == 0.0) {
+  if (h->cfg.updater.noise == 0.0) {
     h->pending_gauss += (long long)h->nf * h->N;
     return PS_OK;
   }
-  settle_rng(h);
-  const long long n = (long long)h->nf * h->N;
-  for (long long i = 0; i < n; ++i) h->h_noise[i] = s * h->rng.gauss();
-  PS_CUDA(h, cudaMemcpyAsync(h->d_noise, h->h_noise, sizeof(double) * (size_t)n,
-                             cudaMemcpyHostToDevice, h->st));
-  return PS_OK;
+  // the draws themselves are kernels of the iteration (noise_launch)
+  int rc = settle_rng(h);
+  if (rc) return rc;
+  return noise_upload(h);
 }
 
 template <typename T> static void free_buffers(Buffers<T>& B) {
@@ -603,13 +611,13 @@ template <typename T> static void free_buffers(Buffers<T>& B) {
 }
 
 static void free_all(ps_handle* h) {
+  noise_free(h);
   filter_free(h);
   poisson_free(h);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(h->d_w); f(h->d_phi); f(h->d_p); f(h->d_noise); f(h->d_rho); f(h->d_psi);
-  if (h->h_noise) cudaFreeHost(h->h_noise);
   free_buffers(h->bf);
   free_buffers(h->bd);
   f(h->d_qpart); f(h->d_upart); f(h->d_sc);
@@ -966,7 +974,8 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
   }
   if (c.updater.noise != 0.0) {
     PS_CUDA(h, cudaMalloc((void**)&h->d_noise, sizeof(double) * nfN));
-    PS_CUDA(h, cudaMallocHost((void**)&h->h_noise, sizeof(double) * nfN));
+    int rn = noise_setup(h);
+    if (rn) return rn;
   }
   PS_CUDA(h, cudaMalloc((void**)&h->d_qpart, sizeof(double) * kRedBlocks));
   PS_CUDA(h, cudaMalloc((void**)&h->d_upart, sizeof(double) * kRedBlocks * kUpdQ));
@@ -997,6 +1006,8 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
 int engine_check_scalars(ps_handle* h) {
   PS_CUDA(h, cudaMemcpyAsync(h->h_sc, h->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
+  int rn = noise_check(h);
+  if (rn) return rn;
   if (h->h_sc->error_flags & 1) {
     h->err = "PsBlock::calcBigQ() found nan/inf?";
     return PS_RUN_ERR;
@@ -1014,12 +1025,11 @@ int engine_check_scalars(ps_handle* h) {
 
 static int iterate_impl(ps_handle* h, int n) {
   PS_CUDA(h, cudaSetDevice(h->dev));
-  const bool use_graph = (h->cfg.updater.noise == 0.0);
   for (int it = 0; it < n; ++it) {
     int rc = engine_prepare_noise(h);
     if (rc) return rc;
     const bool sample = h->timing_cap > 0 && h->timing_count < h->timing_cap;
-    if (!use_graph || h->eager_iters < 1) {
+    if (h->eager_iters < 1) {
       long long nl = 0;
       rc = run_iteration(h, &nl);
       if (rc) return rc;
@@ -1209,9 +1219,10 @@ int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_d
 
 int ps_gpu_init_random(ps_handle* h) {
   if (!h) return PS_ATTRIB_ERR;
-  settle_rng(h);
-  std::vector<double> buf((size_t)h->N);
   PS_CUDA(h, cudaSetDevice(h->dev));
+  int rc = settle_rng(h);
+  if (rc) return rc;
+  std::vector<double> buf((size_t)h->N);
   for (int i = 0; i < h->nf; ++i) {
     for (long long r = 0; r < h->N; ++r) {
       const double u = h->rng.real();

@@ -98,8 +98,8 @@ struct ps_handle {
   double* d_w = nullptr;    // nf*N
   double* d_phi = nullptr;  // nf*N
   double* d_p = nullptr;
-  double* d_noise = nullptr;
-  double* h_noise = nullptr;  // pinned
+  double* d_noise = nullptr;  // nf*N scaled Gaussians of the current iteration
+  void* noise_gen = nullptr;   // device generator of d_noise (noise.cu), or nullptr
   int nq = 0;                 // chargeDens PhysFields
   double* d_rho = nullptr;    // nq*N charge densities
   double* d_psi = nullptr;    // nq*N electric potentials
@@ -203,6 +203,17 @@ int engine_pre(ps_handle* h, long long* nlaunch);
 int engine_post(ps_handle* h, long long* nlaunch);
 // Host-side random-number bookkeeping owed before each iteration.
 int engine_prepare_noise(ps_handle* h);
+// Updater noise drawn on the device (noise.cu).  noise_launch forks the draws of
+// one iteration off h->st and noise_join joins them back (both legal in stream
+// capture); noise_upload / noise_download move the MT19937 state between the
+// host generator and the device.
+int noise_setup(ps_handle* h);
+void noise_free(ps_handle* h);
+int noise_upload(ps_handle* h);
+int noise_download(ps_handle* h);
+int noise_launch(ps_handle* h, long long* nlaunch);
+int noise_join(ps_handle* h);
+int noise_check(ps_handle* h);
 // Copy the device scalars back and turn error flags into status codes.
 int engine_check_scalars(ps_handle* h);
 

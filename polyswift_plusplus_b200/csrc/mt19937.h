@@ -55,6 +55,20 @@ class Mt19937 {
     return gauss_;
   }
 
+  // The whole generator state, e.g. to continue the stream on the device.
+  void get_state(uint32_t* mt, int* idx, bool* have_gauss, double* gauss) const {
+    for (int k = 0; k < 624; ++k) mt[k] = mt_[k];
+    *idx = idx_;
+    *have_gauss = have_gauss_;
+    *gauss = gauss_;
+  }
+  void set_state(const uint32_t* mt, int idx, bool have_gauss, double gauss) {
+    for (int k = 0; k < 624; ++k) mt_[k] = mt[k];
+    idx_ = idx;
+    have_gauss_ = have_gauss;
+    gauss_ = gauss;
+  }
+
  private:
   void refill_() {
     for (int k = 0; k < 624; ++k) {

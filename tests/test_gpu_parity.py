@@ -249,6 +249,53 @@ def test_reference_random_init_and_noise(gpu, oracle_lib):
         assert rel(g.w(i), o.w(i)) < TOL64
 
 
+@pytest.mark.parametrize("case", ["diblock_sd_fp64", "diblock_am_fp64", "diblock_sd_mixed",
+                                  "star_abc_fp64"])
+def test_device_noise_follows_the_host_stream(gpu, oracle_lib, case):
+    """Updater noise is drawn on the device from the MT19937 stream the host
+    generator continues: after noisy iterations (the first eager, the rest
+    graph replays) the fields follow the oracle, and a random initialisation
+    drawn afterwards is bit-identical, so the device left the stream at exactly
+    the oracle's position."""
+    if case == "diblock_sd_fp64":
+        cfg, _ = W.diblock32(n=16)
+        iters, tol = 7, TOL64
+    elif case == "diblock_am_fp64":
+        # Anderson's Gram entries cancel: 1e-6 as in the noiseless trajectory test
+        cfg, _ = W.diblock32(n=16)
+        cfg.updater = Updater(kind="andersonMixing", relaxlambdas=(0.1, 0.05), anderson_depth=4,
+                              anderson_mix=0.1, anderson_start=2)
+        iters, tol = 6, 1e-6
+    elif case == "diblock_sd_mixed":
+        # FP32 sweeps: the fields follow the FP64 oracle to about 1e-5
+        cfg, _ = W.diblock32(n=32, precision="mixed")
+        iters, tol = 5, 1e-4
+    else:
+        cfg, _ = W.star_abc(n=16)
+        iters, tol = 4, TOL64
+    cfg.updater.noise = 0.01
+    g = ScftSolver(cfg)
+    o = O.Oracle(cfg)
+    g.initialize()
+    o.initialize()
+    ho = o.update(iters)
+    g.update(iters)
+    hg = g.scalars()
+    assert hg["iteration"] == iters
+    assert abs(hg["free_energy"] - ho[-1]["free_energy"]) <= tol * max(abs(ho[-1]["free_energy"]), 1.0)
+    for i in range(g.nf):
+        assert rel(g.w(i), o.w(i)) < tol
+    g.initialize()
+    o.initialize()
+    for i in range(g.nf):
+        assert np.array_equal(g.w(i), o.w(i))
+    # and the stream carries on from there on the device
+    ho = o.update(2)
+    g.update(2)
+    for i in range(g.nf):
+        assert rel(g.w(i), o.w(i)) < tol
+
+
 def test_mixed_precision_close_to_fp64_at_convergence(gpu):
     """Mixed (FP32 sweeps) against FP64 at a converged state of a 32^3, Ns = 100
     diblock.  F is stationary in w and phi at the saddle point, but -ln Q enters
