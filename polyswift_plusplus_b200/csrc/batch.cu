@@ -144,7 +144,9 @@ static int launch_batch_iteration(ps_batch* b, long long* nl) {
   for (size_t i = 0; i < b->inst.size(); ++i) {
     ps_handle* h = b->inst[i];
     PB_CUDA(b, cudaStreamWaitEvent(h->st, b->ev_fork, 0));
-    int rc = engine_pre(h, nl);
+    int rc = noise_launch(h, nl);  // the instance's updater noise, if any
+    if (rc) return instance_error(b, (int)i, rc);
+    rc = engine_pre(h, nl);
     if (rc) return instance_error(b, (int)i, rc);
     PB_CUDA(b, cudaEventRecord(b->ev_inst[i], h->st));
   }
@@ -254,11 +256,6 @@ static void batch_free(ps_batch* b) {
 
 static int batch_create(ps_batch* b, const ps_config* cfgs, int count) {
   for (int i = 0; i < count; ++i) {
-    if (cfgs[i].updater.noise != 0.0) {
-      b->err = "instance " + std::to_string(i) +
-               ": noise must be 0 in a batch";
-      return PS_ATTRIB_ERR;
-    }
     if (cfgs[i].device != cfgs[0].device) {
       b->err = "all instances of a batch must be on the same device";
       return PS_ATTRIB_ERR;

@@ -592,9 +592,13 @@ int engine_prepare_noise(ps_handle* h) {
     h->pending_gauss += (long long)h->nf * h->N;
     return PS_OK;
   }
-  // the draws themselves are kernels of the iteration (noise_launch)
-  int rc = settle_rng(h);
-  if (rc) return rc;
+  // The draws themselves are kernels of the iteration (noise_launch).  The
+  // generator moves to the device once and stays there until the host draws
+  // again, so no iteration waits on the host.
+  if (h->pending_gauss > 0) {
+    int rc = settle_rng(h);
+    if (rc) return rc;
+  }
   return noise_upload(h);
 }
 

@@ -321,7 +321,9 @@ int noise_upload(ps_handle* h) {
   return PS_OK;
 }
 
-// Bring the host generator up to date after device draws.
+// Bring the host generator up to date after device draws.  Every iterate call
+// (alone or in a batch) returns with its work finished, so the stored state is
+// the last iteration's.
 int noise_download(ps_handle* h) {
   NoiseState* n = static_cast<NoiseState*>(h->noise_gen);
   if (!n || !n->on_device) return PS_OK;
