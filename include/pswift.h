@@ -261,11 +261,13 @@ void* ps_gpu_stream(const ps_handle* h);
 
 /* Kernel variant of the propagator sweeps (no reference counterpart).  Every
  * variant computes the same result; they differ in how passes are fused
- * (bits 0, 1), in the FFT decomposition (bit 2: row + x-y planes) and in
- * whether an instance's sweeps share launches or run as concurrent launch
- * chains (bit 3).  variant = -1 (the default) times all variants on the
- * handle's own sweeps before its first captured iteration and keeps the
- * fastest; 0..15 forces one.  A handle with a branched polymer runs its sweeps
+ * (bits 0, 1), in the FFT decomposition (bit 2: row + x-y planes; bit 4:
+ * 256 x 256 y-z planes on a cluster of two CTAs instead of a row pass and y
+ * pencils, FP32 sweeps only, PS_ATTRIB_ERR elsewhere) and in whether an
+ * instance's sweeps share launches or run as concurrent launch chains
+ * (bit 3).  variant = -1 (the default) times all variants on the handle's
+ * own sweeps before its first captured iteration and keeps the fastest;
+ * 0..31 forces one.  A handle with a branched polymer runs its sweeps
  * as dependent launch chains (a sweep that starts at a junction waits for the
  * sweeps arriving there), so it takes only variants with bit 3 (PS_ATTRIB_ERR
  * otherwise).

@@ -531,6 +531,7 @@ static int autotune_t(ps_handle* h) {
   for (int v = 0; v < VARIANT_COUNT && e == cudaSuccess && rc == PS_OK; ++v) {
     h->tune_ms[v] = -1.f;
     if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
+    if ((v & VARIANT_CLUSTER) && (!h->cluster_ok || (v & VARIANT_XY))) continue;
     if ((v & VARIANT_SPLIT) && h->sw_st.empty()) continue;                 // one sweep only
     if (!(v & VARIANT_SPLIT) && h->branched) continue;                     // chains only
     long long nl = 0;
@@ -962,6 +963,7 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
   const int pb = (h->prec == PS_PREC_MIXED) ? 4 : 8;
   h->fused_plane = plane_fused_supported(pb, c.n[1], c.n[2]);
   h->xy_ok = xy_supported(pb, c.n[0], c.n[1], c.n[2]);
+  h->cluster_ok = !h->fused_plane && cluster_plane_supported(pb, c.n[1], c.n[2]);
   const size_t nfN = (size_t)h->nf * h->N;
   PS_CUDA(h, cudaMalloc((void**)&h->d_w, sizeof(double) * nfN));
   PS_CUDA(h, cudaMalloc((void**)&h->d_phi, sizeof(double) * nfN));
@@ -1322,6 +1324,10 @@ int ps_gpu_set_variant(ps_handle* h, int variant) {
     h->err = "the row + x-y plane design does not exist for this grid";
     return PS_ATTRIB_ERR;
   }
+  if (variant >= 0 && (variant & VARIANT_CLUSTER) && !h->cluster_ok) {
+    h->err = "the cluster plane pass exists for FP32 sweeps of 256 x 256 y-z planes only";
+    return PS_ATTRIB_ERR;
+  }
   if (variant >= 0 && !(variant & VARIANT_SPLIT) && h->branched) {
     h->err = "a branched polymer's sweeps run as dependent launch chains: set variant bit 8";
     return PS_ATTRIB_ERR;
@@ -1369,6 +1375,7 @@ int ps_gpu_set_precision(ps_handle* h, int precision) {
   const int pb = (precision == PS_PREC_MIXED) ? 4 : 8;
   h->fused_plane = plane_fused_supported(pb, h->n[1], h->n[2]);
   h->xy_ok = xy_supported(pb, h->n[0], h->n[1], h->n[2]);
+  h->cluster_ok = !h->fused_plane && cluster_plane_supported(pb, h->n[1], h->n[2]);
   h->sweep_bytes = 3.0 * (double)h->N * (double)pb * (double)h->sweep_steps;
   h->variant = -1;
   h->eager_iters = 0;

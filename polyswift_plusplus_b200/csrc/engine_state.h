@@ -143,6 +143,7 @@ struct ps_handle {
   int variant = -1;  // kernel variant (VARIANT_* bits); -1: autotune before the graph is built
   float tune_ms[psb::VARIANT_COUNT] = {};
   bool xy_ok = false;  // the row + x-y plane design exists for this grid
+  bool cluster_ok = false;  // the two-CTA cluster plane pass exists for this grid and precision
   bool in_batch = false;  // owned by a ps_batch, whose merged work tables point into it
   bool branched = false;  // a branched polymer: its sweeps run as dependent launch chains only
   int n_jbuf = 0;

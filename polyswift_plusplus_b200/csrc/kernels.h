@@ -47,7 +47,21 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // bit 3: each sweep of an instance runs as its own chain of launches on its
 // own stream (parallel graph branches) instead of all sweeps in lockstep in
 // shared launches; single-instance engine only (kernels ignore the bit).
-enum { VARIANT_FUSE_Z = 1, VARIANT_FUSE_K = 2, VARIANT_XY = 4, VARIANT_SPLIT = 8, VARIANT_COUNT = 16 };
+// bit 4: FP32 256 x 256 y-z planes (too large for one CTA) run as one plane
+// pass on a cluster of two CTAs instead of a row pass and two y pencil passes
+// (cluster_plane_supported); elsewhere the bit changes nothing.
+enum {
+  VARIANT_FUSE_Z = 1,
+  VARIANT_FUSE_K = 2,
+  VARIANT_XY = 4,
+  VARIANT_SPLIT = 8,
+  VARIANT_CLUSTER = 16,
+  VARIANT_COUNT = 32
+};
+bool cluster_plane_supported(int prec_bytes, int ny, int nz);
+// The two-CTA cluster plane pass (FP32, ny = nz = 256): grid 2 nx x nworks.
+cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, int nx, const float2* tw_y,
+                                 const float2* tw_zh, const float2* tw_z, cudaStream_t st);
 
 // The x-y plane design exists for this grid (square x-y planes that fit in
 // shared memory).

@@ -829,6 +829,221 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz) {
   return bytes <= 200 * 1024;
 }
 
+// ---------------------------------------------------------------------------
+// Plane pass of FP32 256 x 256 y-z planes on a cluster of two CTAs
+// (VARIANT_CLUSTER).  A 256 x 129 half plane (264 KB) does not fit one CTA's
+// shared memory; split over two it does, and the step needs no y pencil passes
+// (two fewer spectrum round trips).  CTA c holds:
+//   y phases: kz columns [64c, 64c + 64) for all y (CTA 0 also kz = 128, which
+//             shares the kz = 0 transform), layout Y[y][slot], 65 slots a row;
+//   z phases: y rows [128c, 128c + 128) for all kz, layout Z[r][kz], 129 a row.
+// Between the phases every thread reads its elements into registers, a cluster
+// barrier makes sure both CTAs have read their buffers, the elements are
+// written to their place in the other layout (this CTA's or the peer's shared
+// memory), and a second cluster barrier publishes them.  Both CTAs of a
+// cluster work on the same plane and mode, so they take the same barriers; no
+// shared memory is touched across the cluster after the last one.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Shared-memory address of the same variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t peer_smem(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_peer(uint32_t addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+
+struct PlaneC256 {
+  static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128, TH = 512;
+  static constexpr int CH = 64;           // y-FFT columns per CTA
+  static constexpr int YS = CH + 1;       // Y row stride (slot CH: kz = 128 in CTA 0)
+  static constexpr int RH = NY / 2;       // z rows per CTA
+  static constexpr int YE = NY * YS;      // 16640
+  static constexpr int ZE = RH * NZH;     // 16512
+  static constexpr int BUF = (YE > ZE) ? YE : ZE;
+  static constexpr int UY = NY * CH / TH;            // 32 Y elements per thread (+1 slot-CH element)
+  static constexpr int UZ = (ZE + TH - 1) / TH;      // 33 Z elements per thread
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)BUF + H + NZ + NY);
+};
+
+__global__ void __launch_bounds__(PlaneC256::TH, 1)
+    plane_c256_kernel(const PlaneWork<float>* __restrict__ works, const float2* __restrict__ tw_y,
+                      const float2* __restrict__ tw_zh, const float2* __restrict__ tw_z) {
+  using P = PlaneC256;
+  using T = float;
+  using C = float2;
+  constexpr int NY = P::NY, NZ = P::NZ, NZH = P::NZH, H = P::H, TH = P::TH, CH = P::CH, YS = P::YS,
+                RH = P::RH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* s_tw_zh = buf + P::BUF;
+  C* s_tw_z = s_tw_zh + H;
+  C* s_tw_y = s_tw_z + NZ;
+
+  const uint32_t me = cluster_ctarank();
+  const uint32_t peer = me ^ 1u;
+  const PlaneWork<T> w = works[blockIdx.y];
+  const int x = blockIdx.x >> 1;
+  const int tid = threadIdx.x;
+  const size_t soff = (size_t)x * NY * NZH;
+  const int row0 = (int)me * RH, prow0 = (int)peer * RH;
+  const int col0 = (int)me * CH;
+  const size_t roff = ((size_t)x * NY + row0) * NZ;
+  const uint32_t pbase = peer_smem(buf, peer);
+  for (int i = tid; i < H; i += TH) s_tw_zh[i] = tw_zh[i];
+  for (int i = tid; i < NZ; i += TH) s_tw_z[i] = tw_z[i];
+  for (int i = tid; i < NY; i += TH) s_tw_y[i] = tw_y[i];
+  pdl_wait();  // before any read of the spectrum, src or wfac, and any write
+
+  if (w.mode != MODE_FIRST) {
+    // this CTA's columns of the half plane, Y layout
+    const C* src = w.spec + soff;
+    for (int e = tid; e < NY * CH; e += TH) {
+      const int y = e / CH, c = e - (e / CH) * CH;
+      buf[y * YS + c] = src[(size_t)y * NZH + col0 + c];
+    }
+    if (me == 0)
+      for (int y = tid; y < NY; y += TH) buf[y * YS + CH] = src[(size_t)y * NZH + NZ / 2];
+    __syncthreads();
+    // inverse y FFT of the columns (plane_y_inverse on this CTA's part)
+    if (me == 0) {
+      for (int y = tid; y < NY; y += TH) {
+        const C a = buf[y * YS], b = buf[y * YS + CH];
+        buf[y * YS] = C{a.x - b.y, a.y + b.x};
+      }
+    }
+    __syncthreads();
+    smem_fft<NY, CH, TH, true, true, C, typename PlanY<NY>::type>(buf, 1, YS, s_tw_y);
+    if (me == 0) {
+      for (int y = tid; y < NY; y += TH) {
+        const C c = buf[y * YS];
+        buf[y * YS] = C{c.x, 0.f};
+        buf[y * YS + CH] = C{c.y, 0.f};
+      }
+    }
+    __syncthreads();
+    // Y -> Z: element (y, kz) goes to row y - row0 here or y - prow0 in the peer
+    C v[P::UY];
+    C vx = C{0.f, 0.f};
+#pragma unroll
+    for (int u = 0; u < P::UY; ++u) {
+      const int e = tid + u * TH;
+      v[u] = buf[(e / CH) * YS + (e % CH)];
+    }
+    if (me == 0 && tid < NY) vx = buf[tid * YS + CH];
+    cluster_sync_all();  // both buffers read
+#pragma unroll
+    for (int u = 0; u < P::UY; ++u) {
+      const int e = tid + u * TH;
+      const int y = e / CH, kz = col0 + (e % CH);
+      if (y >= row0 && y < row0 + RH)  // uniform in u: y = tid / 64 + 8 u
+        buf[(y - row0) * NZH + kz] = v[u];
+      else
+        st_peer(pbase + 8u * (uint32_t)((y - prow0) * NZH + kz), v[u]);
+    }
+    if (me == 0 && tid < NY) {
+      const int y = tid;
+      if (y < row0 + RH) buf[(y - row0) * NZH + NZ / 2] = vx;
+      else st_peer(pbase + 8u * (uint32_t)((y - prow0) * NZH + NZ / 2), vx);
+    }
+    cluster_sync_all();  // both Z layouts complete
+    c2r_pre<NZ, RH, TH>(buf, s_tw_z, RH);
+    __syncthreads();
+    smem_fft<H, RH, TH, true, true>(buf, NZH, 1, s_tw_zh);
+  }
+  real_space<T, RH, NZ, TH>(w, reinterpret_cast<T*>(buf), roff, RH);
+  if (w.mode == MODE_LAST) return;  // uniform over the cluster
+  __syncthreads();
+  smem_fft<H, RH, TH, false, true>(buf, NZH, 1, s_tw_zh);
+  r2c_post<NZ, RH, TH>(buf, s_tw_z, RH);
+  __syncthreads();
+  {
+    // Z -> Y: element (r, kz) of row y = row0 + r goes to the CTA owning kz
+    C v[P::UZ];
+#pragma unroll
+    for (int u = 0; u < P::UZ; ++u) {
+      const int e = tid + u * TH;
+      if (e < P::ZE) v[u] = buf[e];
+    }
+    cluster_sync_all();  // both buffers read
+#pragma unroll
+    for (int u = 0; u < P::UZ; ++u) {
+      const int e = tid + u * TH;
+      if (e < P::ZE) {
+        const int r = e / NZH, kz = e - (e / NZH) * NZH;
+        const int y = row0 + r;
+        const int owner = (kz == NZ / 2) ? 0 : (kz / CH);
+        const int slot = (kz == NZ / 2) ? CH : (kz - owner * CH);
+        if (owner == (int)me) buf[y * YS + slot] = v[u];
+        else st_peer(pbase + 8u * (uint32_t)(y * YS + slot), v[u]);
+      }
+    }
+    cluster_sync_all();  // both Y layouts complete
+  }
+  // forward y FFT of the columns (plane_y_forward on this CTA's part)
+  if (me == 0) {
+    for (int y = tid; y < NY; y += TH) buf[y * YS] = C{buf[y * YS].x, buf[y * YS + CH].x};
+  }
+  __syncthreads();
+  smem_fft<NY, CH, TH, false, true, C, typename PlanY<NY>::type>(buf, 1, YS, s_tw_y);
+  if (me == 0) {
+    for (int k = tid; k <= NY / 2; k += TH) {
+      const int km = (NY - k) % NY;
+      const C c = buf[k * YS], d = buf[km * YS];
+      const C a0 = {0.5f * (c.x + d.x), 0.5f * (c.y - d.y)};
+      const C ah = {0.5f * (c.y + d.y), 0.5f * (d.x - c.x)};
+      buf[k * YS] = a0;
+      buf[k * YS + CH] = ah;
+      if (km != k) {
+        buf[km * YS] = C{a0.x, -a0.y};
+        buf[km * YS + CH] = C{ah.x, -ah.y};
+      }
+    }
+  }
+  __syncthreads();
+  C* dst = w.spec + soff;
+  for (int e = tid; e < NY * CH; e += TH) {
+    const int y = e / CH, c = e - (e / CH) * CH;
+    dst[(size_t)y * NZH + col0 + c] = buf[y * YS + c];
+  }
+  if (me == 0)
+    for (int y = tid; y < NY; y += TH) dst[(size_t)y * NZH + NZ / 2] = buf[y * YS + CH];
+}
+
+cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, int nx, const float2* tw_y,
+                                 const float2* tw_zh, const float2* tw_z, cudaStream_t st) {
+  auto kern = plane_c256_kernel;
+  static unsigned attr_mask = 0;
+  cudaError_t e = ensure_smem_attr(kern, PlaneC256::SMEM, &attr_mask);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * nx, nworks);
+  cfg.blockDim = dim3(PlaneC256::TH);
+  cfg.dynamicSmemBytes = PlaneC256::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, kern, d_works, tw_y, tw_zh, tw_z);
+}
+
+bool cluster_plane_supported(int prec_bytes, int ny, int nz) { return prec_bytes == 4 && ny == 256 && nz == 256; }
+
 #define PSB_PLANE_CASE(T, NY, NZ, TH)                                                      \
   if (ny == NY && nz == NZ)                                                                \
     return (variant & 1) ? launch_plane_t<T, NY, NZ, TH, true, true>(                      \

@@ -32,6 +32,23 @@ template <typename T> struct SweepSet {
   const int* pencil_cnt = nullptr;
 };
 
+// The two-CTA cluster plane pass exists for FP32 256 x 256 planes only.
+template <typename T>
+inline bool cluster_path(const SweepSet<T>& s, int variant) {
+  return (variant & VARIANT_CLUSTER) && sizeof(T) == 4 && !s.fused_plane &&
+         cluster_plane_supported((int)sizeof(T), s.n[1], s.n[2]);
+}
+template <typename T>
+inline cudaError_t launch_plane_cluster_t(const PlaneWork<T>*, int, int, const c2_t<T>*, const c2_t<T>*,
+                                          const c2_t<T>*, cudaStream_t) {
+  return cudaErrorInvalidValue;
+}
+template <>
+inline cudaError_t launch_plane_cluster_t<float>(const PlaneWork<float>* w, int nw, int nx, const float2* ty,
+                                                 const float2* tzh, const float2* tz, cudaStream_t st) {
+  return launch_plane_cluster(w, nw, nx, ty, tzh, tz, st);
+}
+
 template <typename T>
 cudaError_t launch_sweep_set(const SweepSet<T>& s, int variant, cudaStream_t st, long long* nlaunch) {
   const int nx = s.n[0], ny = s.n[1], nz = s.n[2];
@@ -53,6 +70,10 @@ cudaError_t launch_sweep_set(const SweepSet<T>& s, int variant, cudaStream_t st,
       if (nxw > 0) PSB_L(launch_xy<T>(xw, nxw, nx, s.nzh, s.tw_x, variant, st));
     } else if (s.fused_plane) {
       PSB_L(launch_plane<T>(pw, np, nx, ny, nz, s.tw_y, s.tw_zh, s.tw_z, variant, st));
+      if (nxw > 0)
+        PSB_L(launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * s.nzh, s.tw_x, nx, ny, nz, variant, st));
+    } else if (cluster_path(s, variant)) {
+      PSB_L(launch_plane_cluster_t<T>(pw, np, nx, s.tw_y, s.tw_zh, s.tw_z, st));
       if (nxw > 0)
         PSB_L(launch_pencil<T>(xw, nxw, PENCIL_KINV, nx, 1, ny * s.nzh, s.tw_x, nx, ny, nz, variant, st));
     } else {
@@ -81,6 +102,7 @@ cudaError_t autotune_sweep_set(const SweepSet<T>& s, cudaStream_t st, float* tun
   for (int v = 0; v < VARIANT_COUNT && e == cudaSuccess; ++v) {
     tune_ms[v] = -1.f;
     if ((v & VARIANT_XY) && (!s.xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
+    if ((v & VARIANT_CLUSTER) && (!cluster_path(s, v) || (v & VARIANT_XY))) continue;
     if (v & VARIANT_SPLIT) continue;  // a property of how an instance's sweeps are launched
     long long nl = 0;
     e = launch_sweep_set<T>(s, v, st, &nl);

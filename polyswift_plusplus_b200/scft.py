@@ -156,7 +156,7 @@ class ScftSolver:
         return int(self._lib.ps_gpu_stream(self._h) or 0)
 
     def set_variant(self, variant: int) -> None:
-        """Force a kernel variant (0..15) or re-enable autotuning (-1)."""
+        """Force a kernel variant (0..31) or re-enable autotuning (-1)."""
         self._check(self._lib.ps_gpu_set_variant(self._h, int(variant)))
 
     def set_spectral_filter(self, spec_filter) -> None:
@@ -191,9 +191,9 @@ class ScftSolver:
         """(chosen variant or -1 before tuning, measured sweep ms of each variant;
         -1 for variants that were not timed)."""
         v = C.c_int()
-        t = (C.c_float * 16)()
-        self._check(self._lib.ps_gpu_get_variant(self._h, C.byref(v), t, 16))
-        return v.value, [t[i] for i in range(16)]
+        t = (C.c_float * 32)()
+        self._check(self._lib.ps_gpu_get_variant(self._h, C.byref(v), t, 32))
+        return v.value, [t[i] for i in range(32)]
 
     def enable_sweep_timing(self, max_samples: int) -> None:
         self._check(self._lib.ps_gpu_enable_sweep_timing(self._h, int(max_samples)))

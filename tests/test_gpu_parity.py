@@ -90,6 +90,72 @@ def test_every_kernel_variant_matches_oracle(gpu, oracle_lib, variant, n):
     assert_parity(cfg, g, o, hg, ho)
 
 
+def _slab256(precision):
+    """A diblock on an 8 x 256 x 256 grid: 256 x 256 y-z planes (the cluster plane
+    pass) at a size the FP64 oracle runs in seconds."""
+    cfg, _ = W.diblock32(n=16, precision=precision)
+    cfg.n = (8, 256, 256)
+    cfg.cell = (0.5, 0.03125, 0.03125)
+    x, y, z = W.coords(cfg)
+    c = np.cos(2 * math.pi * z / cfg.box[2]).reshape(-1) + 0.5 * np.cos(2 * math.pi * y / cfg.box[1]).reshape(-1)
+    w = W.random_fields(cfg, 0.1)
+    return cfg, [w[0] + c, w[1] - c]
+
+
+@pytest.mark.parametrize("base", [0, 8])
+def test_cluster_plane_pass_256(gpu, oracle_lib, base):
+    """Variant bit 4: FP32 256 x 256 y-z planes as one plane pass on a cluster of
+    two CTAs (column halves for the y FFTs, row halves for the z passes,
+    exchanged through distributed shared memory), instead of a row pass and
+    two y pencil passes.  Against the same variant without the bit (the FFT
+    decomposition differs, so FP32 rounding does) and against the FP64 oracle
+    at the mixed-path tolerance."""
+    cfg, w = _slab256("mixed")
+    iters = 3
+    runs = {}
+    for v in (base, base | 16):
+        g = ScftSolver(cfg)
+        g.set_variant(v)
+        g.restore(w)
+        g.update(iters)
+        assert g.variant()[0] == v
+        runs[v] = (g.scalars(), [g.w(i) for i in range(2)], [g.phi(i) for i in range(2)],
+                   g.propagator(0, 1, A.PS_FROM_HEAD, 20))
+        g.close()
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(iters)
+    a, b = runs[base], runs[base | 16]
+    fo = ho[-1]["free_energy"]
+    print(f"F: cluster {b[0]['free_energy']:.10f}, rows {a[0]['free_energy']:.10f}, oracle {fo:.10f}; "
+          f"phi vs oracle: cluster {max(rel(b[2][i], o.phi(i)) for i in range(2)):.2e}, "
+          f"rows {max(rel(a[2][i], o.phi(i)) for i in range(2)):.2e}; "
+          f"cluster vs rows: w {max(rel(b[1][i], a[1][i]) for i in range(2)):.2e}, q {rel(b[3], a[3]):.2e}")
+    # FP32 sweeps: F within the mixed path's floor of a few 1e-6, fields to ~1e-5
+    assert abs(b[0]["free_energy"] - fo) < 1e-5
+    assert abs(b[0]["free_energy"] - a[0]["free_energy"]) < 1e-5
+    assert b[0]["q"][0] == pytest.approx(ho[-1]["q"][0], rel=1e-5)
+    for i in range(2):
+        assert rel(b[1][i], a[1][i]) < 1e-4
+        assert rel(b[2][i], o.phi(i)) < 1e-4
+    assert rel(b[3], a[3]) < 1e-4
+
+
+def test_cluster_variant_only_where_it_exists(gpu):
+    for prec, n in (("mixed", 16), ("fp64", 16)):
+        cfg, _ = W.diblock32(n=n, precision=prec)
+        g = ScftSolver(cfg)
+        with pytest.raises(A.PsError) as e:
+            g.set_variant(16)
+        assert e.value.code == A.PS_ATTRIB_ERR
+        g.close()
+    cfg, _ = _slab256("fp64")  # FP64 256 x 256 planes do not fit two CTAs
+    g = ScftSolver(cfg)
+    with pytest.raises(A.PsError):
+        g.set_variant(16)
+    g.close()
+
+
 def test_autotune_picks_a_measured_variant(gpu):
     cfg, w = W.diblock32(n=32, precision="mixed")
     g = ScftSolver(cfg)
@@ -97,7 +163,7 @@ def test_autotune_picks_a_measured_variant(gpu):
     g.update(3)
     v, ms = g.variant()
     timed = [t for t in ms if t > 0]
-    assert 0 <= v < 16 and len(timed) >= 8
+    assert 0 <= v < 32 and len(timed) >= 8
     assert ms[v] == min(timed)
 
 
