@@ -863,7 +863,7 @@ __device__ __forceinline__ void st_peer(uint32_t addr, float2 v) {
 }
 
 struct PlaneC256 {
-  static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128, TH = 512;
+  static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128, TH = 1024;
   static constexpr int CH = 64;           // y-FFT columns per CTA
   static constexpr int YS = CH + 1;       // Y row stride (slot CH: kz = 128 in CTA 0)
   static constexpr int RH = NY / 2;       // z rows per CTA
@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
     for (int u = 0; u < P::UY; ++u) {
       const int e = tid + u * TH;
       const int y = e / CH, kz = col0 + (e % CH);
-      if (y >= row0 && y < row0 + RH)  // uniform in u: y = tid / 64 + 8 u
+      if (y >= row0 && y < row0 + RH)  // uniform in u: y = tid / 64 + (TH / 64) u
         buf[(y - row0) * NZH + kz] = v[u];
       else
         st_peer(pbase + 8u * (uint32_t)((y - prow0) * NZH + kz), v[u]);
