@@ -905,14 +905,25 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
   pdl_wait();  // before any read of the spectrum, src or wfac, and any write
 
   if (w.mode != MODE_FIRST) {
-    // this CTA's columns of the half plane, Y layout
+    // this CTA's columns of the half plane, Y layout; every load issued before
+    // the first store
     const C* src = w.spec + soff;
-    for (int e = tid; e < NY * CH; e += TH) {
-      const int y = e / CH, c = e - (e / CH) * CH;
-      buf[y * YS + c] = src[(size_t)y * NZH + col0 + c];
+    {
+      C t[P::UY];
+#pragma unroll
+      for (int u = 0; u < P::UY; ++u) {
+        const int e = tid + u * TH;
+        t[u] = __ldg(src + (size_t)(e / CH) * NZH + col0 + (e % CH));
+      }
+      C tx = C{0.f, 0.f};
+      if (me == 0 && tid < NY) tx = __ldg(src + (size_t)tid * NZH + NZ / 2);
+#pragma unroll
+      for (int u = 0; u < P::UY; ++u) {
+        const int e = tid + u * TH;
+        buf[(e / CH) * YS + (e % CH)] = t[u];
+      }
+      if (me == 0 && tid < NY) buf[tid * YS + CH] = tx;
     }
-    if (me == 0)
-      for (int y = tid; y < NY; y += TH) buf[y * YS + CH] = src[(size_t)y * NZH + NZ / 2];
     __syncthreads();
     // inverse y FFT of the columns (plane_y_inverse on this CTA's part)
     if (me == 0) {
