@@ -309,7 +309,7 @@ template <> struct RVec<double> {
   static constexpr int n = 2;
 };
 
-template <typename T, int ROWS, int NZ, int TH>
+template <typename T, int ROWS, int NZ, int TH, int UCMAX = 4>
 __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_t roff, int rows) {
   constexpr int RS = 2 * (NZ / 2 + 1);
   using VT = RVec<T>;
@@ -320,7 +320,9 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
     // issued before any of them is used
     constexpr int G = ROWS * NZ / VN;
     constexpr int U = G / TH;
-    constexpr int UC = (U % 4 == 0) ? 4 : ((U % 3 == 0) ? 3 : ((U % 2 == 0) ? 2 : 1));
+    constexpr int UC = (UCMAX >= 8 && U % 8 == 0)
+                           ? 8
+                           : ((U % 4 == 0) ? 4 : ((U % 3 == 0) ? 3 : ((U % 2 == 0) ? 2 : 1)));
     constexpr int ZV = NZ / VN;
     static_assert(U % UC == 0, "chunking");
     const bool same = (w.wfac_in == w.wfac_out);
@@ -971,7 +973,7 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
     __syncthreads();
     smem_fft<H, RH, TH, true, true>(buf, NZH, 1, s_tw_zh);
   }
-  real_space<T, RH, NZ, TH>(w, reinterpret_cast<T*>(buf), roff, RH);
+  real_space<T, RH, NZ, TH, 8>(w, reinterpret_cast<T*>(buf), roff, RH);
   if (w.mode == MODE_LAST) return;  // uniform over the cluster
   __syncthreads();
   smem_fft<H, RH, TH, false, true>(buf, NZH, 1, s_tw_zh);
