@@ -67,7 +67,7 @@ def parse_args():
                     help="instances of the batched blend workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--variant", type=int, default=-1,
-                    help="pin the propagator kernel variant (0..15) instead of autotuning, e.g. "
+                    help="pin the propagator kernel variant (0..31) instead of autotuning, e.g. "
                          "so that a profiler run uses the variant the plain run chose")
     ap.add_argument("--workload", choices=["diblock128", "triblock256"], default="diblock128",
                     help="triblock256: the 256^3 ABC scale case (about 75 GB on the device; "
