@@ -342,7 +342,9 @@ int ps_gpu_apply_poisson(ps_handle* h);
  * PsDomain per process, polyswift/polyswift/polyswift.cxx:544-588) ----------
  * ps_gpu_batch_create builds `count` independent instances on one device
  * (each exactly as ps_gpu_create would, updater noise included: each instance
- * draws from its own generator) and groups them into
+ * draws from its own generator; spectral filters and Poisson updaters set on an
+ * instance run on its stream between batch iterations, at their scheduled
+ * steps) and groups them into
  * size classes of equal grid and precision.  ps_gpu_batch_iterate runs n_iter
  * iterations of every instance: each class's propagator sweeps are merged into
  * one launch per contour step, the per-instance field updates run as parallel

@@ -168,6 +168,30 @@ static int launch_batch_iteration(ps_batch* b, long long* nl) {
   return PS_OK;
 }
 
+// Updaters that run after the field update (spectral filters, Poisson), per
+// instance in its updaterSequence order, on the instance's stream between this
+// batch iteration and the next (they sit outside the captured graph because
+// their schedule depends on the step, as for a single handle).
+static int run_post_updaters(ps_batch* b) {
+  bool any = false;
+  for (ps_handle* h : b->inst) any |= !h->post_order.empty();
+  if (!any) return PS_OK;
+  PB_CUDA(b, cudaEventRecord(b->ev_fork, b->st));
+  for (size_t i = 0; i < b->inst.size(); ++i) {
+    ps_handle* h = b->inst[i];
+    if (h->post_order.empty()) continue;
+    PB_CUDA(b, cudaStreamWaitEvent(h->st, b->ev_fork, 0));
+    for (int code : h->post_order) {
+      int rc = (code == POST_FILTER) ? filter_after_iteration(h, h->iterations)
+                                     : poisson_after_iteration(h, h->iterations);
+      if (rc) return instance_error(b, (int)i, rc);
+    }
+    PB_CUDA(b, cudaEventRecord(b->ev_inst[i], h->st));
+    PB_CUDA(b, cudaStreamWaitEvent(b->st, b->ev_inst[i], 0));
+  }
+  return PS_OK;
+}
+
 static int batch_autotune(ps_batch* b) {
   PB_CUDA(b, cudaStreamSynchronize(b->st));
   for (BatchClass& c : b->classes) {
@@ -227,6 +251,8 @@ static int batch_iterate(ps_batch* b, int n) {
       }
       PB_CUDA(b, cudaGraphLaunch(b->gexec, b->st));
     }
+    int rc = run_post_updaters(b);
+    if (rc) return rc;
     for (ps_handle* h : b->inst) h->iterations++;
   }
   PB_CUDA(b, cudaStreamSynchronize(b->st));

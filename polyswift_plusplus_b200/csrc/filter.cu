@@ -308,10 +308,6 @@ extern "C" {
 
 int ps_gpu_set_spectral_filter(ps_handle* h, const ps_filter_config* c) {
   if (!h) return PS_ATTRIB_ERR;
-  if (h->in_batch) {
-    h->err = "a batch instance takes no spectral filter";
-    return PS_ATTRIB_ERR;
-  }
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   filter_free(h);

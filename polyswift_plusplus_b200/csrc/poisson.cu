@@ -180,10 +180,6 @@ extern "C" {
 
 int ps_gpu_set_poisson(ps_handle* h, const ps_poisson_config* c) {
   if (!h) return PS_ATTRIB_ERR;
-  if (h->in_batch) {
-    h->err = "a batch instance takes no Poisson updater";
-    return PS_ATTRIB_ERR;
-  }
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   poisson_free(h);

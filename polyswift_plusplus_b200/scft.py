@@ -229,6 +229,13 @@ class ScftBatch:
         self._b = b
         self._views = [ScftSolver(c, _handle=self._lib.ps_gpu_batch_instance(b, i))
                        for i, c in enumerate(self.cfgs)]
+        # updaters after the field updater, installed in updaterSequence order
+        for v, c in zip(self._views, self.cfgs):
+            for kind, u in c.post_updaters():
+                if kind == "filter":
+                    v.set_spectral_filter(u)
+                else:
+                    v.set_poisson(u)
         self.t = 0
 
     def __len__(self) -> int:

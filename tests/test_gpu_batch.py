@@ -144,13 +144,16 @@ def test_batch_instance_precision_is_fixed(gpu):
         assert e.value.code == A.PS_ATTRIB_ERR
 
 
-def test_batch_with_charged_instances_bit_identical(gpu):
-    """Charged diblocks (ions + charged block, no Poisson updater: a batch takes no
-    post-update updaters) batched with a plain diblock: bit-identical to single runs."""
+@pytest.mark.parametrize("poisson", [False, True])
+def test_batch_with_charged_instances_bit_identical(gpu, poisson):
+    """Charged diblocks (ions + charged block; with and without their Poisson
+    updater, which runs between batch iterations) batched with a plain diblock:
+    bit-identical to single runs."""
     items = []
     for i, n in enumerate(((16, 16, 16), (16, 16, 16))):
-        cfg, w, psi = W.charged_diblock(n=n, seed=300 + i)
-        cfg.poisson = None
+        cfg, w, psi = W.charged_diblock(n=n, seed=300 + i, poisson_every=2)
+        if not poisson:
+            cfg.poisson = None
         items.append((cfg, w, psi))
     plain, wp = W.diblock32(n=16)
     with ScftBatch([c for c, _, _ in items] + [plain]) as b:
@@ -171,4 +174,35 @@ def test_batch_with_charged_instances_bit_identical(gpu):
             for c in range(2):
                 assert np.array_equal(v.rho(c), s.rho(c))
             assert np.array_equal(v.w(0), s.w(0))
+            s.close()
+
+
+def test_batch_with_filtered_instances_bit_identical(gpu):
+    """Spectral filters (simple and multi) on batch instances run at their scheduled
+    steps between batch iterations: each instance bit-identical to its single run."""
+    from polyswift_plusplus_b200.config import SpecFilter
+    items = []
+    for i, kind in enumerate(("simple", "multi", None)):
+        cfg, w = W.diblock32(n=16, precision="fp64" if i != 1 else "mixed")
+        if kind is not None:
+            cfg = dataclasses.replace(cfg, spec_filter=SpecFilter(
+                updatefields=["A", "B"], cutoff_factor=0.02, filter_strength=0.5, apply_start=1,
+                apply_frequency=2, apply_end=9, spec_cells=(4, 4, 4) if kind == "multi" else None))
+        items.append((cfg, w))
+    iters = 7
+    with ScftBatch([c for c, _ in items]) as b:
+        b.set_variant(0)
+        for i, (_, w) in enumerate(items):
+            b.instance(i).restore(w)
+        b.update(3)
+        b.update(iters - 3)
+        for i, (cfg, w) in enumerate(items):
+            s = ScftSolver(cfg)
+            s.set_variant(0)
+            s.restore(w)
+            s.update(iters)
+            v = b.instance(i)
+            assert v.scalars()["free_energy"] == s.scalars()["free_energy"]
+            for f in range(2):
+                assert np.array_equal(v.w(f), s.w(f))
             s.close()
