@@ -206,3 +206,32 @@ def test_batch_with_filtered_instances_bit_identical(gpu):
             for f in range(2):
                 assert np.array_equal(v.w(f), s.w(f))
             s.close()
+
+
+def test_batch_class_with_cluster_plane_pass(gpu):
+    """A size class of 8 x 256 x 256 FP32 instances with the cluster plane pass
+    forced (variant 16: one merged plane launch covers every member's sweeps):
+    each instance bit-identical to its single run with the same variant."""
+    items = []
+    for i in range(3):
+        cfg, _ = W.diblock32(n=16, precision="mixed")
+        cfg = dataclasses.replace(cfg, n=(8, 256, 256), cell=(0.5, 0.03125, 0.03125), seed=700 + i)
+        items.append((cfg, W.random_fields(cfg, 0.3)))
+    iters = 3
+    with ScftBatch([c for c, _ in items]) as b:
+        b.set_variant(16)
+        for i, (_, w) in enumerate(items):
+            b.instance(i).restore(w)
+        b.update(iters)
+        _, variants = b.classes()
+        assert variants == [16]
+        for i, (cfg, w) in enumerate(items):
+            s = ScftSolver(cfg)
+            s.set_variant(16)
+            s.restore(w)
+            s.update(iters)
+            v = b.instance(i)
+            assert v.scalars()["free_energy"] == s.scalars()["free_energy"]
+            for f in range(2):
+                assert np.array_equal(v.phi(f), s.phi(f))
+            s.close()
