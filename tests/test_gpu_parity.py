@@ -64,6 +64,31 @@ def test_fft_plugin_matches_oracle(gpu, oracle_lib, shape):
     assert rel(got, ref) < 1e-12
 
 
+@pytest.mark.parametrize("shape", [(1, 16, 32), (16, 1, 32), (64, 1, 1), (1, 1, 64), (1, 64, 1)])
+def test_fft_plugin_degenerate_axes(gpu, oracle_lib, shape):
+    """Grids with extent-1 axes (1-D and 2-D runs in any orientation)."""
+    rng = np.random.default_rng(5)
+    d = rng.standard_normal(shape)
+    k = rng.standard_normal(shape)
+    got = B200FFT(shape).scaledFFTPair(d, k).reshape(shape)
+    assert rel(got, O.scaled_fft_pair(d, k)) < 1e-12
+
+
+@pytest.mark.parametrize("shape", [(64, 1, 1), (1, 1, 64), (1, 32, 32)])
+def test_fp64_low_dimensional_grids(gpu, oracle_lib, shape):
+    """One- and two-dimensional SCFT (lamellae along the one long axis)."""
+    cfg, _ = W.diblock32(n=8)
+    cfg.n = shape
+    cfg.cell = tuple(4.0 / s if s > 1 else 0.125 for s in shape)
+    w = W.random_fields(cfg, 0.3)
+    ax = [i for i, s in enumerate(shape) if s > 1][0]
+    x = W.coords(cfg)[ax].reshape(-1)
+    c = np.cos(2 * math.pi * x / cfg.box[ax])
+    w = [w[0] + c, w[1] - c]
+    g, o, hg, ho = run_both(cfg, w, 8)
+    assert_parity(cfg, g, o, hg, ho)
+
+
 @pytest.mark.parametrize("n", [16, 32])
 def test_fp64_diblock_parity(gpu, oracle_lib, n):
     cfg, w = W.diblock32(n=n)
