@@ -256,6 +256,24 @@ def test_fp64_triblock_three_fields(gpu, oracle_lib):
     assert_parity(cfg, g, o, hg, ho)
 
 
+def test_fp64_triblock_three_fields_anderson(gpu, oracle_lib):
+    """Anderson mixing on three fields (the nf = 3 update kernels) against the
+    oracle; as for the diblock trajectory test, the Gram entries cancel, so 1e-6."""
+    ds = 0.02
+    tri = Polymer("abc", 1.0, 100, [Block("a", "A", ds, 0.3, ["freeEnd"], ["b"]),
+                                    Block("b", "B", ds, 0.4, ["a"], ["c"]),
+                                    Block("c", "C", ds, 0.3, ["b"], ["freeEnd"])])
+    cfg = ScftConfig(n=(16, 16, 16), cell=(0.25,) * 3, fields=["A", "B", "C"], polymers=[tri],
+                     interactions=[Interaction("AB", 0.3, ["A", "B"]),
+                                   Interaction("BC", 0.3, ["B", "C"]),
+                                   Interaction("AC", 0.45, ["A", "C"])],
+                     updater=Updater(kind="andersonMixing", relaxlambdas=(0.05, 0.025), anderson_depth=4,
+                                     anderson_mix=0.1, anderson_start=3), seed=91)
+    w = W.random_fields(cfg, 0.3)
+    g, o, hg, ho = run_both(cfg, w, 12)
+    assert_parity(cfg, g, o, hg, ho, tol=1e-6)
+
+
 def test_fp64_blend_with_homopolymer(gpu, oracle_lib):
     cfg = W.blend(16, 18.0, 0.35, 0.15, precision="fp64", seed=12, anderson=False)
     w = W.random_fields(cfg, 0.3)
