@@ -89,6 +89,27 @@ def test_fp64_low_dimensional_grids(gpu, oracle_lib, shape):
     assert_parity(cfg, g, o, hg, ho)
 
 
+def test_mixed_long_x_axis(gpu, oracle_lib):
+    """FP32 sweeps on a 256 x 8 x 8 grid (x pencils of length 256) against the
+    FP64 oracle at the mixed-path tolerance."""
+    cfg, _ = W.diblock32(n=8, precision="mixed")
+    cfg.n = (256, 8, 8)
+    cfg.cell = (8.0 / 256, 0.25, 0.25)
+    x = W.coords(cfg)[0].reshape(-1)
+    c = np.cos(2 * math.pi * x / cfg.box[0])
+    w = W.random_fields(cfg, 0.2)
+    w = [w[0] + c, w[1] - c]
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(4)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(4)
+    assert abs(g.scalars()["free_energy"] - ho[-1]["free_energy"]) < 1e-5
+    for i in range(2):
+        assert rel(g.phi(i), o.phi(i)) < 1e-4
+
+
 @pytest.mark.parametrize("n", [16, 32])
 def test_fp64_diblock_parity(gpu, oracle_lib, n):
     cfg, w = W.diblock32(n=n)
