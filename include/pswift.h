@@ -19,6 +19,18 @@
  *   ps_gpu_get_propagator  PsBlock qs/qts storage                pspolymer/PsBlock.cpp:131-134
  *   ps_fft_scaled_pair     PsFFTBase::scaledFFTPair              psbase/PsFFTBase.h:105,
  *                                                               psfft/PsFFTW.cpp:196-224
+ *   ps_fft_scaled_pair_im  PsFFTBase::scaledFFTPairIm            psbase/PsFFTBase.h:116,
+ *                                                               psfft/PsFFTW.cpp:227-257
+ *   ps_fft_convolve_re     PsFFTBase::convolveRe                 psbase/PsFFTBase.h:94,
+ *                                                               psfft/PsFFTW.cpp:150-189
+ *   ps_fft_forward_abs     PsFFTBase::forwardFFTAbs              psbase/PsFFTBase.h:83,
+ *                                                               psfft/PsFFTW.cpp:122-149
+ *   ps_fft_forward         PsFFTBase::calcForwardFFT             psbase/PsFFTBase.h:125,
+ *                                                               psfft/PsFFTW.cpp:260-278
+ *   ps_fft_backward        PsFFTBase::calcBackwardFFT            psbase/PsFFTBase.h:134,
+ *                                                               psfft/PsFFTW.cpp:281-297
+ *   ps_fft_size            PsFFTBase::getFFTSize                 psbase/PsFFTBase.h:75
+ *   ps_fft_get_grid        PsFFTBase::getGrid (the grid extents) psbase/PsFFTBase.h:70
  */
 #ifndef PSWIFT_H
 #define PSWIFT_H
@@ -394,14 +406,39 @@ void* ps_adj_stream(const ps_adj* a);
 /* Message for the last error of an adjoint (or of the calling thread when a is NULL). */
 const char* ps_adj_last_error(const ps_adj* a);
 
-/* --- FFT plugin: PsFFTBase<T,3>::scaledFFTPair with host pointers ---------
- * res = Re(IFFT(kdata * FFT(data))), both transforms unnormalised, as the
- * reference's FFTW c2c pair.  Inputs and outputs are host arrays of n[0]*n[1]*n[2]
- * doubles; the call copies them over PCIe (a correct plugin, not the fast path). */
+/* --- Fault injection for the bounded waits --------------------------------
+ * No counterpart in the reference.  Every wait of a kernel on a bulk copy is
+ * bounded; when a plane pass's wait runs out, the pass sets error bit 2 of the
+ * handle's status word, drains the copy still in flight (full bound) and
+ * returns, and the handle reports PS_GPU_ERR with the context still usable.
+ * This sets the poll limit of that first wait on the current device (default
+ * 2^22 polls; 0 gives up at once, 0xFFFFFFFF restores the default), so a test
+ * can drive the timeout path without a fault.  Not for production runs. */
+int ps_gpu_set_bulk_wait_limit(unsigned int polls);
+
+/* --- FFT plugin: PsFFTBase<T,3> with host pointers ------------------------
+ * The transforms are unnormalised and follow the reference's FFTW c2c calls on
+ * real data (forward sign -1, backward +1).  Inputs and outputs are host arrays
+ * of n[0]*n[1]*n[2] doubles in row-major order; each call copies them over
+ * PCIe (a correct plugin, not the fast path) and returns when res is written.
+ * Errors: PS_ATTRIB_ERR (null argument), PS_GPU_ERR (CUDA).
+ *   ps_fft_scaled_pair     res = Re(IFFT(kdata * FFT(data)))
+ *   ps_fft_scaled_pair_im  res = Re(IFFT(kdata * FFT(i*data)))  (data is the imaginary part)
+ *   ps_fft_convolve_re     res = Re(IFFT(FFT(data1) * FFT(data2)))
+ *   ps_fft_forward_abs     res = |FFT(data)|^2  (re^2 + im^2, as the reference computes it)
+ *   ps_fft_forward         res = Re(FFT(data))
+ *   ps_fft_backward        res = Re(IFFT(data)) for real data (the spectrum's imaginary part is 0)
+ *   ps_fft_size            n[0]*n[1]*n[2];  ps_fft_get_grid  the extents n[3] */
 int ps_fft_create(const int n[3], int precision, int device, ps_fft** out);
 int ps_fft_destroy(ps_fft* f);
 int ps_fft_size(const ps_fft* f, size_t* n_total);
+int ps_fft_get_grid(const ps_fft* f, int n[3]);
 int ps_fft_scaled_pair(ps_fft* f, const double* data, const double* kdata, double* res);
+int ps_fft_scaled_pair_im(ps_fft* f, const double* data, const double* kdata, double* res);
+int ps_fft_convolve_re(ps_fft* f, const double* data1, const double* data2, double* res);
+int ps_fft_forward_abs(ps_fft* f, const double* data, double* res);
+int ps_fft_forward(ps_fft* f, const double* data, double* res);
+int ps_fft_backward(ps_fft* f, const double* data, double* res);
 /* Message for the last FFT-plugin error of the calling thread. */
 const char* ps_fft_last_error(void);
 
@@ -419,8 +456,11 @@ const char* ps_fft_last_error(void);
  * tables exceed it return PS_INPUT_ERR (64^3 fits, 96^3 does not).  All calls on a device
  * share that storage, so calls that overlap on the GPU (other streams or
  * threads) race.  The first call on each device resolves the storage's
- * address; make it before any stream capture.  Errors: PS_ATTRIB_ERR (null or
- * misaligned pointer), PS_INPUT_ERR (extent or size), PS_GPU_ERR (CUDA). */
+ * address; make it before any stream capture (calls outside a capture resolve
+ * it again, so a device reset by the host does not leave it stale).  A bulk
+ * copy that times out inside the kernels leaves res unwritten and is not
+ * reported.  Errors: PS_ATTRIB_ERR (null or misaligned pointer), PS_INPUT_ERR
+ * (extent or size), PS_GPU_ERR (CUDA). */
 int ps_fft_scaled_pair_noalloc(const int n[3], const double* data, const double* kdata,
                                double* res, void* stream);
 size_t ps_fft_noalloc_scratch_bytes(void);

@@ -33,6 +33,11 @@ def lib() -> C.CDLL:
         L.oracle_mt_u32.argtypes = [C.c_ulonglong, C.c_long, vp]
         L.oracle_fft3d.argtypes = [C.POINTER(C.c_int), vp, vp, C.c_int]
         L.oracle_scaled_fft_pair.argtypes = [C.POINTER(C.c_int), vp, vp, vp]
+        L.oracle_scaled_fft_pair_im.argtypes = [C.POINTER(C.c_int), vp, vp, vp]
+        L.oracle_convolve_re.argtypes = [C.POINTER(C.c_int), vp, vp, vp]
+        L.oracle_forward_fft_abs.argtypes = [C.POINTER(C.c_int), vp, vp]
+        L.oracle_calc_forward_fft.argtypes = [C.POINTER(C.c_int), vp, vp]
+        L.oracle_calc_backward_fft.argtypes = [C.POINTER(C.c_int), vp, vp]
         L.oracle_create.restype = C.c_int
         L.oracle_create.argtypes = [C.POINTER(A.ps_config), C.POINTER(vp), C.c_char_p, C.c_int]
         L.oracle_destroy.argtypes = [vp]
@@ -101,6 +106,48 @@ def scaled_fft_pair(data: np.ndarray, kdata: np.ndarray) -> np.ndarray:
     res = np.empty_like(d)
     lib().oracle_scaled_fft_pair(n, _ptr(d), _ptr(k), _ptr(res))
     return res
+
+
+def _two_input(fn: str, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    n = (C.c_int * 3)(*a.shape)
+    x = np.ascontiguousarray(a, dtype=np.float64)
+    y = np.ascontiguousarray(b, dtype=np.float64)
+    res = np.empty_like(x)
+    getattr(lib(), fn)(n, _ptr(x), _ptr(y), _ptr(res))
+    return res
+
+
+def _one_input(fn: str, a: np.ndarray) -> np.ndarray:
+    n = (C.c_int * 3)(*a.shape)
+    x = np.ascontiguousarray(a, dtype=np.float64)
+    res = np.empty_like(x)
+    getattr(lib(), fn)(n, _ptr(x), _ptr(res))
+    return res
+
+
+def scaled_fft_pair_im(data: np.ndarray, kdata: np.ndarray) -> np.ndarray:
+    """PsFFTW::scaledFFTPairIm: Re(IFFT(kdata * FFT(i*data)))."""
+    return _two_input("oracle_scaled_fft_pair_im", data, kdata)
+
+
+def convolve_re(data1: np.ndarray, data2: np.ndarray) -> np.ndarray:
+    """PsFFTW::convolveRe: Re(IFFT(FFT(data1) * FFT(data2)))."""
+    return _two_input("oracle_convolve_re", data1, data2)
+
+
+def forward_fft_abs(data: np.ndarray) -> np.ndarray:
+    """PsFFTW::forwardFFTAbs: |FFT(data)|^2 elementwise."""
+    return _one_input("oracle_forward_fft_abs", data)
+
+
+def calc_forward_fft(data: np.ndarray) -> np.ndarray:
+    """PsFFTW::calcForwardFFT: Re(FFT(data))."""
+    return _one_input("oracle_calc_forward_fft", data)
+
+
+def calc_backward_fft(data: np.ndarray) -> np.ndarray:
+    """PsFFTW::calcBackwardFFT: Re(IFFT(data)), unnormalised."""
+    return _one_input("oracle_calc_backward_fft", data)
 
 
 def gauss_laguerre(n: int, a: float):

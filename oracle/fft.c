@@ -191,6 +191,88 @@ void oracle_scaled_fft_pair(const int n[3], const double* data, const double* kd
   free(c);
 }
 
+/* The other transforms of PsFFTBase<T,3> (psbase/PsFFTBase.h:83-134), serial
+ * branch of PsFFTW (psfft/PsFFTW.cpp): each packs its real input into the
+ * complex work array, runs the unnormalised c2c FFTW-sign transforms and keeps
+ * what the reference keeps. */
+
+/* PsFFTW::forwardFFTAbs (psfft/PsFFTW.cpp:122-149): res = re^2 + im^2 of the
+ * forward transform (the squared modulus, as the reference computes it). */
+void oracle_forward_fft_abs(const int n[3], const double* data, double* res) {
+  long N = (long)n[0] * n[1] * n[2];
+  double* c = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) { c[2 * i] = data[i]; c[2 * i + 1] = 0.0; }
+  oracle_fftnd_inplace(n, c, -1);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) res[i] = (c[2 * i] * c[2 * i]) + (c[2 * i + 1] * c[2 * i + 1]);
+  free(c);
+}
+
+/* PsFFTW::convolveRe (psfft/PsFFTW.cpp:150-189): both inputs forward, the
+ * complex product, backward, real part. */
+void oracle_convolve_re(const int n[3], const double* data1, const double* data2, double* res) {
+  long N = (long)n[0] * n[1] * n[2];
+  double* c = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+  double* c2 = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) {
+    c[2 * i] = data1[i]; c[2 * i + 1] = 0.0;
+    c2[2 * i] = data2[i]; c2[2 * i + 1] = 0.0;
+  }
+  oracle_fftnd_inplace(n, c, -1);
+  oracle_fftnd_inplace(n, c2, -1);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) {
+    const double ar = c[2 * i], ai = c[2 * i + 1], br = c2[2 * i], bi = c2[2 * i + 1];
+    c[2 * i] = (ar * br) - (ai * bi);
+    c[2 * i + 1] = (ai * br) + (ar * bi);
+  }
+  oracle_fftnd_inplace(n, c, +1);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) res[i] = c[2 * i];
+  free(c2);
+  free(c);
+}
+
+/* PsFFTW::scaledFFTPairIm (psfft/PsFFTW.cpp:227-257): the input is the
+ * imaginary part, the transform is scaled by the real kdata, real part kept. */
+void oracle_scaled_fft_pair_im(const int n[3], const double* data, const double* kdata,
+                               double* res) {
+  long N = (long)n[0] * n[1] * n[2];
+  double* c = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) { c[2 * i] = 0.0; c[2 * i + 1] = data[i]; }
+  oracle_fftnd_inplace(n, c, -1);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) { c[2 * i] *= kdata[i]; c[2 * i + 1] *= kdata[i]; }
+  oracle_fftnd_inplace(n, c, +1);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) res[i] = c[2 * i];
+  free(c);
+}
+
+/* PsFFTW::calcForwardFFT / calcBackwardFFT (psfft/PsFFTW.cpp:260-297): the real
+ * part of the forward (sign -1) or backward (sign +1) transform of real data. */
+static void real_part_of_transform(const int n[3], const double* data, double* res, int sign) {
+  long N = (long)n[0] * n[1] * n[2];
+  double* c = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) { c[2 * i] = data[i]; c[2 * i + 1] = 0.0; }
+  oracle_fftnd_inplace(n, c, sign);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) res[i] = c[2 * i];
+  free(c);
+}
+
+void oracle_calc_forward_fft(const int n[3], const double* data, double* res) {
+  real_part_of_transform(n, data, res, -1);
+}
+
+void oracle_calc_backward_fft(const int n[3], const double* data, double* res) {
+  real_part_of_transform(n, data, res, +1);
+}
+
 int oracle_set_threads(int nt) {
 #ifdef _OPENMP
   if (nt > 0) omp_set_num_threads(nt);

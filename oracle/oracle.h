@@ -38,6 +38,17 @@ void oracle_fft3d(const int n[3], double* re, double* im, int sign);
 void oracle_scaled_fft_pair(const int n[3], const double* data, const double* kdata,
                             double* res);
 
+/* The rest of PsFFTBase<T,3> as PsFFTW computes it in serial
+ * (psfft/PsFFTW.cpp:122-297): |FFT|^2 (forwardFFTAbs), Re(IFFT(FFT(a)FFT(b)))
+ * (convolveRe), Re(IFFT(kdata*FFT(i*data))) (scaledFFTPairIm), Re(FFT(data))
+ * (calcForwardFFT) and Re(IFFT(data)) (calcBackwardFFT); unnormalised. */
+void oracle_forward_fft_abs(const int n[3], const double* data, double* res);
+void oracle_convolve_re(const int n[3], const double* data1, const double* data2, double* res);
+void oracle_scaled_fft_pair_im(const int n[3], const double* data, const double* kdata,
+                               double* res);
+void oracle_calc_forward_fft(const int n[3], const double* data, double* res);
+void oracle_calc_backward_fft(const int n[3], const double* data, double* res);
+
 /* Build a whole SCFT instance (same checks as the device path). */
 int oracle_create(const ps_config* cfg, oracle_state** out, char* err, int errlen);
 void oracle_destroy(oracle_state* s);

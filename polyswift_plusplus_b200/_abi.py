@@ -174,7 +174,14 @@ SIGNATURES = {
     "ps_fft_create": (C.c_int, [C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(_vp)]),
     "ps_fft_destroy": (C.c_int, [_vp]),
     "ps_fft_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "ps_gpu_set_bulk_wait_limit": (C.c_int, [C.c_uint]),
+    "ps_fft_get_grid": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "ps_fft_scaled_pair": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ps_fft_scaled_pair_im": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ps_fft_convolve_re": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ps_fft_forward_abs": (C.c_int, [_vp, _vp, _vp]),
+    "ps_fft_forward": (C.c_int, [_vp, _vp, _vp]),
+    "ps_fft_backward": (C.c_int, [_vp, _vp, _vp]),
     "ps_gauss_laguerre": (C.c_int, [C.c_int, C.c_double, _vp, _vp]),
     "ps_fft_last_error": (C.c_char_p, []),
     "ps_fft_scaled_pair_noalloc": (C.c_int, [C.POINTER(C.c_int), _vp, _vp, _vp, _vp]),

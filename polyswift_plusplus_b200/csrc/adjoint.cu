@@ -806,6 +806,7 @@ int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out) {
     g_adj_err = a->err;
     adj_free(a);
     delete a;
+    cudaGetLastError();  // clear a failed allocation's last-error state
     return rc;
   }
   *out = a;

@@ -352,6 +352,7 @@ int ps_gpu_batch_create(const ps_config* cfgs, int count, ps_batch** out) {
     g_batch_err = b->err;
     batch_free(b);
     delete b;
+    cudaGetLastError();  // clear a failed allocation's last-error state
     return rc;
   }
   *out = b;

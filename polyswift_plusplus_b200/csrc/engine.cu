@@ -1014,6 +1014,12 @@ int engine_check_scalars(ps_handle* h) {
   PS_CUDA(h, cudaStreamSynchronize(h->st));
   int rn = noise_check(h);
   if (rn) return rn;
+  // a timed-out bulk copy first: the pass it stopped leaves stale data that
+  // may also make Q or F non-finite
+  if (h->h_sc->error_flags & 4) {
+    h->err = "a bulk shared-memory copy did not complete within the wait limit";
+    return PS_GPU_ERR;
+  }
   if (h->h_sc->error_flags & 1) {
     h->err = "PsBlock::calcBigQ() found nan/inf?";
     return PS_RUN_ERR;
@@ -1021,10 +1027,6 @@ int engine_check_scalars(ps_handle* h) {
   if (h->h_sc->error_flags & 2) {
     h->err = "non-finite free energy";
     return PS_RUN_ERR;
-  }
-  if (h->h_sc->error_flags & 4) {
-    h->err = "a bulk shared-memory copy did not complete within the wait limit";
-    return PS_GPU_ERR;
   }
   return PS_OK;
 }
@@ -1143,6 +1145,9 @@ int ps_gpu_create(const ps_config* cfg, ps_handle** out) {
     g_thread_err = h->err;
     free_all(h);
     delete h;
+    // a failed allocation leaves a (non-sticky) error in the runtime's
+    // last-error slot; clear it so the next launch check does not report it
+    cudaGetLastError();
     return rc;
   }
   *out = h;

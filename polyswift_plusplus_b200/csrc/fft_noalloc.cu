@@ -19,9 +19,14 @@
 //   host threads racing) corrupt each other's results;
 // * the first call on a device resolves the scratch address
 //   (cudaGetSymbolAddress) with that device current; make that first call
-//   before any stream capture;
+//   before any stream capture.  Later calls outside a capture resolve it
+//   again (cheap, allocates nothing), so the address stays right after the
+//   host application resets the device;
 // * the call is asynchronous on `stream`: res is valid once the stream is
-//   synchronised.
+//   synchronised;
+// * the transform kernels bound their waits on the bulk copies; a copy that
+//   does not land in time leaves res unwritten, and this entry point does not
+//   report it (it returns before the GPU runs).
 // No cudaMalloc, cudaFree or allocating library routine is called.
 #include <math.h>
 #include <stdint.h>
@@ -69,16 +74,24 @@ __global__ void noalloc_works_kernel(PlaneWork<double>* pw, PencilWork<double>* 
   xw[0] = x;
 }
 
+// Launched without programmatic serialisation between the set-up kernels and
+// the first transform kernel.  The transform kernels are launched with it and
+// read their work descriptors and twiddles before waiting on the kernel ahead
+// of them; behind this ordinary launch that kernel cannot start before the
+// set-up kernels have finished and their writes are visible.
+__global__ void noalloc_order_kernel() {}
+
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-// Resolve the scratch address for the current device (once per device).
-static int noalloc_scratch(int dev, unsigned char** out) {
+// Resolve the scratch address for the current device: on the first call, and
+// on every call made outside a stream capture (`refresh`).
+static int noalloc_scratch(int dev, bool refresh, unsigned char** out) {
   if (dev < 0 || dev >= 64) {
     g_noalloc_err = "device ordinal out of range";
     return PS_GPU_ERR;
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev] || refresh) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -155,10 +168,12 @@ int ps_fft_scaled_pair_noalloc(const int n[3], const double* d_data, const doubl
   }
   int dev = 0;
   NA_CUDA(cudaGetDevice(&dev));
-  unsigned char* base = nullptr;
-  int rc = noalloc_scratch(dev, &base);
-  if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  NA_CUDA(cudaStreamIsCapturing(st, &cap));
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(dev, cap == cudaStreamCaptureStatusNone, &base);
+  if (rc) return rc;
   double2* spec = reinterpret_cast<double2*>(base + o_spec);
   double2* twx = reinterpret_cast<double2*>(base + o_twx);
   double2* twy = reinterpret_cast<double2*>(base + o_twy);
@@ -171,6 +186,7 @@ int ps_fft_scaled_pair_noalloc(const int n[3], const double* d_data, const doubl
   noalloc_twiddle_kernel<<<1, 256, 0, st>>>(twz, nz);
   noalloc_twiddle_kernel<<<1, 256, 0, st>>>(twzh, nzhalf);
   noalloc_works_kernel<<<1, 1, 0, st>>>(pw, xw, d_data, d_kdata, d_res, spec);
+  noalloc_order_kernel<<<1, 1, 0, st>>>();
   NA_CUDA(cudaGetLastError());
   if (plane_fused_supported(8, ny, nz)) {
     NA_CUDA(launch_plane<double>(pw, 1, nx, ny, nz, twy, twzh, twz, 0, st));

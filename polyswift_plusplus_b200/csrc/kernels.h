@@ -23,13 +23,22 @@ template <typename T> struct PlaneWork {
 };
 
 // Pencil pass along a strided axis of the half spectrum.
-enum { PENCIL_FWD = 0, PENCIL_INV = 1, PENCIL_KINV = 2, PENCIL_KFULL = 3 };
+// PENCIL_KFULL_IM and PENCIL_KSPEC exist for FP64 only (the FFT plugin).
+enum {
+  PENCIL_FWD = 0,
+  PENCIL_INV = 1,
+  PENCIL_KINV = 2,
+  PENCIL_KFULL = 3,
+  PENCIL_KFULL_IM = 4,
+  PENCIL_KSPEC = 5
+};
 
 template <typename T> struct PencilWork {
   c2_t<T>* spec;
   const T* kx;        // PENCIL_KINV: factor along the pencil axis (1/N folded in)
   const T* kyz;       // PENCIL_KINV: factor per (y, kz) column
-  const double* kfull;// PENCIL_KFULL: full real k array [nx][ny][nz] (plugin path)
+  const double* kfull;// PENCIL_KFULL(_IM): full real k array [nx][ny][nz] (plugin path)
+  const c2_t<T>* kspec;// PENCIL_KSPEC: a second, fully transformed half spectrum (same layout)
 };
 
 bool extent_supported(int n);

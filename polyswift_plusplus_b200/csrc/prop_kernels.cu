@@ -18,11 +18,17 @@
 #include <stdlib.h>
 #include <cstdio>
 
+#include "../../include/pswift.h"
 #include "fft_smem.cuh"
 #include "kernels.h"
 #include "tma.cuh"
 
 namespace psb {
+
+// Poll limit of the plane pass's first wait on its bulk spectrum copy (the
+// wait in the timeout path that drains a copy still in flight keeps kMaxPolls).
+// Lowered only by ps_gpu_set_bulk_wait_limit, to test the timeout path.
+__constant__ uint32_t c_bulk_wait_polls = kMaxPolls;
 
 template <typename T>
 __device__ __forceinline__ T ld_or_one(const T* p, size_t i) {
@@ -479,7 +485,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     if constexpr (BULK) {
       __syncthreads();  // the mbarrier is initialised before anyone polls it
       // every thread waits (bounded); the CTA then agrees on the outcome
-      const int ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0);
+      const int ok = __syncthreads_and(mbar_wait_bounded(bar, 0, c_bulk_wait_polls) ? 1 : 0);
       if (!ok) {
         // the copy did not land in time: flag it, give the copy in flight one
         // more bounded wait, and leave without touching the buffer
@@ -721,6 +727,42 @@ __global__ void __launch_bounds__(TH)
         const T f = T(0.5 * (k1 + k2));
         const C v = buf[e];
         buf[e] = {v.x * f, v.y * f};
+      }
+    }
+    __syncthreads();
+  } else if (MODE == PENCIL_KFULL_IM) {
+    // scaledFFTPairIm: Re(IFFT(kdata * FFT(i*data))) is the c2r of
+    // i * (kdata(k) - kdata(-k))/2 * X for the Hermitian X = FFT(data); the
+    // even part of kdata only produces an imaginary result.
+    const int nzh = nz / 2 + 1;
+    for (int e = tid; e < L * TK; e += TH) {
+      const int i = e / TK;
+      const int cc = e - i * TK;
+      const int c = c0 + cc;
+      if (c < inner) {
+        const int y = c / nzh;
+        const int kz = c - y * nzh;
+        const int xm = (nx - i) % nx, ym = (ny - y) % ny, zm = (nz - kz) % nz;
+        const double k1 = w.kfull[((size_t)i * ny + y) * nz + kz];
+        const double k2 = w.kfull[((size_t)xm * ny + ym) * nz + zm];
+        const T f = T(0.5 * (k1 - k2));
+        const C v = buf[e];
+        buf[e] = {-f * v.y, f * v.x};
+      }
+    }
+    __syncthreads();
+  } else if (MODE == PENCIL_KSPEC) {
+    // convolveRe: multiply by the second operand's transform, element by
+    // element in the same (pencil, column) position.
+    const C* kb = w.kspec + (size_t)o * L * inner;
+    for (int e = tid; e < L * TK; e += TH) {
+      const int i = e / TK;
+      const int cc = e - i * TK;
+      const int c = c0 + cc;
+      if (c < inner) {
+        const C b = kb[(size_t)i * inner + c];
+        const C v = buf[e];
+        buf[e] = {v.x * b.x - v.y * b.y, v.y * b.x + v.x * b.y};
       }
     }
     __syncthreads();
@@ -1308,6 +1350,16 @@ static cudaError_t launch_pencil_modes(const PencilWork<T>* d_works, int nworks,
                                                                      nx, ny, nz, st);
     case PENCIL_KFULL:
       return launch_pencil_t<T, L, TK, TH, PENCIL_KFULL, false>(d_works, nworks, outer, inner, tw, nx, ny, nz, st);
+    case PENCIL_KFULL_IM:
+      if constexpr (sizeof(T) == 8)
+        return launch_pencil_t<T, L, TK, TH, PENCIL_KFULL_IM, false>(d_works, nworks, outer, inner, tw, nx, ny,
+                                                                     nz, st);
+      break;
+    case PENCIL_KSPEC:
+      if constexpr (sizeof(T) == 8)
+        return launch_pencil_t<T, L, TK, TH, PENCIL_KSPEC, false>(d_works, nworks, outer, inner, tw, nx, ny,
+                                                                  nz, st);
+      break;
   }
   return cudaErrorInvalidValue;
 }
@@ -1400,3 +1452,8 @@ cudaError_t launch_pencil<double>(const PencilWork<double>* w, int nw, int mode,
 }
 
 }  // namespace psb
+
+extern "C" int ps_gpu_set_bulk_wait_limit(unsigned int polls) {
+  const uint32_t v = (polls == 0xFFFFFFFFu) ? psb::kMaxPolls : (uint32_t)polls;
+  return cudaMemcpyToSymbol(psb::c_bulk_wait_polls, &v, sizeof(v)) == cudaSuccess ? PS_OK : PS_GPU_ERR;
+}

@@ -60,8 +60,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kMaxPolls; ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint32_t max_polls = kMaxPolls) {
+  for (uint32_t i = 0; i < max_polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

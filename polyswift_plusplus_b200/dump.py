@@ -48,24 +48,62 @@ def dump(solver, path, history=None, pressure_field: str = "defaultPressure") ->
     return path
 
 
+class DumpError(ValueError):
+    """A dump that cannot be restored: unreadable, truncated, or not this grid."""
+
+
+def _read_dump(path, cfg, pressure_field: str) -> dict:
+    """Read and check every dataset restore needs before anything is set."""
+    shape = tuple(int(v) for v in cfg.n)
+    out = {"w": [], "phi": []}
+    try:
+        with np.load(Path(path)) as d:
+            if "numCellsGlobal" not in d:
+                raise DumpError(f"{path}: no numCellsGlobal dataset")
+            got = tuple(int(v) for v in d["numCellsGlobal"])
+            if got != shape:
+                raise DumpError(f"dump grid {got} does not match the solver grid {shape}")
+
+            def field(key):
+                a = np.asarray(d[key], dtype=np.float64)
+                if a.shape != shape:
+                    raise DumpError(f"{path}: {key} has shape {a.shape}, the grid is {shape}")
+                if not np.all(np.isfinite(a)):
+                    raise DumpError(f"{path}: {key} holds non-finite values")
+                return a.reshape(-1).copy()
+
+            for name in cfg.fields:
+                key = f"{name}/{MONO_CONJ}"
+                if key not in d:
+                    raise DumpError(f"dump has no {key}")
+                out["w"].append(field(key))
+                dk = f"{name}/{MONO_DENS}"
+                out["phi"].append(field(dk) if dk in d else None)
+            pkey = f"{pressure_field}/{PRES}"
+            out["p"] = field(pkey) if pkey in d else np.zeros(int(np.prod(shape)))
+            out["meta"] = {
+                "iteration": int(d["iteration"]) if "iteration" in d else 0,
+                "freeEnergy": d["freeEnergy"].copy() if "freeEnergy" in d else None,
+                "cellSizes": tuple(float(v) for v in d["cellSizes"]) if "cellSizes" in d else None}
+    except DumpError:
+        raise
+    except Exception as e:  # truncated or corrupt container (zip, npy header, data)
+        raise DumpError(f"{path}: unreadable dump ({type(e).__name__}: {e})") from e
+    return out
+
+
 def restore(solver, path, pressure_field: str = "defaultPressure") -> dict:
     """Set the conjugate fields, densities and pressure of `solver` from a dump;
-    returns the dump's metadata (iteration, free-energy history)."""
-    cfg = solver.cfg
-    shape = tuple(int(v) for v in cfg.n)
-    with np.load(Path(path)) as d:
-        got = tuple(int(v) for v in d["numCellsGlobal"])
-        if got != shape:
-            raise ValueError(f"dump grid {got} does not match the solver grid {shape}")
-        for i, name in enumerate(cfg.fields):
-            key = f"{name}/{MONO_CONJ}"
-            if key not in d:
-                raise KeyError(f"dump has no {key}")
-            solver.set_field(A.PS_FIELD_W, i, d[key].reshape(-1))
-            if f"{name}/{MONO_DENS}" in d:
-                solver.set_field(A.PS_FIELD_PHI, i, d[f"{name}/{MONO_DENS}"].reshape(-1))
-        pkey = f"{pressure_field}/{PRES}"
-        solver.set_field(A.PS_FIELD_PRES, 0, d[pkey].reshape(-1) if pkey in d else np.zeros(int(np.prod(shape))))
-        return {"iteration": int(d["iteration"]) if "iteration" in d else 0,
-                "freeEnergy": d["freeEnergy"].copy() if "freeEnergy" in d else None,
-                "cellSizes": tuple(float(v) for v in d["cellSizes"])}
+    returns the dump's metadata (iteration, free-energy history).
+
+    The whole file is read and checked first (grid, dataset shapes, finite
+    values); an unreadable, truncated or mismatched dump raises DumpError and
+    leaves the solver's fields as they were (PsPhysFldFuncs::restore,
+    psphysf/PsPhysFldFuncs.cpp:150-166, reads each dataset of the dump)."""
+    data = _read_dump(path, solver.cfg, pressure_field)
+    for i in range(len(solver.cfg.fields)):
+        solver.set_field(A.PS_FIELD_W, i, data["w"][i])
+        if data["phi"][i] is not None:
+            solver.set_field(A.PS_FIELD_PHI, i, data["phi"][i])
+    solver.set_field(A.PS_FIELD_PRES, 0, data["p"])
+    return data["meta"]

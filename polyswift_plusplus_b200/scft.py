@@ -102,8 +102,11 @@ class ScftSolver:
         self._check(self._lib.ps_gpu_set_fields(self._h, which, index, x.ctypes.data_as(C.c_void_p), 0))
 
     def get_field(self, which: int, index: int = 0, out=None):
-        if out is not None and hasattr(out, "data_ptr"):
-            self._check(self._lib.ps_gpu_get_fields(self._h, which, index, C.c_void_p(out.data_ptr()), 1))
+        if out is not None and hasattr(out, "data_ptr"):  # torch tensor: device or (pinned) host
+            if out.dtype != __import__("torch").float64 or not out.is_contiguous() or out.numel() != self.N:
+                raise ValueError("out must be a contiguous float64 tensor of N values")
+            self._check(self._lib.ps_gpu_get_fields(self._h, which, index, C.c_void_p(out.data_ptr()),
+                                                    1 if out.is_cuda else 0))
             return out
         x = np.empty(self.N, dtype=np.float64) if out is None else out
         self._check(self._lib.ps_gpu_get_fields(self._h, which, index, x.ctypes.data_as(C.c_void_p), 0))
@@ -294,7 +297,10 @@ class ScftBatch:
 
 
 class B200FFT:
-    """PsFFTBase<double,3>::scaledFFTPair plugin (host arrays in and out)."""
+    """PsFFTBase<double,3> plugin (psbase/PsFFTBase.h:40-134): every transform
+    of the interface, host arrays in and out, FFTW-2 c2c semantics on real data
+    (psfft/PsFFTW.cpp:122-297).  Each method returns a new flat array of
+    getFFTSize() doubles."""
 
     def __init__(self, n, device: int = 0):
         self._lib = A.load_library()
@@ -310,16 +316,47 @@ class B200FFT:
         A.check(self._lib.ps_fft_size(self._h, C.byref(v)), fft=True)
         return int(v.value)
 
-    def scaledFFTPair(self, data, kdata) -> np.ndarray:
-        d = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
-        k = np.ascontiguousarray(kdata, dtype=np.float64).reshape(-1)
-        if d.size != self.N or k.size != self.N:
-            raise ValueError("data/kdata size must equal getFFTSize()")
+    def getGrid(self) -> tuple:
+        """The grid extents (PsFFTBase::getGrid reduced to what the transforms use)."""
+        n = (C.c_int * 3)()
+        A.check(self._lib.ps_fft_get_grid(self._h, n), fft=True)
+        return tuple(int(v) for v in n)
+
+    def _flat(self, a, name: str) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if a.size != self.N:
+            raise ValueError(f"{name} size must equal getFFTSize()")
+        return a
+
+    def _call(self, fn: str, *arrays) -> np.ndarray:
         res = np.empty(self.N, dtype=np.float64)
-        A.check(self._lib.ps_fft_scaled_pair(self._h, d.ctypes.data_as(C.c_void_p),
-                                             k.ctypes.data_as(C.c_void_p),
-                                             res.ctypes.data_as(C.c_void_p)), fft=True)
+        ptrs = [a.ctypes.data_as(C.c_void_p) for a in arrays]
+        A.check(getattr(self._lib, fn)(self._h, *ptrs, res.ctypes.data_as(C.c_void_p)), fft=True)
         return res
+
+    def scaledFFTPair(self, data, kdata) -> np.ndarray:
+        """Re(IFFT(kdata * FFT(data)))."""
+        return self._call("ps_fft_scaled_pair", self._flat(data, "data"), self._flat(kdata, "kdata"))
+
+    def scaledFFTPairIm(self, data, kdata) -> np.ndarray:
+        """Re(IFFT(kdata * FFT(i * data))): data is the imaginary part of the input."""
+        return self._call("ps_fft_scaled_pair_im", self._flat(data, "data"), self._flat(kdata, "kdata"))
+
+    def convolveRe(self, data1, data2) -> np.ndarray:
+        """Re(IFFT(FFT(data1) * FFT(data2)))."""
+        return self._call("ps_fft_convolve_re", self._flat(data1, "data1"), self._flat(data2, "data2"))
+
+    def forwardFFTAbs(self, data) -> np.ndarray:
+        """|FFT(data)|^2 elementwise (re^2 + im^2, as the reference computes it)."""
+        return self._call("ps_fft_forward_abs", self._flat(data, "data"))
+
+    def calcForwardFFT(self, data) -> np.ndarray:
+        """Re(FFT(data))."""
+        return self._call("ps_fft_forward", self._flat(data, "data"))
+
+    def calcBackwardFFT(self, data) -> np.ndarray:
+        """Re(IFFT(data)) of real data, unnormalised."""
+        return self._call("ps_fft_backward", self._flat(data, "data"))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

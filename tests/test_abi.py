@@ -27,6 +27,30 @@ def test_header_declares_entry_points():
         assert must in names
 
 
+def test_every_fft_interface_method_is_exported(native_lib):
+    """Each pure virtual of PsFFTBase<T,3> (psbase/PsFFTBase.h:58-134) that
+    computes something has a C-ABI entry point; buildData/buildSolvers map to
+    ps_fft_create.  B200FFT exposes the same method names."""
+    from polyswift_plusplus_b200.scft import B200FFT
+    methods = {
+        "getGrid": "ps_fft_get_grid",
+        "getFFTSize": "ps_fft_size",
+        "forwardFFTAbs": "ps_fft_forward_abs",
+        "convolveRe": "ps_fft_convolve_re",
+        "scaledFFTPair": "ps_fft_scaled_pair",
+        "scaledFFTPairIm": "ps_fft_scaled_pair_im",
+        "calcForwardFFT": "ps_fft_forward",
+        "calcBackwardFFT": "ps_fft_backward",
+        "buildSolvers": "ps_fft_create",
+    }
+    names = declared_functions()
+    for method, sym in methods.items():
+        assert sym in names, sym
+        assert hasattr(native_lib, sym), sym
+        if method != "buildSolvers":
+            assert callable(getattr(B200FFT, method)), method
+
+
 def test_library_exports_every_declared_symbol(native_lib):
     out = subprocess.run(["nm", "-D", "--defined-only", str(A.LIB_PATH)], capture_output=True,
                          text=True, check=True).stdout
@@ -224,6 +248,76 @@ def test_dump_restore_round_trip_on_host(tmp_path):
     for which in a.f:
         for x, y in zip(a.f[which], b.f[which]):
             assert np.array_equal(x, y)
+
+
+def test_bad_dumps_raise_and_leave_the_solver_untouched(tmp_path):
+    """A truncated file, a corrupt byte range, another grid, a missing dataset,
+    a wrongly shaped or non-finite dataset: each raises DumpError before any
+    field is set (the reference's restore reads every dataset it needs,
+    psphysf/PsPhysFldFuncs.cpp:150-166)."""
+    import numpy as np
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.dump import DumpError, dump, restore
+
+    class Stub:
+        def __init__(self, cfg, seed):
+            rng = np.random.default_rng(seed)
+            self.cfg = cfg
+            self.sets = 0
+            self.f = {A.PS_FIELD_W: [rng.standard_normal(cfg.n_total) for _ in cfg.fields],
+                      A.PS_FIELD_PHI: [rng.random(cfg.n_total) for _ in cfg.fields],
+                      A.PS_FIELD_PRES: [rng.standard_normal(cfg.n_total)]}
+
+        def w(self, i): return self.f[A.PS_FIELD_W][i]
+        def phi(self, i): return self.f[A.PS_FIELD_PHI][i]
+        def pressure(self): return self.f[A.PS_FIELD_PRES][0]
+        def scalars(self): return {"iteration": 7}
+
+        def set_field(self, which, i, x):
+            self.sets += 1
+            self.f[which][i] = np.array(x)
+
+    cfg, _ = W.diblock32(n=8)
+    good = dump(Stub(cfg, 1), tmp_path / "good.npz")
+    raw = good.read_bytes()
+    bad = {}
+    bad["truncated"] = tmp_path / "trunc.npz"
+    bad["truncated"].write_bytes(raw[: len(raw) // 2])
+    bad["corrupt"] = tmp_path / "corrupt.npz"
+    bad["corrupt"].write_bytes(raw[:200] + bytes(1000) + raw[1200:])
+    bad["empty"] = tmp_path / "empty.npz"
+    bad["empty"].write_bytes(b"")
+    cfg16, _ = W.diblock32(n=16)
+    bad["grid"] = dump(Stub(cfg16, 2), tmp_path / "grid.npz")
+    with np.load(good) as d:
+        items = {k: d[k] for k in d.files}
+    drop = dict(items)
+    del drop["B/ConjugateDensity"]
+    bad["missing"] = tmp_path / "missing.npz"
+    np.savez(bad["missing"], **drop)
+    shaped = dict(items)
+    shaped["B/ConjugateDensity"] = shaped["B/ConjugateDensity"][:4]
+    bad["shape"] = tmp_path / "shape.npz"
+    np.savez(bad["shape"], **shaped)
+    nonfin = dict(items)
+    nonfin["defaultPressure/PressureField"] = nonfin["defaultPressure/PressureField"].copy()
+    nonfin["defaultPressure/PressureField"][1, 2, 3] = np.nan
+    bad["nan"] = tmp_path / "nan.npz"
+    np.savez(bad["nan"], **nonfin)
+    bad["absent"] = tmp_path / "no_such_file.npz"
+
+    target = Stub(cfg, 3)
+    before = {k: [x.copy() for x in v] for k, v in target.f.items()}
+    for name, path in bad.items():
+        with pytest.raises(DumpError):
+            restore(target, path)
+        assert target.sets == 0, name
+    for which in before:
+        for x, y in zip(before[which], target.f[which]):
+            assert np.array_equal(x, y)
+    restore(target, good)  # the same target still takes a good dump
+    assert target.sets == 2 * len(cfg.fields) + 1
 
 
 _SPEC_FILTER_DECK = """

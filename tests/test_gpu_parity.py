@@ -64,6 +64,57 @@ def test_fft_plugin_matches_oracle(gpu, oracle_lib, shape):
     assert rel(got, ref) < 1e-12
 
 
+@pytest.mark.parametrize("shape", [(8, 8, 8), (12, 16, 24), (32, 32, 32), (24, 48, 48),
+                                   (16, 64, 1), (8, 4, 256), (1, 16, 32), (64, 1, 1),
+                                   (64, 64, 64), (128, 128, 128)])
+def test_fft_plugin_interface_matches_oracle(gpu, oracle_lib, shape):
+    """Every other transform of PsFFTBase<double,3> (psbase/PsFFTBase.h:83-134):
+    scaledFFTPairIm, convolveRe, forwardFFTAbs, calcForwardFFT and
+    calcBackwardFFT against the oracle's c2c restatement of PsFFTW, on fused
+    planes, row-pass grids (256-point z rows) and degenerate axes."""
+    rng = np.random.default_rng(11)
+    d = rng.standard_normal(shape)
+    d2 = rng.standard_normal(shape)
+    k = rng.standard_normal(shape)  # no symmetry: the odd part drives scaledFFTPairIm
+    f = B200FFT(shape)
+    assert f.getGrid() == tuple(shape)
+    r = lambda a: a.reshape(shape)
+    assert rel(r(f.scaledFFTPairIm(d, k)), O.scaled_fft_pair_im(d, k)) < 1e-12
+    assert rel(r(f.convolveRe(d, d2)), O.convolve_re(d, d2)) < 1e-12
+    assert rel(r(f.forwardFFTAbs(d)), O.forward_fft_abs(d)) < 1e-12
+    assert rel(r(f.calcForwardFFT(d)), O.calc_forward_fft(d)) < 1e-12
+    assert rel(r(f.calcBackwardFFT(d)), O.calc_backward_fft(d)) < 1e-12
+    # the handle's buffers are reused: a second call with other inputs
+    assert rel(r(f.convolveRe(d2, k)), O.convolve_re(d2, k)) < 1e-12
+    assert rel(r(f.scaledFFTPair(d, k)), O.scaled_fft_pair(d, k)) < 1e-12
+    f.close()
+
+
+def test_fft_plugin_interface_known_answers(gpu):
+    """Known answers independent of the oracle: the transforms of a single
+    cosine mode and a delta function."""
+    n = (16, 8, 12)
+    N = n[0] * n[1] * n[2]
+    x, y, z = np.meshgrid(*[np.arange(v) for v in n], indexing="ij")
+    c = np.cos(2 * np.pi * (2 * x / n[0] + 3 * z / n[2]))
+    f = B200FFT(n)
+    pw = f.forwardFFTAbs(c).reshape(n)
+    exp = np.zeros(n)
+    exp[2, 0, 3] = exp[-2, 0, -3] = (N / 2) ** 2
+    assert np.abs(pw - exp).max() < 1e-9 * N * N
+    delta = np.zeros(n)
+    delta[0, 0, 0] = 1.0
+    # FFT of a delta at the origin is 1 everywhere; convolving with it is the identity
+    assert np.abs(f.calcForwardFFT(delta) - 1.0).max() < 1e-14
+    assert np.abs(f.convolveRe(c, delta).reshape(n) - c).max() < 1e-12
+    # scaledFFTPairIm with an odd kdata i*sign(kx): a Hilbert-like transform of the cosine
+    kx = np.fft.fftfreq(n[0])[:, None, None] * np.ones(n)
+    res = f.scaledFFTPairIm(c, np.sign(kx)).reshape(n)
+    ref = np.fft.ifftn(np.fft.fftn(1j * c) * np.sign(kx)).real * N
+    assert np.abs(res - ref).max() < 1e-10
+    f.close()
+
+
 @pytest.mark.parametrize("shape", [(1, 16, 32), (16, 1, 32), (64, 1, 1), (1, 1, 64), (1, 64, 1)])
 def test_fft_plugin_degenerate_axes(gpu, oracle_lib, shape):
     """Grids with extent-1 axes (1-D and 2-D runs in any orientation)."""

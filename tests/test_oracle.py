@@ -44,6 +44,25 @@ def test_scaled_fft_pair_matches_numpy(oracle_lib):
     assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
 
 
+def test_other_fft_operations_match_numpy(oracle_lib):
+    """forwardFFTAbs, convolveRe, scaledFFTPairIm, calcForwardFFT and
+    calcBackwardFFT as numpy computes them from full complex transforms."""
+    rng = np.random.default_rng(3)
+    d = rng.standard_normal((8, 12, 16))
+    d2 = rng.standard_normal((8, 12, 16))
+    k = rng.standard_normal((8, 12, 16))
+    N = d.size
+
+    def close(got, ref, tol=1e-13):
+        assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+
+    close(O.forward_fft_abs(d), np.abs(np.fft.fftn(d)) ** 2)
+    close(O.convolve_re(d, d2), np.fft.ifftn(np.fft.fftn(d) * np.fft.fftn(d2)).real * N)
+    close(O.scaled_fft_pair_im(d, k), np.fft.ifftn(np.fft.fftn(1j * d) * k).real * N)
+    close(O.calc_forward_fft(d), np.fft.fftn(d).real)
+    close(O.calc_backward_fft(d), np.fft.ifftn(d).real * N)
+
+
 @pytest.mark.parametrize("name", ["diblock8", "triblock8", "blend8"])
 def test_oracle_matches_golden(oracle_lib, name):
     import sys
