@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched blend workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--batch128", type=int, default=4,
+                    help="instances of the 128^3 mixed workload run as one batch (0 = skip)")
     ap.add_argument("--no-cufft", dest="cufft", action="store_false",
                     help="skip the cuFFT (torch.fft) comparison of the propagator step")
     ap.add_argument("--variant", type=int, default=-1,
@@ -381,6 +383,48 @@ def batched_rate(count: int, steps: int, device: int) -> dict:
             "class_variants": variants, "launches_per_iteration": launches}
 
 
+def batched128_rate(count: int, steps: int, device: int) -> dict:
+    """`count` seeded instances of the 128^3 Ns=200 mixed workload as one batch
+    (the mixed-precision batched path: every instance's sweeps in the same
+    launches, one graph per iteration); aggregate instance-iterations/s after
+    each instance's Anderson history has filled."""
+    import torch
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftBatch
+    cfgs, fields = [], []
+    for i in range(count):
+        cfg, _ = W.diblock128(precision="mixed")
+        cfg.seed = 38383 + i
+        cfg.device = device
+        hx = W.hex_seed(cfg)
+        r = W.random_fields(cfg, 0.05)
+        cfgs.append(cfg)
+        fields.append([r[0] + hx, r[1] - hx])
+    b = ScftBatch(cfgs)
+    for i, w in enumerate(fields):
+        b.instance(i).restore(w)
+    u = cfgs[0].updater
+    b.update(u.anderson_start + u.anderson_depth + 3)
+    st = torch.cuda.ExternalStream(b.stream_ptr, device=torch.device("cuda", device))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    b.update(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, variants = b.classes()
+    launches = b.launches_per_iteration
+    fe = [sc["free_energy"] for sc in b.scalars()]
+    b.close()
+    return {"workload": f"{count} seeded instances of diblock128 (seeds 38383..{38383 + count - 1}), "
+                        "FP32 sweeps, FP64 Q/F/quadrature/Anderson, as one batch",
+            "value": count * steps / (ms / 1000.0), "unit": "instance-iter/s", "steps": steps,
+            "class_variants": variants, "launches_per_iteration": launches,
+            "free_energy": fe}
+
+
 def run_reference(args, world, rank):
     """The reference's CPU path: its C restatement (the reference itself cannot be
     built), one full FP64 iteration of the same workload per timed step."""
@@ -589,6 +633,11 @@ def run_ours(args, world, rank, local):
         out["mixed_over_fp64"] = value / out["fp64_path"]["value"]
     if rank == 0 and world == 1 and args.batch_instances > 0:
         out["batched"] = batched_rate(args.batch_instances, args.batch_steps, local)
+    if rank == 0 and world == 1 and args.precision == "mixed" and args.batch128 > 0:
+        out["batched128"] = batched128_rate(args.batch128, args.batch_steps, local)
+        if "fp64_path" in out:
+            out["batched128"]["over_fp64_path"] = (out["batched128"]["value"] /
+                                                   out["fp64_path"]["value"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_full_iteration(args.n)
     if rank == 0:

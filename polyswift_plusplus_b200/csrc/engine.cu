@@ -10,6 +10,7 @@
 // reset, PsBlockCopolymer::update for each polymer, then the updater with F
 // evaluated on the updated w (pseffhamil/PsSteepDUpdater.cpp:200-201).
 #include <math.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -245,6 +246,13 @@ static double kcomp(int i, int n, double dx) {
   return k / dx;
 }
 
+// The FP32 sweeps carry their mean mode in FP64 (PlaneWork in kernels.h) unless
+// the environment sets PSB_DC_CARRY=0 (kept to measure what the carry buys).
+static bool dc_carry_enabled() {
+  const char* e = getenv("PSB_DC_CARRY");
+  return !(e && e[0] == '0');
+}
+
 template <typename T>
 static int build_device_tables(ps_handle* h) {
   Buffers<T>& B = bufs<T>(h);
@@ -268,6 +276,18 @@ static int build_device_tables(ps_handle* h) {
     T* jb = nullptr;
     PS_CUDA(h, cudaMalloc((void**)&jb, sizeof(T) * (size_t)N));
     B.jbuf.push_back(jb);
+  }
+  // Mean-mode carry of the FP32 sweeps: one buffer per executed sweep, room for
+  // a partial per CTA of any plane/row pass variant (fused plane: nx, cluster:
+  // 2 nx, row passes: at least 8 rows per CTA).
+  if (sizeof(T) == 4 && dc_carry_enabled()) {
+    B.dc_cap = std::max(kDcMinSlots, std::max(2 * h->n[0], (h->n[0] * h->n[1] + 7) / 8));
+    for (size_t e = 0; e < h->exec.size(); ++e) {
+      double* d = nullptr;
+      PS_CUDA(h, cudaMalloc((void**)&d, sizeof(double) * (size_t)(B.dc_cap + 2)));
+      B.dcbuf.push_back(d);
+      PS_CUDA(h, cudaMemset(d, 0, sizeof(double) * (size_t)(B.dc_cap + 2)));
+    }
   }
   for (auto& kk : h->ktab_keys) {
     const double ds = kk.first, b = kk.second;
@@ -337,6 +357,14 @@ static int build_device_tables(ps_handle* h) {
       w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
       w.store = B.slices[e] ? B.slices[e] + (size_t)k * N : nullptr;
       w.status = &h->d_sc->error_flags;
+      double* dc = B.dcbuf.empty() ? nullptr : B.dcbuf[e];
+      if (dc) {
+        if (w.mode != MODE_FIRST) w.dc_in = dc + B.dc_cap;
+        if (w.mode != MODE_LAST) {
+          w.dc_out = dc;
+          w.dc_count = dc + B.dc_cap + 1;
+        }
+      }
       pw.push_back(w);
       if (k < sw.total) {
         PencilWork<T> x;
@@ -344,6 +372,12 @@ static int build_device_tables(ps_handle* h) {
         x.spec = B.spec[e];
         x.kx = B.kx[seg_of(sw, k).ktab_id];
         x.kyz = B.kyz[seg_of(sw, k).ktab_id];
+        if (dc) {
+          x.dc_parts = dc;
+          x.dc_count = dc + B.dc_cap + 1;
+          x.dc_total = dc + B.dc_cap;
+          x.dc_scale = 1.0 / (double)N;
+        }
         xw.push_back(x);
       }
     }
@@ -609,6 +643,7 @@ template <typename T> static void free_buffers(Buffers<T>& B) {
   for (auto p : B.spec) f(p);
   for (auto p : B.wfac) f(p);
   for (auto p : B.jbuf) f(p);
+  for (auto p : B.dcbuf) f(p);
   for (auto p : B.kx) f(p);
   for (auto p : B.kyz) f(p);
   f(B.tw_x); f(B.tw_y); f(B.tw_z); f(B.tw_zh); f(B.d_plane); f(B.d_pencil);

@@ -272,7 +272,9 @@ __device__ __forceinline__ void smem_fft_tail(C* buf, int bs, int is, const C* t
 // elementwise operation in registers, and the first pass (radix R, NS = 1) of
 // an FFT in direction INV_B, as one shared-memory round trip.  With the same
 // radix both passes give a thread's butterfly j the elements j + r*L/R.
-// op(b, j, v) receives pencil b's values v[r] at natural positions j + r*L/R.
+// op.apply(b, j, v) receives pencil b's values v[r] at natural positions
+// j + r*L/R; op.after(b, s) then receives output 0 of the second DFT (the sum
+// of the values apply left).
 template <int L, int R, int B, int T, bool INV_A, bool INV_B, bool BFAST, typename C, typename OP>
 __device__ __forceinline__ void fused_pass_pair(C* buf, int bs, int is, const C* tw, OP& op) {
   constexpr int M = L / R;
@@ -307,6 +309,7 @@ __device__ __forceinline__ void fused_pass_pair(C* buf, int bs, int is, const C*
       Dft<R, INV_A, C>::run(v[u]);
       op.apply(b, j, v[u]);
       Dft<R, INV_B, C>::run(v[u]);
+      op.after(b, v[u][0]);  // output 0 of the second DFT: the sum of its inputs
       C* base = buf + b * bs;
 #pragma unroll
       for (int r = 0; r < R; ++r) base[(j * R + r) * is] = v[u][r];

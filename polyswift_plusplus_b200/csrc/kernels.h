@@ -11,6 +11,20 @@ namespace psb {
 // One propagator step of one sweep, real-space side (see prop_kernels.cu).
 enum { MODE_FIRST = 0, MODE_MID = 1, MODE_LAST = 2 };
 
+// Mean-mode carry (FP32 sweeps).  The k = 0 coefficient of each step's
+// transform is a sum over all N points; summed by the FP32 FFT its rounding is
+// the same for every point and accumulates over the sweep (about 1e-6 in Q
+// after 200 steps at 128^3).  With the carry the plane/row pass also sums its
+// forward input (one FP64 partial per CTA in dc_out[blockIdx.x], the count
+// gridDim.x in *dc_count); the x pencil pass (or the x-y pass) drops the FP32
+// k = 0 coefficient, and one warp of its first CTA writes the FP64 mean
+// (sum of the partials) * dc_scale (= 1/N) to dc_total; the next plane/row
+// pass adds that value to every point of its inverse transform (dc_in) as a
+// two-float sum, so its rounding differs from point to point.  The partials
+// buffer holds at least kDcMinSlots slots.  nullptr: no carry (FP64 sweeps,
+// the plugins).
+constexpr int kDcMinSlots = 128;
+
 template <typename T> struct PlaneWork {
   const T* src;       // MODE_FIRST: initial q (nullptr = ones)
   c2_t<T>* spec;      // half spectrum [nx][ny][nz/2+1]
@@ -20,6 +34,9 @@ template <typename T> struct PlaneWork {
   int* status;        // error word: bit 2 set when a bulk copy did not land in time
   int mode;
   int pad;
+  const double* dc_in;  // MID/LAST: the mean-mode value added after the inverse transform
+  double* dc_out;       // FIRST/MID: per-CTA FP64 sums of the forward input, [blockIdx.x]
+  double* dc_count;     // FIRST/MID: CTA 0 writes the number of partials (gridDim.x)
 };
 
 // Pencil pass along a strided axis of the half spectrum.
@@ -39,6 +56,10 @@ template <typename T> struct PencilWork {
   const T* kyz;       // PENCIL_KINV: factor per (y, kz) column
   const double* kfull;// PENCIL_KFULL(_IM): full real k array [nx][ny][nz] (plugin path)
   const c2_t<T>* kspec;// PENCIL_KSPEC: a second, fully transformed half spectrum (same layout)
+  const double* dc_parts;  // PENCIL_KINV / x-y pass: the plane pass's dc_out (mean-mode carry)
+  const double* dc_count;  // ... its number of partials
+  double* dc_total;        // ... and where the FP64 mean goes
+  double dc_scale;         // 1 / N
 };
 
 bool extent_supported(int n);

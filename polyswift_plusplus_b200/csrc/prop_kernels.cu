@@ -35,6 +35,91 @@ __device__ __forceinline__ T ld_or_one(const T* p, size_t i) {
   return p ? __ldg(p + i) : T(1);
 }
 
+// ---------------------------------------------------------------------------
+// Mean-mode carry (see PlaneWork in kernels.h).
+// ---------------------------------------------------------------------------
+// Per-warp FP64 sums of the forward input, summed into one CTA partial.
+__shared__ double s_dc_warp[32];
+// The mean-mode value of the inverse transform as (hi, lo) of T; written by
+// thread 0 after pdl_wait(), read after the barriers that precede the inverse
+// step (kept in shared memory, not in registers, through the FFT passes).
+__shared__ __align__(16) double s_dc_hilo[2];
+
+template <typename T>
+__device__ __forceinline__ void dc_hilo_store(const double* dc_in) {
+  if (threadIdx.x == 0 && dc_in) {
+    const double d = *dc_in;
+    const T hi = T(d);
+    reinterpret_cast<T*>(s_dc_hilo)[0] = hi;
+    reinterpret_cast<T*>(s_dc_hilo)[1] = T(d - (double)hi);
+  }
+}
+
+// x + mean-mode value, as (x + hi) + lo
+template <typename T>
+__device__ __forceinline__ c2_t<T> dc_add2(c2_t<T> x) {
+  const c2_t<T> hl = *reinterpret_cast<const c2_t<T>*>(s_dc_hilo);
+  return cadd(cadd(x, c2_t<T>{hl.x, hl.x}), c2_t<T>{hl.y, hl.y});
+}
+template <typename T>
+__device__ __forceinline__ T dc_add(T x) {
+  const T* hl = reinterpret_cast<const T*>(s_dc_hilo);
+  return (x + hl[0]) + hl[1];
+}
+
+// Every thread of the CTA calls this (CTA-uniform): lane 0 keeps its warp's sum.
+__device__ __forceinline__ void dc_warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) s_dc_warp[threadIdx.x >> 5] = v;
+}
+
+// After a __syncthreads() that follows dc_warp_sum: thread 0 stores the CTA's
+// partial (warps in order) and CTA 0 the number of partials.  The pointers are
+// read from the descriptor here, not kept in registers through the kernel.
+template <typename T>
+__device__ __forceinline__ void dc_cta_store(const PlaneWork<T>* wp) {
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += s_dc_warp[i];
+    double* out = reinterpret_cast<double*>(
+        __ldg(reinterpret_cast<const unsigned long long*>(&wp->dc_out)));
+    out[blockIdx.x] = s;
+    if (blockIdx.x == 0) {
+      double* cnt = reinterpret_cast<double*>(
+          __ldg(reinterpret_cast<const unsigned long long*>(&wp->dc_count)));
+      *cnt = (double)gridDim.x;
+    }
+  }
+}
+
+// Spectral pass side: one warp sums the plane pass's partials in a fixed order
+// (lane l takes slots l, l + 32, ...; then a butterfly) and stores the mean.
+// load() issues the count and the first kDcMinSlots slots (before the count is
+// known) so that they travel with the tile loads; finish() sums them.
+template <typename T> struct DcFinish {
+  double cnt;
+  double v[kDcMinSlots / 32];
+  __device__ __forceinline__ void load(const PencilWork<T>& w) {
+    const int lane = threadIdx.x & 31;
+    cnt = *w.dc_count;
+#pragma unroll
+    for (int k = 0; k < kDcMinSlots / 32; ++k) v[k] = w.dc_parts[lane + 32 * k];
+  }
+  __device__ __forceinline__ void finish(const PencilWork<T>& w) const {
+    const int lane = threadIdx.x & 31;
+    const int n = (int)cnt;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kDcMinSlots / 32; ++k)
+      if (lane + 32 * k < n) s += v[k];
+    for (int i = kDcMinSlots + lane; i < n; i += 32) s += w.dc_parts[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) *w.dc_total = s * w.dc_scale;
+  }
+};
+
 // 16-byte vector of T: 4 floats or 2 doubles.
 template <typename T> struct Vec16;
 template <> struct Vec16<float> {
@@ -335,6 +420,9 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
     const bool need_in = (w.mode != MODE_FIRST) && w.wfac_in;
     const bool need_out = (w.mode != MODE_LAST) && w.wfac_out && !(w.mode == MODE_MID && same);
     const bool need_src = (w.mode == MODE_FIRST) && w.src;
+    const bool dc_in = (w.mode != MODE_FIRST) && w.dc_in;
+    const bool dc_sum = (w.mode != MODE_LAST) && w.dc_out;
+    T acc = T(0);
 #pragma unroll 1
     for (int u0 = 0; u0 < U; u0 += UC) {
       V a[UC], b[UC];
@@ -363,7 +451,11 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
         for (int i = 0; i < VN; ++i) {
           T v;
           if (w.mode == MODE_FIRST) v = need_src ? vget<V, T>(a[c], i) : T(1);
-          else v = vget<V, T>(cur, i) * (need_in ? vget<V, T>(a[c], i) : T(1));
+          else {
+            T x = vget<V, T>(cur, i);
+            if (dc_in) x = dc_add(x);
+            v = x * (need_in ? vget<V, T>(a[c], i) : T(1));
+          }
           vset(q, i, v);
         }
         if (w.store) *reinterpret_cast<V*>(w.store + gi) = q;
@@ -375,12 +467,16 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
             if (need_out) f = vget<V, T>(b[c], i);
             else if (w.mode == MODE_MID && same && need_in) f = vget<V, T>(a[c], i);
             vset(o, i, vget<V, T>(q, i) * f);
+            acc += vget<V, T>(o, i);
           }
           *sp = o;
         }
       }
     }
+    if (dc_sum) dc_warp_sum((double)acc);
   } else {
+    const bool dc_in = (w.mode != MODE_FIRST) && w.dc_in;
+    T acc = T(0);
     for (int e = threadIdx.x; e < ROWS * NZ; e += TH) {
       const int r = e / NZ;
       const int z = e - r * NZ;
@@ -388,10 +484,15 @@ __device__ __forceinline__ void real_space(const PlaneWork<T>& w, T* rbuf, size_
       const size_t g = roff + (size_t)e;
       T q;
       if (w.mode == MODE_FIRST) q = w.src ? w.src[g] : T(1);
-      else q = rbuf[r * RS + z] * ld_or_one(w.wfac_in, g);
+      else q = (dc_in ? dc_add(rbuf[r * RS + z]) : rbuf[r * RS + z]) * ld_or_one(w.wfac_in, g);
       if (w.store) w.store[g] = q;
-      if (w.mode != MODE_LAST) rbuf[r * RS + z] = q * ld_or_one(w.wfac_out, g);
+      if (w.mode != MODE_LAST) {
+        const T o = q * ld_or_one(w.wfac_out, g);
+        rbuf[r * RS + z] = o;
+        acc += o;
+      }
     }
+    if ((w.mode != MODE_LAST) && w.dc_out) dc_warp_sum((double)acc);
   }
 }
 
@@ -406,6 +507,8 @@ struct RealStepOp {
   T* store;
   size_t roff;
   int rows;
+  bool dc_on = false;  // add the mean-mode value (s_dc_hilo) after the inverse transform
+  T acc = T(0);        // sum of the forward input (mean-mode carry)
   T2 wf[R];
   __device__ __forceinline__ void prefetch(int b, int j) {
     if (b >= rows) return;
@@ -418,11 +521,17 @@ struct RealStepOp {
     T* st = store + roff + (size_t)b * NZ;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const T q0 = v[r].x * wf[r].x;
-      const T q1 = v[r].y * wf[r].y;
+      const T2 x = dc_on ? dc_add2<T>(v[r]) : v[r];
+      const T q0 = x.x * wf[r].x;
+      const T q1 = x.y * wf[r].y;
       *reinterpret_cast<T2*>(st + 2 * (j + r * M)) = T2{q0, q1};
       v[r] = T2{q0 * wf[r].x, q1 * wf[r].y};
     }
+  }
+  // s = the sum of this butterfly's forward inputs (a local FP32 sum: its
+  // rounding differs from butterfly to butterfly)
+  __device__ __forceinline__ void after(int b, T2 s) {
+    if (b < rows) acc += s.x + s.y;
   }
 };
 
@@ -464,6 +573,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
   const size_t roff = (size_t)row0 * NZ;
   const size_t soff = (size_t)row0 * NZH;
   const bool load_spec = (w.mode != MODE_FIRST);
+  const bool dc_sum = (w.mode != MODE_LAST) && (w.dc_out != nullptr);  // mean-mode carry
 
   if (BULK && load_spec && tid == 0) {
     pdl_wait();
@@ -480,6 +590,7 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
     for (int i = tid; i < ROWS; i += TH) s_tw_y[i] = tw_y[i];
   }
   pdl_wait();  // before any read of the spectrum, src or wfac, and any write
+  if (load_spec) dc_hilo_store<T>(w.dc_in);  // used after the barriers below
 
   if (load_spec) {
     if constexpr (BULK) {
@@ -530,7 +641,9 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
           op.store = w.store;
           op.roff = roff;
           op.rows = rows;
+          op.dc_on = (w.dc_in != nullptr);
           fused_pass_pair<H, 8, ROWS, TH, true, false, false>(buf, NZH, 1, s_tw_zh, op);
+          if (dc_sum) dc_warp_sum((double)op.acc);
           z64_forward_last<ROWS, TH>(buf, s_tw_zh, s_tw_z);
           goto forward_y;
         }
@@ -547,7 +660,9 @@ __global__ void __launch_bounds__(TH, (PlaneMinBlocks<T, TH>::v))
         op.store = w.store;
         op.roff = roff;
         op.rows = rows;
+        op.dc_on = (w.dc_in != nullptr);
         fused_pass_pair<H, RF, ROWS, TH, true, false, true>(buf, NZH, 1, s_tw_zh, op);
+        if (dc_sum) dc_warp_sum((double)op.acc);
         smem_fft_tail<H, PF, ROWS, TH, false, true>(buf, NZH, 1, s_tw_zh);
         r2c_post<NZ, ROWS, TH>(buf, s_tw_z, rows);
         __syncthreads();
@@ -605,6 +720,8 @@ forward_y:
       }
     }
   }
+  // the warps' sums were stored before at least one barrier on every path above
+  if (dc_sum) dc_cta_store(works + blockIdx.y);
 }
 
 // k2 multiply applied inside the fused x pass: exp(-ds b^2 k^2)/N as the
@@ -617,6 +734,7 @@ struct KStepOp {
   const T* kyz;
   int c0;
   int inner;
+  bool dc0;  // this tile holds the k = 0 coefficient and the mean mode is carried in FP64
   T fyz;
   __device__ __forceinline__ void prefetch(int b, int j) {
     const int c = c0 + b;
@@ -628,7 +746,9 @@ struct KStepOp {
       const T f = __ldg(kx + j + r * M) * fyz;
       v[r] = T2{v[r].x * f, v[r].y * f};
     }
+    if (dc0 && b == 0 && j == 0) v[0] = T2{T(0), T(0)};
   }
+  __device__ __forceinline__ void after(int, T2) {}
 };
 
 // ---------------------------------------------------------------------------
@@ -655,8 +775,13 @@ __global__ void __launch_bounds__(TH)
   const int c0 = (blockIdx.x - o * tiles) * TK;
   C* base = w.spec + (size_t)o * L * inner;
   const bool full = (c0 + TK <= inner) && (inner % CPV == 0);
+  // mean-mode carry: the tile of column 0 drops the FP32 k = 0 coefficient and
+  // its first warp turns the plane pass's FP64 partials into the mean
+  const bool dc0 = (MODE == PENCIL_KINV) && w.dc_total && o == 0 && c0 == 0;
   for (int i = tid; i < L; i += TH) s_tw[i] = tw[i];
   pdl_wait();  // before any read or write of the spectrum
+  DcFinish<T> dcf;
+  if (dc0 && tid < 32) dcf.load(w);
   if (full) {
     V v[UV];
 #pragma unroll
@@ -681,6 +806,7 @@ __global__ void __launch_bounds__(TH)
       buf[e] = (c < inner) ? base[(size_t)i * inner + c] : C{T(0), T(0)};
     }
   }
+  if (dc0 && tid < 32) dcf.finish(w);
   __syncthreads();
   if constexpr (MODE == PENCIL_KINV && L > 1 && FK) {
     // forward FFT, k2 multiply and inverse FFT with the last forward pass, the
@@ -693,6 +819,7 @@ __global__ void __launch_bounds__(TH)
     op.kyz = w.kyz;
     op.c0 = c0;
     op.inner = inner;
+    op.dc0 = dc0;
     fused_pass_pair<L, RF, TK, TH, false, true, true>(buf, 1, TK, s_tw, op);
     smem_fft_tail<L, RI, TK, TH, true, true>(buf, 1, TK, s_tw);
     goto store_tile;
@@ -706,7 +833,7 @@ __global__ void __launch_bounds__(TH)
       if (c < inner) {
         const T f = __ldg(w.kx + i) * __ldg(w.kyz + c);
         const C v = buf[e];
-        buf[e] = {v.x * f, v.y * f};
+        buf[e] = (dc0 && e == 0) ? C{T(0), T(0)} : C{v.x * f, v.y * f};
       }
     }
     __syncthreads();
@@ -947,6 +1074,7 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
   for (int i = tid; i < NZ; i += TH) s_tw_z[i] = tw_z[i];
   for (int i = tid; i < NY; i += TH) s_tw_y[i] = tw_y[i];
   pdl_wait();  // before any read of the spectrum, src or wfac, and any write
+  if (w.mode != MODE_FIRST) dc_hilo_store<T>(w.dc_in);  // used after the barriers below
 
   if (w.mode != MODE_FIRST) {
     // this CTA's columns of the half plane, Y layout; every load issued before
@@ -1072,6 +1200,8 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
   }
   if (me == 0)
     for (int y = tid; y < NY; y += TH) dst[(size_t)y * NZH + NZ / 2] = buf[y * YS + CH];
+  // mean-mode carry: a partial per CTA (two per plane), after the barriers above
+  if (w.dc_out) dc_cta_store(works + blockIdx.y);
 }
 
 cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, int nx, const float2* tw_y,
@@ -1185,6 +1315,7 @@ struct XYKOp {
   const T* kyz;
   int kz;
   int nzh;
+  bool dc0;  // kz = 0 plane with the mean mode carried in FP64
   T fyz;
   __device__ __forceinline__ void prefetch(int y, int j) { fyz = __ldg(kyz + (size_t)y * nzh + kz); }
   __device__ __forceinline__ void apply(int y, int j, T2 (&v)[R]) {
@@ -1193,7 +1324,9 @@ struct XYKOp {
       const T f = __ldg(kx + j + r * M) * fyz;
       v[r] = T2{v[r].x * f, v[r].y * f};
     }
+    if (dc0 && y == 0 && j == 0) v[0] = T2{T(0), T(0)};
   }
+  __device__ __forceinline__ void after(int, T2) {}
 };
 
 template <typename T, int NXY, int TH, bool FK>
@@ -1214,8 +1347,11 @@ __global__ void __launch_bounds__(TH)
   const int kz = blockIdx.x;
   const int tid = threadIdx.x;
   C* base = w.spec + (size_t)kz * NE;
+  const bool dc0 = w.dc_total && kz == 0;  // mean-mode carry (see the pencil pass)
   for (int i = tid; i < NXY; i += TH) s_tw[i] = tw[i];
   pdl_wait();  // before any read or write of the spectrum
+  DcFinish<T> dcf;
+  if (dc0 && tid < 32) dcf.load(w);
   {
     V v[UV];
 #pragma unroll
@@ -1236,6 +1372,7 @@ __global__ void __launch_bounds__(TH)
       }
     }
   }
+  if (dc0 && tid < 32) dcf.finish(w);
   __syncthreads();
   smem_fft<NXY, NXY, TH, false, true, C, RL>(buf, NP, 1, s_tw);  // y, rows x
   if constexpr (FK && NXY > 1) {
@@ -1247,6 +1384,7 @@ __global__ void __launch_bounds__(TH)
     op.kyz = w.kyz;
     op.kz = kz;
     op.nzh = nzh;
+    op.dc0 = dc0;
     fused_pass_pair<NXY, RF, NXY, TH, false, true, true>(buf, 1, NP, s_tw, op);
     smem_fft_tail<NXY, RI, NXY, TH, true, true>(buf, 1, NP, s_tw);
   } else {
@@ -1256,7 +1394,7 @@ __global__ void __launch_bounds__(TH)
       const int y = e - x * NXY;
       const T f = __ldg(w.kx + x) * __ldg(w.kyz + (size_t)y * nzh + kz);
       const C v = buf[x * NP + y];
-      buf[x * NP + y] = C{v.x * f, v.y * f};
+      buf[x * NP + y] = (dc0 && e == 0) ? C{T(0), T(0)} : C{v.x * f, v.y * f};
     }
     __syncthreads();
     smem_fft<NXY, NXY, TH, true, true, C, RL>(buf, 1, NP, s_tw);

@@ -99,3 +99,31 @@ def test_diblock128_full_size_mixed_variant11(gpu, diblock128_oracle):
         assert np.abs(g.phi(i) - ref["phi"][i]).max() < 1e-4
         assert rel(g.w(i), ref["w_out"][i]) < 1e-5
     g.close()
+
+
+def test_mean_mode_carry_reduces_fp32_error(gpu):
+    """FP32 sweeps carry the k = 0 coefficient of every step in FP64 (PlaneWork's
+    mean-mode carry).  At full size, Q of the FP32 sweeps must be closer to the
+    FP64 device path's with the carry than without it, and within 2e-7."""
+    import os
+    cfg64, w = W.diblock128(precision="fp64")
+    g = ScftSolver(cfg64)
+    g.restore(w)
+    g.update(1)
+    q64 = g.scalars()["q"][0]
+    g.close()
+    errs = {}
+    for carry in ("1", "0"):
+        os.environ["PSB_DC_CARRY"] = carry
+        try:
+            cfg, _ = W.diblock128(precision="mixed")
+            m = ScftSolver(cfg)
+            m.set_variant(11)
+            m.restore(w)
+            m.update(1)
+            errs[carry] = abs(m.scalars()["q"][0] - q64) / q64
+            m.close()
+        finally:
+            os.environ.pop("PSB_DC_CARRY", None)
+    assert errs["1"] < 2e-7, errs
+    assert errs["1"] < errs["0"], errs
