@@ -279,10 +279,12 @@ void* ps_gpu_stream(const ps_handle* h);
  * instance's sweeps share launches or run as concurrent launch chains
  * (bit 3).  variant = -1 (the default) times all variants on the handle's
  * own sweeps before its first captured iteration and keeps the fastest;
- * 0..31 forces one.  A handle with a branched polymer runs its sweeps
- * as dependent launch chains (a sweep that starts at a junction waits for the
- * sweeps arriving there), so it takes only variants with bit 3 (PS_ATTRIB_ERR
- * otherwise).
+ * 0..31 forces one.  Branched polymers take every variant: with bit 3 a
+ * sweep that starts at a junction is a launch chain that waits for the chains
+ * arriving there; without it, all sweeps share launches step by step and a
+ * sweep leaving a junction starts one step after the last arriving sweep
+ * ends, its junction product launched in between (so branched polymers also
+ * run in batches).
  * ps_gpu_get_variant also returns the measured sweep time of each variant (ms). */
 int ps_gpu_set_variant(ps_handle* h, int variant);
 int ps_gpu_get_variant(const ps_handle* h, int* variant, float* tune_ms, int n_tune);
@@ -361,8 +363,10 @@ int ps_gpu_apply_poisson(ps_handle* h);
  * iterations of every instance: each class's propagator sweeps are merged into
  * one launch per contour step, the per-instance field updates run as parallel
  * branches, and the whole iteration is one captured CUDA graph after the
- * first.  Each instance's result equals ps_gpu_iterate on it alone with the
- * same kernel variant.  ps_gpu_batch_instance returns the instance's handle
+ * first.  Instances may hold linear or branched polymers (branched sweeps
+ * are offset to start after their junction's arriving sweeps, see
+ * ps_gpu_set_variant).  Each instance's result equals ps_gpu_iterate on it
+ * alone with the same kernel variant.  ps_gpu_batch_instance returns the instance's handle
  * for ps_gpu_set_fields / get_fields / get_scalars / get_propagator (owned by
  * the batch: do not destroy it; do not iterate it while the batch runs).
  * ps_gpu_batch_set_variant forces one kernel variant for every class (-1:

@@ -34,6 +34,10 @@ struct BatchClass {
   std::vector<int> members;
   int kmax = -1;
   std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
+  // members' junction starts (branched polymers), by global step
+  std::vector<JunctionLaunch<float>> junc_f;
+  std::vector<JunctionLaunch<double>> junc_d;
+  std::vector<int> junc_off, junc_cnt;
   void* d_plane = nullptr;   // PlaneWork<T>[]
   void* d_pencil = nullptr;  // PencilWork<T>[]
   cudaStream_t st = nullptr;
@@ -73,6 +77,10 @@ namespace psb {
     }                                                                    \
   } while (0)
 
+template <typename T> static std::vector<JunctionLaunch<T>>& class_junc(BatchClass& c);
+template <> std::vector<JunctionLaunch<float>>& class_junc<float>(BatchClass& c) { return c.junc_f; }
+template <> std::vector<JunctionLaunch<double>>& class_junc<double>(BatchClass& c) { return c.junc_d; }
+
 template <typename T>
 static SweepSet<T> class_sweep_set(ps_batch* b, BatchClass& c) {
   ps_handle* h0 = b->inst[c.members[0]];
@@ -84,6 +92,10 @@ static SweepSet<T> class_sweep_set(ps_batch* b, BatchClass& c) {
   s.plane_cnt = c.plane_cnt.data();
   s.pencil_off = c.pencil_off.data();
   s.pencil_cnt = c.pencil_cnt.data();
+  std::vector<JunctionLaunch<T>>& jv = class_junc<T>(c);
+  s.junc = jv.empty() ? nullptr : jv.data();
+  s.junc_off = c.junc_off.data();
+  s.junc_cnt = c.junc_cnt.data();
   return s;
 }
 
@@ -98,9 +110,21 @@ static int build_class_tables(ps_batch* b, BatchClass& c) {
   c.plane_cnt.assign(c.kmax + 1, 0);
   c.pencil_off.assign(c.kmax + 1, 0);
   c.pencil_cnt.assign(c.kmax + 1, 0);
+  std::vector<JunctionLaunch<T>>& jv = class_junc<T>(c);
+  jv.clear();
+  c.junc_off.assign(c.kmax + 1, 0);
+  c.junc_cnt.assign(c.kmax + 1, 0);
   for (int k = 0; k <= c.kmax; ++k) {
     c.plane_off[k] = (int)pw.size();
     c.pencil_off[k] = (int)xw.size();
+    c.junc_off[k] = (int)jv.size();
+    for (int i : c.members) {
+      ps_handle* h = b->inst[i];
+      if (k > h->kmax) continue;
+      const Buffers<T>& B = bufs<T>(h);
+      for (int j = 0; j < h->junc_cnt[k]; ++j) jv.push_back(B.junc[h->junc_off[k] + j]);
+    }
+    c.junc_cnt[k] = (int)jv.size() - c.junc_off[k];
     for (int i : c.members) {
       ps_handle* h = b->inst[i];
       if (k > h->kmax) continue;
@@ -298,11 +322,6 @@ static int batch_create(ps_batch* b, const ps_config* cfgs, int count) {
     }
     h->in_batch = true;
     b->inst.push_back(h);
-    if (h->branched) {
-      b->err = "instance " + std::to_string(i) +
-               ": a branched polymer runs as its own handle (its sweeps depend on one another)";
-      return PS_INPUT_ERR;
-    }
     auto key = std::make_tuple(h->n[0], h->n[1], h->n[2], h->prec);
     auto it = cls.find(key);
     int ci;

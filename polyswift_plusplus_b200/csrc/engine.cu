@@ -341,21 +341,23 @@ static int build_device_tables(ps_handle* h) {
     h->pencil_off[k] = (int)xw.size();
     for (size_t e = 0; e < h->exec.size(); ++e) {
       const Sweep& sw = h->sweeps[h->exec[e]];
-      if (k > sw.total) continue;
-      h->sw_plane_off[e][k] = (int)pw.size();
-      h->sw_plane_cnt[e][k] = 1;
-      if (k < sw.total) {
-        h->sw_pencil_off[e][k] = (int)xw.size();
-        h->sw_pencil_cnt[e][k] = 1;
+      const int kg = k;                    // global step
+      const int kl = kg - h->sw_start[e];  // this sweep's own step
+      if (kl < 0 || kl > sw.total) continue;
+      h->sw_plane_off[e][kg] = (int)pw.size();
+      h->sw_plane_cnt[e][kg] = 1;
+      if (kl < sw.total) {
+        h->sw_pencil_off[e][kg] = (int)xw.size();
+        h->sw_pencil_cnt[e][kg] = 1;
       }
       PlaneWork<T> w;
       memset(&w, 0, sizeof(w));
-      w.mode = (k == 0) ? MODE_FIRST : (k == sw.total ? MODE_LAST : MODE_MID);
-      w.src = (k == 0 && sw.jbuf >= 0) ? B.jbuf[sw.jbuf] : nullptr;
+      w.mode = (kl == 0) ? MODE_FIRST : (kl == sw.total ? MODE_LAST : MODE_MID);
+      w.src = (kl == 0 && sw.jbuf >= 0) ? B.jbuf[sw.jbuf] : nullptr;
       w.spec = B.spec[e];
-      w.wfac_in = (k > 0) ? B.wfac[seg_of(sw, k - 1).wfac_id] : nullptr;
-      w.wfac_out = (k < sw.total) ? B.wfac[seg_of(sw, k).wfac_id] : nullptr;
-      w.store = B.slices[e] ? B.slices[e] + (size_t)k * N : nullptr;
+      w.wfac_in = (kl > 0) ? B.wfac[seg_of(sw, kl - 1).wfac_id] : nullptr;
+      w.wfac_out = (kl < sw.total) ? B.wfac[seg_of(sw, kl).wfac_id] : nullptr;
+      w.store = B.slices[e] ? B.slices[e] + (size_t)kl * N : nullptr;
       w.status = &h->d_sc->error_flags;
       double* dc = B.dcbuf.empty() ? nullptr : B.dcbuf[e];
       if (dc) {
@@ -366,12 +368,12 @@ static int build_device_tables(ps_handle* h) {
         }
       }
       pw.push_back(w);
-      if (k < sw.total) {
+      if (kl < sw.total) {
         PencilWork<T> x;
         memset(&x, 0, sizeof(x));
         x.spec = B.spec[e];
-        x.kx = B.kx[seg_of(sw, k).ktab_id];
-        x.kyz = B.kyz[seg_of(sw, k).ktab_id];
+        x.kx = B.kx[seg_of(sw, kl).ktab_id];
+        x.kyz = B.kyz[seg_of(sw, kl).ktab_id];
         if (dc) {
           x.dc_parts = dc;
           x.dc_count = dc + B.dc_cap + 1;
@@ -388,6 +390,26 @@ static int build_device_tables(ps_handle* h) {
   if (!rc) rc = alloc_copy(h, &B.d_pencil, xw);
   B.h_plane = pw;
   B.h_pencil = xw;
+  // junction starts for lockstep launches, before the leaving sweep's first step
+  B.junc.clear();
+  h->junc_off.assign(h->kmax + 1, 0);
+  h->junc_cnt.assign(h->kmax + 1, 0);
+  for (int k = 0; k <= h->kmax; ++k) {
+    h->junc_off[k] = (int)B.junc.size();
+    for (size_t e = 0; e < h->exec.size(); ++e) {
+      const Sweep& sw = h->sweeps[h->exec[e]];
+      if (sw.jbuf < 0 || h->sw_start[e] != k) continue;
+      JunctionLaunch<T> jl;
+      memset(&jl, 0, sizeof(jl));
+      jl.in.n = (int)sw.jin.size();
+      for (int i = 0; i < jl.in.n; ++i)
+        jl.in.q[i] = B.slices[h->sweeps[sw.jin[i].first].storage] + (size_t)sw.jin[i].second * N;
+      jl.out = B.jbuf[sw.jbuf];
+      jl.n = N;
+      B.junc.push_back(jl);
+    }
+    h->junc_cnt[k] = (int)B.junc.size() - h->junc_off[k];
+  }
   return rc;
 }
 
@@ -395,10 +417,7 @@ static int build_device_tables(ps_handle* h) {
 template <typename T>
 static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
   if (!(variant & VARIANT_SPLIT) || h->sw_st.empty()) {
-    if (h->branched) {
-      h->err = "a branched polymer's sweeps run as dependent launch chains (variant bit 8) only";
-      return PS_ATTRIB_ERR;
-    }
+    // lockstep: every sweep's step in shared launches, junction starts between steps
     PS_CUDA(h, launch_sweep_set<T>(handle_sweep_set<T>(h), variant, h->st, nlaunch));
     return PS_OK;
   }
@@ -410,6 +429,7 @@ static int launch_sweeps(ps_handle* h, long long* nlaunch, int variant) {
     s.plane_cnt = h->sw_plane_cnt[e].data();
     s.pencil_off = h->sw_pencil_off[e].data();
     s.pencil_cnt = h->sw_pencil_cnt[e].data();
+    s.junc = nullptr;  // this chain launches its own junction start below
     PS_CUDA(h, cudaStreamWaitEvent(h->sw_st[e], h->ev_split, 0));
     const Sweep& sw = h->sweeps[h->exec[e]];
     if (sw.jbuf >= 0) {
@@ -567,7 +587,6 @@ static int autotune_t(ps_handle* h) {
     if ((v & VARIANT_XY) && (!h->xy_ok || (v & VARIANT_FUSE_Z))) continue;  // absent / same
     if ((v & VARIANT_CLUSTER) && (!h->cluster_ok || (v & VARIANT_XY))) continue;
     if ((v & VARIANT_SPLIT) && h->sw_st.empty()) continue;                 // one sweep only
-    if (!(v & VARIANT_SPLIT) && h->branched) continue;                     // chains only
     long long nl = 0;
     rc = launch_sweeps<T>(h, &nl, v);  // warm-up
     if (rc == PS_OK) e = cudaEventRecord(a, h->st);
@@ -942,8 +961,18 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
         g.ktab_id = (int)(it2 - h->ktab_keys.begin());
       }
     }
+  // Lockstep schedule (engine_state.h): junction-leaving sweeps start one step
+  // after the last sweep arriving at their junction ends.
+  h->sw_start.assign(h->exec.size(), 0);
   h->kmax = 0;
-  for (int s : h->exec) h->kmax = std::max(h->kmax, h->sweeps[s].total);
+  for (size_t e = 0; e < h->exec.size(); ++e) {
+    const Sweep& sw = h->sweeps[h->exec[e]];
+    for (const auto& in : sw.jin) {
+      const Sweep& src = h->sweeps[in.first];
+      h->sw_start[e] = std::max(h->sw_start[e], h->sw_start[src.storage] + src.total + 1);
+    }
+    h->kmax = std::max(h->kmax, h->sw_start[e] + sw.total);
+  }
   // Field model
   FieldModel& fm = h->fm;
   memset(&fm, 0, sizeof(fm));
@@ -1366,10 +1395,6 @@ int ps_gpu_set_variant(ps_handle* h, int variant) {
   }
   if (variant >= 0 && (variant & VARIANT_CLUSTER) && !h->cluster_ok) {
     h->err = "the cluster plane pass exists for FP32 sweeps of 256 x 256 y-z planes only";
-    return PS_ATTRIB_ERR;
-  }
-  if (variant >= 0 && !(variant & VARIANT_SPLIT) && h->branched) {
-    h->err = "a branched polymer's sweeps run as dependent launch chains: set variant bit 8";
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));

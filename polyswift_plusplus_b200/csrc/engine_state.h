@@ -75,6 +75,7 @@ template <typename T> struct Buffers {
   PencilWork<T>* d_pencil = nullptr;
   std::vector<PlaneWork<T>> h_plane;    // host copies of the work tables
   std::vector<PencilWork<T>> h_pencil;
+  std::vector<JunctionLaunch<T>> junc;  // junction starts, by global step (junc_off/junc_cnt)
 };
 
 }  // namespace psb
@@ -115,6 +116,11 @@ struct ps_handle {
   std::vector<std::pair<double, double>> ktab_keys;
   int kmax = 0;
   std::vector<int> plane_off, plane_cnt, pencil_off, pencil_cnt;
+  // Lockstep schedule: executed sweep e runs its local step k - sw_start[e] at
+  // global step k; a sweep leaving a junction starts one step after the last
+  // arriving sweep's final step, and its junction kernel runs in between.
+  std::vector<int> sw_start;
+  std::vector<int> junc_off, junc_cnt;  // per global step, into Buffers<T>::junc
   // the same tables restricted to one executed sweep (VARIANT_SPLIT), and the
   // streams and events of its launch chain
   std::vector<std::vector<int>> sw_plane_off, sw_plane_cnt, sw_pencil_off, sw_pencil_cnt;
@@ -243,6 +249,11 @@ template <typename T> SweepSet<T> handle_sweep_set(ps_handle* h) {
   s.plane_cnt = h->plane_cnt.data();
   s.pencil_off = h->pencil_off.data();
   s.pencil_cnt = h->pencil_cnt.data();
+  if (!B.junc.empty()) {
+    s.junc = B.junc.data();
+    s.junc_off = h->junc_off.data();
+    s.junc_cnt = h->junc_cnt.data();
+  }
   return s;
 }
 

@@ -10,9 +10,19 @@
 
 #include <vector>
 
+#include "field_kernels.cuh"
 #include "kernels.h"
 
 namespace psb {
+
+// A junction start of a branched polymer in lockstep launches: the product of
+// the arriving sweeps' final slices (PsBlock::combineSetJnt), written into the
+// leaving sweep's start buffer between two global steps.
+template <typename T> struct JunctionLaunch {
+  JunctionIn<T> in;
+  T* out;
+  long long n;
+};
 
 template <typename T> struct SweepSet {
   int n[3] = {0, 0, 0};
@@ -30,6 +40,10 @@ template <typename T> struct SweepSet {
   const int* plane_cnt = nullptr;
   const int* pencil_off = nullptr;
   const int* pencil_cnt = nullptr;
+  // junction starts launched before global step k (branched polymers in lockstep)
+  const JunctionLaunch<T>* junc = nullptr;
+  const int* junc_off = nullptr;
+  const int* junc_cnt = nullptr;
 };
 
 // The two-CTA cluster plane pass exists for FP32 256 x 256 planes only.
@@ -60,6 +74,9 @@ cudaError_t launch_sweep_set(const SweepSet<T>& s, int variant, cudaStream_t st,
     ++*nlaunch;                \
   } while (0)
   for (int k = 0; k <= s.kmax; ++k) {
+    if (s.junc)
+      for (int j = s.junc_off[k]; j < s.junc_off[k] + s.junc_cnt[k]; ++j)
+        PSB_L(launch_junction<T>(s.junc[j].in, s.junc[j].n, s.junc[j].out, st));
     const PlaneWork<T>* pw = s.d_plane + s.plane_off[k];
     const int np = s.plane_cnt[k];
     const PencilWork<T>* xw = s.d_pencil + s.pencil_off[k];

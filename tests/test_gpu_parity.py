@@ -1030,7 +1030,6 @@ def test_fp64_branched_polymer_parity(gpu, oracle_lib, case):
         cfg, w = _tree_h()
     g, o, hg, ho = run_both(cfg, w, 6)
     assert_parity(cfg, g, o, hg, ho)
-    assert g.variant()[0] & 8  # dependent launch chains
     for b in range(len(cfg.polymers[0].blocks)):
         steps = o.block_steps(0, b)
         assert g.block_steps(0, b) == steps
@@ -1061,10 +1060,29 @@ def test_kat7_star_debye_response_gpu(gpu):
         assert mode_amplitude(g.phi(i), cfg, 0) == pytest.approx(-eps * want[i], rel=1e-4)
 
 
-def test_branched_polymer_mixed_and_errors(gpu):
-    """Mixed-precision star within 1e-5 of FP64; a star takes only dependent-chain variants
-    and no batch."""
-    from polyswift_plusplus_b200.scft import ScftBatch
+@pytest.mark.parametrize("case", ["star3", "star4", "tree_h"])
+@pytest.mark.parametrize("variant", [0, 3, 11])
+def test_branched_polymer_every_variant(gpu, oracle_lib, case, variant):
+    """Branched sweeps in shared (lockstep) launches, each leaving-junction sweep
+    offset to start one step after the last arriving sweep with its junction
+    product launched in between (variants 0, 3), and as dependent launch chains
+    (variant 11), all against the oracle at 1e-10."""
+    cfg, w = {"star3": lambda: W.star_abc(n=16), "star4": _star4, "tree_h": _tree_h}[case]()
+    g = ScftSolver(cfg)
+    g.set_variant(variant)
+    g.restore(w)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(5)
+    hg = []
+    for _ in range(5):
+        g.update(1)
+        hg.append(g.scalars())
+    assert_parity(cfg, g, o, hg, ho)
+
+
+def test_branched_polymer_mixed(gpu):
+    """Mixed-precision star within 1e-5 of FP64."""
     out = []
     for prec in ("fp64", "mixed"):
         cfg, w = W.star_abc(n=16, precision=prec)
@@ -1072,11 +1090,30 @@ def test_branched_polymer_mixed_and_errors(gpu):
         g.restore(w)
         g.update(10)
         out.append(g.scalars()["free_energy"])
-        with pytest.raises(A.PsError):
-            g.set_variant(1)
-        g.set_variant(9)
-        g.update(1)
     assert abs(out[1] - out[0]) < 1e-5 * max(abs(out[0]), 1.0)
-    cfg, _ = W.star_abc(n=16)
-    with pytest.raises(A.PsError):
-        ScftBatch([cfg])
+
+
+@pytest.mark.parametrize("variant", [0, 3])
+def test_branched_polymers_in_a_batch(gpu, variant):
+    """Stars and a two-junction tree batched with a diblock blend of the same grid:
+    each instance bit-identical to its single run with the same variant."""
+    from polyswift_plusplus_b200.scft import ScftBatch
+    items = [W.star_abc(n=16), _star4(), _tree_h(), W.star_abc(n=16, precision="mixed")]
+    cfg_b = W.blend(16, 15.0, 0.3, 0.1, precision="fp64", seed=5)
+    items.append((cfg_b, W.random_fields(cfg_b, 0.1)))
+    with ScftBatch([c for c, _ in items]) as b:
+        b.set_variant(variant)
+        for i, (_, w) in enumerate(items):
+            b.instance(i).restore(w)
+        b.update(4)
+        for i, (cfg, w) in enumerate(items):
+            s = ScftSolver(cfg)
+            s.set_variant(variant)
+            s.restore(w)
+            s.update(4)
+            v = b.instance(i)
+            assert v.scalars()["free_energy"] == s.scalars()["free_energy"]
+            for f in range(len(cfg.fields)):
+                assert np.array_equal(v.phi(f), s.phi(f))
+                assert np.array_equal(v.w(f), s.w(f))
+            s.close()
