@@ -104,9 +104,10 @@ def test_fft_plugin_interface_known_answers(gpu):
     assert np.abs(pw - exp).max() < 1e-9 * N * N
     delta = np.zeros(n)
     delta[0, 0, 0] = 1.0
-    # FFT of a delta at the origin is 1 everywhere; convolving with it is the identity
+    # FFT of a delta at the origin is 1 everywhere; convolving with it gives N times
+    # the input (both transforms unnormalised)
     assert np.abs(f.calcForwardFFT(delta) - 1.0).max() < 1e-14
-    assert np.abs(f.convolveRe(c, delta).reshape(n) - c).max() < 1e-12
+    assert np.abs(f.convolveRe(c, delta).reshape(n) - N * c).max() < 1e-12 * N
     # scaledFFTPairIm with an odd kdata i*sign(kx): a Hilbert-like transform of the cosine
     kx = np.fft.fftfreq(n[0])[:, None, None] * np.ones(n)
     res = f.scaledFFTPairIm(c, np.sign(kx)).reshape(n)
