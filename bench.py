@@ -258,6 +258,27 @@ def precision_check(n: int, iters: int, device: int) -> dict:
                     "saddle point); max_d_abs_fft_phi is translation invariant"}
 
 
+def l2_copy_bandwidth(device: int, mbytes: int = 16, reps: int = 400) -> float:
+    """Copy bandwidth of an L2-resident buffer (read + write bytes per second,
+    GB/s): a tensor of `mbytes` MB copied into another `reps` times, both far
+    smaller than the 126 MB L2.  The ceiling for passes whose data stays in L2."""
+    import torch
+    dev = torch.device("cuda", device)
+    n = mbytes * (1 << 20) // 4
+    a = torch.ones(n, device=dev)
+    b = torch.empty(n, device=dev)
+    for _ in range(20):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(reps):
+        b.copy_(a)
+    e1.record()
+    e1.synchronize()
+    return 2.0 * n * 4 * reps / (e0.elapsed_time(e1) / 1000.0) / 1e9
+
+
 def cufft_comparison(n: int, device: int, reps: int = 3, steps: int = 200) -> dict:
     """The propagator step built from library FFTs, for comparison only: torch.fft
     (cuFFT) r2c and c2r of n^3 FP32 data, unnormalised, with the two real-space
@@ -573,6 +594,24 @@ def run_ours(args, world, rank, local):
                 "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_step": 3 * N * (4 if args.precision == "mixed" else 8),
                 "step_us": per_step_ms * 1000.0, "samples": len(sweep_ms)}
+    # The step's spectrum passes stay in L2: per sweep and step the plane pass
+    # reads the half spectrum and the Boltzmann factors and writes the slice and
+    # the spectrum, and the pencil pass reads and writes the spectrum.
+    sq = 4 if args.precision == "mixed" else 8
+    spec_b = grid * grid * (grid // 2 + 1) * 2 * sq
+    l2_bytes = 2 * (2 * spec_b + 2 * N * sq + 2 * spec_b)  # both sweeps
+    if rank == 0 and not tri:  # the two-pass design of the 128^2 fused planes
+        try:
+            l2_peak = l2_copy_bandwidth(local)
+            l2_ach = l2_bytes / (per_step_ms / 1000.0) / 1e9
+            roofline["l2"] = {"bound": "l2", "achieved": l2_ach, "peak": l2_peak, "unit": "GB/s",
+                              "frac": l2_ach / l2_peak, "bytes_per_step": l2_bytes,
+                              "floor_step_us": l2_bytes / (l2_peak * 1e9) * 1e6,
+                              "what": "L2 traffic of both sweeps per step (two half-spectrum round trips, "
+                                      "Boltzmann factors, slice writes) against the measured copy "
+                                      "bandwidth of a 16 MB L2-resident buffer"}
+        except Exception as e:
+            roofline["l2"] = {"error": f"{type(e).__name__}: {e}"}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None,
