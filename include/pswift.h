@@ -237,6 +237,18 @@ int ps_gpu_block_steps(const ps_handle* h, int polymer, int block, int* steps);
 int ps_gpu_set_fields(ps_handle* h, int which, int index, const double* data, int on_device);
 int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_device);
 
+/* Read a field back without waiting for it (no reference counterpart: the
+ * reference's PhysFields live in host memory).  The field's current value is
+ * copied on the handle's stream into a device snapshot, and from there into
+ * `host` on a separate copy stream, so the transfer overlaps the iterations
+ * that follow; `host` should be pinned (page-locked) memory for the copy to
+ * run asynchronously.  `host` holds the field once ps_gpu_fields_wait returns.
+ * Each (which, index) has one snapshot, allocated on its first use: a second
+ * read of the same field waits (on the device) for the first one's host copy
+ * before its snapshot is taken. */
+int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host);
+int ps_gpu_fields_wait(ps_handle* h);
+
 /* Reference initialisation: every monomerDens w_i = U[0,1) - 0.5 drawn from
  * MT19937 seeded with cfg->seed, fields in declaration order; p = 0. */
 int ps_gpu_init_random(ps_handle* h);

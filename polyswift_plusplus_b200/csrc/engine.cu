@@ -689,6 +689,14 @@ static void free_all(ps_handle* h) {
   for (auto s : h->sw_st) cudaStreamDestroy(s);
   for (auto e : h->sw_ev) cudaEventDestroy(e);
   if (h->ev_split) cudaEventDestroy(h->ev_split);
+  if (h->io_st) cudaStreamSynchronize(h->io_st);
+  for (auto& kv : h->read_slots) {
+    f(kv.second.d);
+    if (kv.second.snap) cudaEventDestroy(kv.second.snap);
+    if (kv.second.done) cudaEventDestroy(kv.second.done);
+  }
+  h->read_slots.clear();
+  if (h->io_st) cudaStreamDestroy(h->io_st);
   if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -1289,6 +1297,41 @@ int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_d
   PS_CUDA(h, cudaMemcpyAsync(data, src, sizeof(double) * (size_t)h->N,
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->st));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host) {
+  if (!h || !host) return PS_ATTRIB_ERR;
+  double* src = field_ptr(h, which, index);
+  if (!src) {
+    h->err = "bad field selector";
+    return PS_ATTRIB_ERR;
+  }
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  if (!h->io_st) PS_CUDA(h, cudaStreamCreateWithFlags(&h->io_st, cudaStreamNonBlocking));
+  ps_handle::ReadSlot& rs = h->read_slots[std::make_pair(which, index)];
+  const size_t bytes = sizeof(double) * (size_t)h->N;
+  if (!rs.d) {
+    PS_CUDA(h, cudaMalloc((void**)&rs.d, bytes));
+    PS_CUDA(h, cudaEventCreateWithFlags(&rs.snap, cudaEventDisableTiming));
+    PS_CUDA(h, cudaEventCreateWithFlags(&rs.done, cudaEventDisableTiming));
+    PS_CUDA(h, cudaEventRecord(rs.done, h->io_st));
+  }
+  // the previous host copy out of this snapshot has finished before it is overwritten
+  PS_CUDA(h, cudaStreamWaitEvent(h->st, rs.done, 0));
+  PS_CUDA(h, cudaMemcpyAsync(rs.d, src, bytes, cudaMemcpyDeviceToDevice, h->st));
+  PS_CUDA(h, cudaEventRecord(rs.snap, h->st));
+  PS_CUDA(h, cudaStreamWaitEvent(h->io_st, rs.snap, 0));
+  PS_CUDA(h, cudaMemcpyAsync(host, rs.d, bytes, cudaMemcpyDeviceToHost, h->io_st));
+  PS_CUDA(h, cudaEventRecord(rs.done, h->io_st));
+  return PS_OK;
+}
+
+int ps_gpu_fields_wait(ps_handle* h) {
+  if (!h) return PS_ATTRIB_ERR;
+  if (!h->io_st) return PS_OK;
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  PS_CUDA(h, cudaStreamSynchronize(h->io_st));
   return PS_OK;
 }
 

@@ -2,6 +2,7 @@
 // functions that the batch driver (batch.cu) composes into its own graph.
 #pragma once
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -173,6 +174,16 @@ struct ps_handle {
   cudaGraphNode_t node_start = nullptr, node_end = nullptr;  // event-record nodes in the graph
   bool graph_has_timing = false;
   std::vector<float> eager_ms;  // samples taken on eager iterations
+
+  // Asynchronous field read-back (ps_gpu_get_fields_async): per (which, index) a
+  // device snapshot taken on st and copied to the host on io_st.
+  struct ReadSlot {
+    double* d = nullptr;
+    cudaEvent_t snap = nullptr;  // snapshot complete (st)
+    cudaEvent_t done = nullptr;  // host copy complete (io_st)
+  };
+  std::map<std::pair<int, int>, ReadSlot> read_slots;
+  cudaStream_t io_st = nullptr;
   double sweep_bytes = 0.0;  // algorithmic bytes of the sweeps of one iteration
   long long sweep_steps = 0; // propagator steps (all sweeps) of one iteration
 };

@@ -112,6 +112,22 @@ class ScftSolver:
         self._check(self._lib.ps_gpu_get_fields(self._h, which, index, x.ctypes.data_as(C.c_void_p), 0))
         return x
 
+    def get_field_async(self, which: int, index: int, out) -> None:
+        """Start reading a field into `out` (a pinned host float64 tensor or a numpy
+        array of N values) without waiting; `out` holds it after fields_wait()."""
+        if hasattr(out, "data_ptr"):
+            if out.is_cuda or out.dtype != __import__("torch").float64 or out.numel() != self.N:
+                raise ValueError("out must be a host float64 tensor of N values")
+            ptr = C.c_void_p(out.data_ptr())
+        else:
+            if out.dtype != np.float64 or out.size != self.N or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array of N values")
+            ptr = out.ctypes.data_as(C.c_void_p)
+        self._check(self._lib.ps_gpu_get_fields_async(self._h, which, index, ptr))
+
+    def fields_wait(self) -> None:
+        self._check(self._lib.ps_gpu_fields_wait(self._h))
+
     def w(self, i: int) -> np.ndarray:
         return self.get_field(A.PS_FIELD_W, i)
 

@@ -1118,3 +1118,32 @@ def test_branched_polymers_in_a_batch(gpu, variant):
                 assert np.array_equal(v.phi(f), s.phi(f))
                 assert np.array_equal(v.w(f), s.w(f))
             s.close()
+
+
+def test_async_field_readback_matches_blocking_read(gpu):
+    """ps_gpu_get_fields_async: the snapshot taken at the call reaches the host
+    buffer by ps_gpu_fields_wait, while later iterations run; a second read of
+    the same field into another buffer waits for the first copy."""
+    import torch
+    cfg, w = W.diblock32(n=32)
+    g = ScftSolver(cfg)
+    g.restore(w)
+    g.update(2)
+    N = cfg.n_total
+    bufs = [torch.empty(N, dtype=torch.float64).pin_memory() for _ in range(4)]
+    g.get_field_async(A.PS_FIELD_W, 0, bufs[0])
+    g.get_field_async(A.PS_FIELD_PHI, 1, bufs[1])
+    w0, phi1 = g.w(0), g.phi(1)
+    g.update(1)  # runs while the copies may still be in flight
+    g.get_field_async(A.PS_FIELD_W, 0, bufs[2])
+    host_p = np.empty(N)
+    g.get_field_async(A.PS_FIELD_PRES, 0, host_p)  # pageable numpy memory also works
+    g.fields_wait()
+    assert np.array_equal(bufs[0].numpy(), w0)
+    assert np.array_equal(bufs[1].numpy(), phi1)
+    assert np.array_equal(bufs[2].numpy(), g.w(0))
+    assert not np.array_equal(bufs[2].numpy(), w0)
+    assert np.array_equal(host_p, g.pressure())
+    with pytest.raises(A.PsError):
+        g.get_field_async(A.PS_FIELD_W, 7, bufs[3])
+    g.close()
