@@ -604,12 +604,13 @@ def run_ours(args, world, rank, local):
                 "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_step": 3 * N * (4 if args.precision == "mixed" else 8),
                 "step_us": per_step_ms * 1000.0, "samples": len(sweep_ms)}
-    # The step's spectrum passes stay in L2: per sweep and step the plane pass
-    # reads the half spectrum and the Boltzmann factors and writes the slice and
-    # the spectrum, and the pencil pass reads and writes the spectrum.
+    # The step's spectrum passes stay in L2: per propagator step (one sweep,
+    # like step_us) the plane pass reads the half spectrum and the Boltzmann
+    # factors and writes the slice and the spectrum, and the pencil pass reads
+    # and writes the spectrum.
     sq = 4 if args.precision == "mixed" else 8
     spec_b = grid * grid * (grid // 2 + 1) * 2 * sq
-    l2_bytes = 2 * (2 * spec_b + 2 * N * sq + 2 * spec_b)  # both sweeps
+    l2_bytes = 2 * spec_b + 2 * N * sq + 2 * spec_b
     if rank == 0 and not tri:  # the two-pass design of the 128^2 fused planes
         try:
             l2_peak = l2_copy_bandwidth(local)
@@ -617,8 +618,8 @@ def run_ours(args, world, rank, local):
             roofline["l2"] = {"bound": "l2", "achieved": l2_ach, "peak": l2_peak, "unit": "GB/s",
                               "frac": l2_ach / l2_peak, "bytes_per_step": l2_bytes,
                               "floor_step_us": l2_bytes / (l2_peak * 1e9) * 1e6,
-                              "what": "L2 traffic of both sweeps per step (two half-spectrum round trips, "
-                                      "Boltzmann factors, slice writes) against the measured copy "
+                              "what": "L2 traffic per propagator step (two half-spectrum round trips, "
+                                      "Boltzmann factors, slice write) against the measured copy "
                                       "bandwidth of a 16 MB L2-resident buffer"}
         except Exception as e:
             roofline["l2"] = {"error": f"{type(e).__name__}: {e}"}
