@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched blend workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--scale256", type=int, default=5,
+                    help="timed iterations of the 256^3 ABC scale case (0 = skip)")
     ap.add_argument("--batch128", type=int, default=4,
                     help="instances of the 128^3 mixed workload run as one batch (0 = skip)")
     ap.add_argument("--no-cufft", dest="cufft", action="store_false",
@@ -446,6 +448,40 @@ def batched128_rate(count: int, steps: int, device: int) -> dict:
             "free_energy": fe}
 
 
+def scale256_rate(steps: int, device: int) -> dict:
+    """The 256^3 ABC triblock scale case (box 16 Rg, fractions 0.3/0.4/0.3,
+    chiN 30/30/45, Ns = 400, mixed precision; about 75 GB on the device):
+    device-timed iterations/s and time per propagator step after 3 warm-up
+    iterations, autotuned kernel variant.  The iterations are in the workload's
+    steepest-descent phase (Anderson starts at iteration 200); the propagator
+    sweeps, which dominate, are the same either way."""
+    import torch
+
+    from polyswift_plusplus_b200 import workloads as W
+    from polyswift_plusplus_b200.scft import ScftSolver
+    cfg, w = W.triblock256(precision="mixed")
+    cfg.device = device
+    s = ScftSolver(cfg)
+    s.restore(w)
+    s.update(3)
+    s.enable_sweep_timing(steps)
+    st = torch.cuda.ExternalStream(s.stream_ptr, device=torch.device("cuda", device))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    s.update(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sweep_ms, sweep_bytes, sweep_steps = s.sweep_timing()
+    v, _ = s.variant()
+    s.close()
+    step_us = 1000.0 * statistics.mean(sweep_ms) / max(sweep_steps, 1) if sweep_ms else None
+    return {"workload": TRIBLOCK, "value": steps / (ms / 1000.0), "unit": UNIT, "steps": steps,
+            "step_us": step_us, "kernel_variant": v,
+            "algorithmic_bytes_per_step": 3 * cfg.n_total * 4}
+
+
 def run_reference(args, world, rank):
     """The reference's CPU path: its C restatement (the reference itself cannot be
     built), one full FP64 iteration of the same workload per timed step."""
@@ -685,6 +721,11 @@ def run_ours(args, world, rank, local):
         out["mixed_over_fp64"] = value / out["fp64_path"]["value"]
     if rank == 0 and world == 1 and args.batch_instances > 0:
         out["batched"] = batched_rate(args.batch_instances, args.batch_steps, local)
+    if rank == 0 and world == 1 and args.precision == "mixed" and args.scale256 > 0:
+        try:
+            out["scale256"] = scale256_rate(args.scale256, local)
+        except Exception as e:  # e.g. a device with less memory than the case needs
+            out["scale256"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and args.precision == "mixed" and args.batch128 > 0:
         out["batched128"] = batched128_rate(args.batch128, args.batch_steps, local)
         if "fp64_path" in out:

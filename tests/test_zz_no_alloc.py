@@ -65,6 +65,15 @@ def test_noalloc_two_calls_match_plugin_at_64cubed(gpu):
         assert _rel(got, _plugin(shape, d, k)) < TOL
 
 
+def test_noalloc_matches_the_oracle_directly(gpu, oracle_lib):
+    """The same check without the indirection through the allocating plugin:
+    the CPU restatement of PsFFTW::scaledFFTPair, on a fused-plane grid."""
+    import oracle as O
+    shape = (32, 32, 32)
+    d, k = _inputs(shape, 31)
+    assert _rel(_noalloc(gpu, shape, d, k), O.scaled_fft_pair(d, k)) < TOL
+
+
 def test_noalloc_two_calls_of_different_shapes(gpu):
     # a fused-plane grid and a row-kernel grid back to back on the same scratch
     for shape, seed in (((24, 48, 48), 21), ((8, 4, 256), 22), ((32, 32, 32), 23)):
