@@ -381,6 +381,9 @@ int ps_gpu_apply_poisson(ps_handle* h);
  * alone with the same kernel variant.  ps_gpu_batch_instance returns the instance's handle
  * for ps_gpu_set_fields / get_fields / get_scalars / get_propagator (owned by
  * the batch: do not destroy it; do not iterate it while the batch runs).
+ * Within a size class the instances' sweeps either share one launch per
+ * contour step, or (variant bit 3) run as each instance's own concurrent
+ * launch chains; the per-class autotuner times both, and
  * ps_gpu_batch_set_variant forces one kernel variant for every class (-1:
  * autotune each class on its merged sweeps). */
 typedef struct ps_batch ps_batch;

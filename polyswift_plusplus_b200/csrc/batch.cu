@@ -44,6 +44,11 @@ struct BatchClass {
   cudaEvent_t ev = nullptr;
   int variant = -1;
   float tune_ms[VARIANT_COUNT] = {};
+  // Chains mode: each member runs its sweeps as its own concurrent launch chains
+  // (the single-instance split variants) instead of all members' sweeps merged
+  // into one launch per step; chosen by timing, or by a forced variant with bit 3.
+  bool chains = false;
+  float chains_ms = -1.f;
 };
 
 static thread_local std::string g_batch_err;
@@ -145,7 +150,24 @@ static int build_class_tables(ps_batch* b, BatchClass& c) {
 static int class_variant(ps_batch* b, const BatchClass& c) {
   int v = (b->forced_variant >= 0) ? b->forced_variant : (c.variant < 0 ? 0 : c.variant);
   if ((v & VARIANT_XY) && !b->inst[c.members[0]]->xy_ok) v &= ~VARIANT_XY;
-  return v & ~VARIANT_SPLIT;  // a class's sweeps always share launches
+  return v & ~VARIANT_SPLIT;  // the kernels; bit 3 is the class's chains mode
+}
+
+static bool class_chains(const ps_batch* b, const BatchClass& c) {
+  return (b->forced_variant >= 0) ? ((b->forced_variant & VARIANT_SPLIT) != 0) : c.chains;
+}
+
+// Chains mode: every member's sweeps on its own stream (after its pre work).
+static int launch_class_chains(ps_batch* b, BatchClass& c, long long* nl) {
+  const int v = class_variant(b, c) | VARIANT_SPLIT;
+  for (int i : c.members) {
+    int rc = engine_sweeps(b->inst[i], nl, v);
+    if (rc) {
+      b->err = "instance " + std::to_string(i) + ": " + b->inst[i]->err;
+      return rc;
+    }
+  }
+  return PS_OK;
 }
 
 static int launch_class(ps_batch* b, BatchClass& c, long long* nl) {
@@ -175,6 +197,11 @@ static int launch_batch_iteration(ps_batch* b, long long* nl) {
     PB_CUDA(b, cudaEventRecord(b->ev_inst[i], h->st));
   }
   for (BatchClass& c : b->classes) {
+    if (class_chains(b, c)) {
+      int rc = launch_class_chains(b, c, nl);  // on the members' own streams
+      if (rc) return rc;
+      continue;
+    }
     for (int i : c.members) PB_CUDA(b, cudaStreamWaitEvent(c.st, b->ev_inst[i], 0));
     int rc = launch_class(b, c, nl);
     if (rc) return rc;
@@ -183,7 +210,8 @@ static int launch_batch_iteration(ps_batch* b, long long* nl) {
   }
   for (size_t i = 0; i < b->inst.size(); ++i) {
     ps_handle* h = b->inst[i];
-    PB_CUDA(b, cudaStreamWaitEvent(h->st, b->classes[b->class_of[i]].ev, 0));
+    if (!class_chains(b, b->classes[b->class_of[i]]))
+      PB_CUDA(b, cudaStreamWaitEvent(h->st, b->classes[b->class_of[i]].ev, 0));
     int rc = engine_post(h, nl);
     if (rc) return instance_error(b, (int)i, rc);
     PB_CUDA(b, cudaEventRecord(b->ev_inst[i], h->st));
@@ -226,6 +254,34 @@ static int batch_autotune(ps_batch* b) {
                         : autotune_sweep_set<double>(class_sweep_set<double>(b, c), c.st, c.tune_ms, &best);
     PB_CUDA(b, e);
     c.variant = best;
+    // the same kernels as the members' own concurrent chains: one warm-up and
+    // one timed pass, forked from and joined back into c.st
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PB_CUDA(b, cudaEventCreate(&e0));
+    PB_CUDA(b, cudaEventCreate(&e1));
+    float ms = -1.f;
+    int rc = PS_OK;
+    for (int pass = 0; pass < 2 && rc == PS_OK; ++pass) {
+      if (pass == 1) PB_CUDA(b, cudaEventRecord(e0, c.st));
+      PB_CUDA(b, cudaEventRecord(b->ev_fork, c.st));
+      for (int i : c.members) PB_CUDA(b, cudaStreamWaitEvent(b->inst[i]->st, b->ev_fork, 0));
+      long long nl = 0;
+      rc = launch_class_chains(b, c, &nl);
+      for (int i : c.members) {
+        PB_CUDA(b, cudaEventRecord(b->ev_inst[i], b->inst[i]->st));
+        PB_CUDA(b, cudaStreamWaitEvent(c.st, b->ev_inst[i], 0));
+      }
+    }
+    if (rc == PS_OK) {
+      PB_CUDA(b, cudaEventRecord(e1, c.st));
+      PB_CUDA(b, cudaEventSynchronize(e1));
+      PB_CUDA(b, cudaEventElapsedTime(&ms, e0, e1));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    c.chains_ms = ms;
+    c.chains = (ms >= 0.f && ms < c.tune_ms[best]);
   }
   return PS_OK;
 }
@@ -419,7 +475,10 @@ int ps_gpu_batch_classes(const ps_batch* b, int* n_classes, int* class_of, int m
   *n_classes = (int)b->classes.size();
   for (int i = 0; class_of && i < max_inst && i < (int)b->class_of.size(); ++i) class_of[i] = b->class_of[i];
   for (int c = 0; variants && c < max_classes && c < (int)b->classes.size(); ++c)
-    variants[c] = (b->forced_variant >= 0) ? b->forced_variant : b->classes[c].variant;
+    variants[c] = (b->forced_variant >= 0)
+                      ? b->forced_variant
+                      : (b->classes[c].variant < 0 ? -1
+                                                   : (b->classes[c].variant | (b->classes[c].chains ? VARIANT_SPLIT : 0)));
   return PS_OK;
 }
 

@@ -623,6 +623,11 @@ int engine_pre(ps_handle* h, long long* nlaunch) {
   return (h->prec == PS_PREC_MIXED) ? launch_pre<float>(h, nlaunch) : launch_pre<double>(h, nlaunch);
 }
 
+int engine_sweeps(ps_handle* h, long long* nlaunch, int variant) {
+  return (h->prec == PS_PREC_MIXED) ? launch_sweeps<float>(h, nlaunch, variant)
+                                    : launch_sweeps<double>(h, nlaunch, variant);
+}
+
 int engine_post(ps_handle* h, long long* nlaunch) {
   return (h->prec == PS_PREC_MIXED) ? launch_post<float>(h, nlaunch) : launch_post<double>(h, nlaunch);
 }

@@ -222,6 +222,9 @@ enum { POST_FILTER = 1, POST_POISSON = 2 };
 void post_order_set(ps_handle* h, int code, bool on);
 int engine_pre(ps_handle* h, long long* nlaunch);
 int engine_post(ps_handle* h, long long* nlaunch);
+// The instance's propagator sweeps alone, on h->st (variant bit 3: as concurrent
+// launch chains forked from and joined back into h->st).
+int engine_sweeps(ps_handle* h, long long* nlaunch, int variant);
 // Host-side random-number bookkeeping owed before each iteration.
 int engine_prepare_noise(ps_handle* h);
 // Updater noise drawn on the device (noise.cu).  noise_launch forks the draws of

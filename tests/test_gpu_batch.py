@@ -54,8 +54,10 @@ def _run_single(cfg, w, iters, variant):
 
 
 @pytest.mark.parametrize("noise", [0.0, 0.01])
-@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("variant", [0, 2, 10])
 def test_batch_bit_identical_to_single_instances(gpu, variant, noise):
+    """variant 10 (bit 3): every instance's sweeps as its own concurrent launch
+    chains inside the batch graph, instead of shared launches per step."""
     items = _mixed_batch()
     if noise:  # every other instance draws updater noise on the device
         items = [(dataclasses.replace(c, updater=dataclasses.replace(c.updater, noise=noise)) if i % 2 else c, w)
