@@ -720,14 +720,17 @@ def run_ours(args, world, rank, local):
         return
     if rank == 0 and world == 1 and args.precision == "mixed" and args.precision_iters > 0:
         out["precision"] = precision_check(args.n, args.precision_iters, local)
-        esc = out["precision"]["escalated"]
-        # The rate of the whole job that meets the metric's accuracy condition:
-        # FP32 sweeps, then FP64 sweeps for the last iterations (switch included).
+        mix, esc = out["precision"]["mixed"], out["precision"]["escalated"]
+        # The rate of the whole 1000-iteration job that meets the metric's
+        # accuracy condition |dF/F| < 1e-6 against the FP64 path: the FP32-sweep
+        # job when it does, else the job that finishes its last iterations with
+        # FP64 sweeps (switch included).
+        job, name = (mix, "mixed") if mix["dF_over_F"] < 1e-6 else (esc, "escalated")
         out["value_at_tolerance"] = {
-            "value": esc["iter_per_s"], "unit": UNIT, "dF_over_F": esc["dF_over_F"],
-            "iterations": args.precision_iters,
-            "fp64_finish_iterations": esc["fp64_finish_iterations"],
-            "what": "device-timed rate of the whole escalated job from the seeded start"}
+            "value": job["iter_per_s"], "unit": UNIT, "dF_over_F": job["dF_over_F"],
+            "job": name, "iterations": args.precision_iters,
+            "fp64_finish_iterations": esc["fp64_finish_iterations"] if name == "escalated" else 0,
+            "what": "device-timed rate of the whole job from the seeded start"}
     if rank == 0 and world == 1 and args.precision == "mixed" and args.cufft:
         try:
             cmpf = cufft_comparison(args.n, local)

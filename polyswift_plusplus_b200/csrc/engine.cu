@@ -284,9 +284,9 @@ static int build_device_tables(ps_handle* h) {
     B.dc_cap = std::max(kDcMinSlots, std::max(2 * h->n[0], (h->n[0] * h->n[1] + 7) / 8));
     for (size_t e = 0; e < h->exec.size(); ++e) {
       double* d = nullptr;
-      PS_CUDA(h, cudaMalloc((void**)&d, sizeof(double) * (size_t)(B.dc_cap + 2)));
+      PS_CUDA(h, cudaMalloc((void**)&d, sizeof(double) * (size_t)(B.dc_cap + 3)));
       B.dcbuf.push_back(d);
-      PS_CUDA(h, cudaMemset(d, 0, sizeof(double) * (size_t)(B.dc_cap + 2)));
+      PS_CUDA(h, cudaMemset(d, 0, sizeof(double) * (size_t)(B.dc_cap + 3)));
     }
   }
   for (auto& kk : h->ktab_keys) {
@@ -378,7 +378,9 @@ static int build_device_tables(ps_handle* h) {
           x.dc_parts = dc;
           x.dc_count = dc + B.dc_cap + 1;
           x.dc_total = dc + B.dc_cap;
+          x.dc_err = dc + B.dc_cap + 2;
           x.dc_scale = 1.0 / (double)N;
+          x.dc_first = (kl == 0) ? 1 : 0;
         }
         xw.push_back(x);
       }

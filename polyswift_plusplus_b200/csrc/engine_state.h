@@ -64,8 +64,9 @@ template <typename T> struct Buffers {
   std::vector<c2_t<T>*> spec;    // per executed sweep
   std::vector<T*> wfac;          // per (field, ds) key
   std::vector<T*> jbuf;          // junction start buffers of branched polymers (N each)
-  std::vector<double*> dcbuf;    // per executed sweep, FP32 sweeps: mean-mode carry
-                                 // (partials [0, dc_cap), the mean at dc_cap, the count at dc_cap + 1)
+  std::vector<double*> dcbuf;    // per executed sweep, FP32 sweeps: mean-mode carry (partials
+                                 // [0, dc_cap), the mean at dc_cap, the count at dc_cap + 1, the
+                                 // fed-back rounding at dc_cap + 2)
   int dc_cap = 0;
   std::vector<T*> kx, kyz;       // per (ds, bseg) key
   c2_t<T>* tw_x = nullptr;

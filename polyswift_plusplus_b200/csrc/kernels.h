@@ -19,10 +19,12 @@ enum { MODE_FIRST = 0, MODE_MID = 1, MODE_LAST = 2 };
 // gridDim.x in *dc_count); the x pencil pass (or the x-y pass) drops the FP32
 // k = 0 coefficient, and one warp of its first CTA writes the FP64 mean
 // (sum of the partials) * dc_scale (= 1/N) to dc_total; the next plane/row
-// pass adds that value to every point of its inverse transform (dc_in) as a
-// two-float sum, so its rounding differs from point to point.  The partials
-// buffer holds at least kDcMinSlots slots.  nullptr: no carry (FP64 sweeps,
-// the plugins).
+// pass adds that value, rounded to T, to every point of its inverse transform
+// (dc_in).  The part the rounding drops (the same at every point, so it would
+// accumulate over the sweep) is kept in *dc_err and added to the next step's
+// mean: what one step loses, the next one puts back (reset at the sweep's
+// first step, dc_first).  The partials buffer holds at least kDcMinSlots
+// slots.  nullptr: no carry (FP64 sweeps, the plugins).
 constexpr int kDcMinSlots = 128;
 
 template <typename T> struct PlaneWork {
@@ -59,7 +61,9 @@ template <typename T> struct PencilWork {
   const double* dc_parts;  // PENCIL_KINV / x-y pass: the plane pass's dc_out (mean-mode carry)
   const double* dc_count;  // ... its number of partials
   double* dc_total;        // ... and where the FP64 mean goes
+  double* dc_err;          // ... the rounding the previous step's mean lost (error feedback)
   double dc_scale;         // 1 / N
+  int dc_first;            // the sweep's first step: no error to feed back
 };
 
 bool extent_supported(int n);

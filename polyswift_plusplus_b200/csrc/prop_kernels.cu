@@ -40,31 +40,26 @@ __device__ __forceinline__ T ld_or_one(const T* p, size_t i) {
 // ---------------------------------------------------------------------------
 // Per-warp FP64 sums of the forward input, summed into one CTA partial.
 __shared__ double s_dc_warp[32];
-// The mean-mode value of the inverse transform as (hi, lo) of T; written by
+// The mean-mode value of the inverse transform rounded to T; written by
 // thread 0 after pdl_wait(), read after the barriers that precede the inverse
-// step (kept in shared memory, not in registers, through the FFT passes).
+// step (kept in shared memory, not in registers, through the FFT passes).  What
+// the rounding drops comes back through the next step's mean (dc_err).
 __shared__ __align__(16) double s_dc_hilo[2];
 
 template <typename T>
 __device__ __forceinline__ void dc_hilo_store(const double* dc_in) {
-  if (threadIdx.x == 0 && dc_in) {
-    const double d = *dc_in;
-    const T hi = T(d);
-    reinterpret_cast<T*>(s_dc_hilo)[0] = hi;
-    reinterpret_cast<T*>(s_dc_hilo)[1] = T(d - (double)hi);
-  }
+  if (threadIdx.x == 0 && dc_in) reinterpret_cast<T*>(s_dc_hilo)[0] = T(*dc_in);
 }
 
-// x + mean-mode value, as (x + hi) + lo
+// x + mean-mode value
 template <typename T>
 __device__ __forceinline__ c2_t<T> dc_add2(c2_t<T> x) {
-  const c2_t<T> hl = *reinterpret_cast<const c2_t<T>*>(s_dc_hilo);
-  return cadd(cadd(x, c2_t<T>{hl.x, hl.x}), c2_t<T>{hl.y, hl.y});
+  const T m = reinterpret_cast<const T*>(s_dc_hilo)[0];
+  return cadd(x, c2_t<T>{m, m});
 }
 template <typename T>
 __device__ __forceinline__ T dc_add(T x) {
-  const T* hl = reinterpret_cast<const T*>(s_dc_hilo);
-  return (x + hl[0]) + hl[1];
+  return x + reinterpret_cast<const T*>(s_dc_hilo)[0];
 }
 
 // Every thread of the CTA calls this (CTA-uniform): lane 0 keeps its warp's sum.
@@ -116,7 +111,12 @@ template <typename T> struct DcFinish {
     for (int i = kDcMinSlots + lane; i < n; i += 32) s += w.dc_parts[i];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) *w.dc_total = s * w.dc_scale;
+    if (lane == 0) {
+      // error feedback: add what the previous step's rounding to T dropped
+      const double m = s * w.dc_scale + (w.dc_first ? 0.0 : *w.dc_err);
+      *w.dc_total = m;
+      *w.dc_err = m - (double)T(m);
+    }
   }
 };
 

@@ -103,9 +103,10 @@ def test_diblock128_full_size_mixed_variant11(gpu, diblock128_oracle):
 
 def test_mean_mode_carry_reduces_fp32_error(gpu):
     """FP32 sweeps carry the k = 0 coefficient of every step in FP64 (PlaneWork's
-    mean-mode carry).  At full size, after one iteration Q of the FP32 sweeps
-    must be within 5e-7 of the FP64 device path's and at most 0.6 times the
-    error without the carry (measured on a B200: 3.0e-7 with, 7.7e-7 without)."""
+    mean-mode carry, with the rounding of the added mean fed back into the next
+    step).  At full size, after one iteration Q of the FP32 sweeps must be
+    within 1.5e-7 of the FP64 device path's and at most 0.3 times the error
+    without the carry (measured on a B200: 6.7e-8 with, 7.7e-7 without)."""
     import os
     cfg64, w = W.diblock128(precision="fp64")
     g = ScftSolver(cfg64)
@@ -126,5 +127,5 @@ def test_mean_mode_carry_reduces_fp32_error(gpu):
             m.close()
         finally:
             os.environ.pop("PSB_DC_CARRY", None)
-    assert errs["1"] < 5e-7, errs
-    assert errs["1"] < 0.6 * errs["0"], errs
+    assert errs["1"] < 1.5e-7, errs
+    assert errs["1"] < 0.3 * errs["0"], errs
