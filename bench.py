@@ -68,7 +68,7 @@ def parse_args():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--scale256", type=int, default=5,
                     help="timed iterations of the 256^3 ABC scale case (0 = skip)")
-    ap.add_argument("--batch128", type=int, default=4,
+    ap.add_argument("--batch128", type=int, default=2,
                     help="instances of the 128^3 mixed workload run as one batch (0 = skip)")
     ap.add_argument("--no-cufft", dest="cufft", action="store_false",
                     help="skip the cuFFT (torch.fft) comparison of the propagator step")
