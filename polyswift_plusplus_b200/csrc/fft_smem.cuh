@@ -282,6 +282,9 @@ __device__ __forceinline__ void fused_pass_pair(C* buf, int bs, int is, const C*
   constexpr int U = (NB + T - 1) / T;
   C v[U][R];
   const int t = threadIdx.x;
+  // the first butterfly's operand loads (global memory) are issued before the
+  // shared-memory reads and the barrier, so their latency overlaps them
+  if ((NB % T) == 0 || t < NB) op.prefetch(BFAST ? (t % B) : (t / M), BFAST ? (t / B) : (t % M));
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     const int g = t + u * T;
@@ -300,7 +303,7 @@ __device__ __forceinline__ void fused_pass_pair(C* buf, int bs, int is, const C*
     if ((NB % T) == 0 || g < NB) {
       const int b = BFAST ? (g % B) : (g / M);
       const int j = BFAST ? (g / B) : (g % M);
-      op.prefetch(b, j);
+      if (u > 0) op.prefetch(b, j);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
         const C w = tw[r * j];
