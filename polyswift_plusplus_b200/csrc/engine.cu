@@ -1444,7 +1444,7 @@ int ps_gpu_set_variant(ps_handle* h, int variant) {
     return PS_ATTRIB_ERR;
   }
   if (variant >= 0 && (variant & VARIANT_CLUSTER) && !h->cluster_ok) {
-    h->err = "the cluster plane pass exists for FP32 sweeps of 256 x 256 y-z planes only";
+    h->err = "the cluster plane pass exists for 256 x 256 y-z planes only";
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));

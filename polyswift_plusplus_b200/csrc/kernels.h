@@ -81,9 +81,9 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // bit 3: each sweep of an instance runs as its own chain of launches on its
 // own stream (parallel graph branches) instead of all sweeps in lockstep in
 // shared launches; single-instance engine only (kernels ignore the bit).
-// bit 4: FP32 256 x 256 y-z planes (too large for one CTA) run as one plane
-// pass on a cluster of two CTAs instead of a row pass and two y pencil passes
-// (cluster_plane_supported); elsewhere the bit changes nothing.
+// bit 4: 256 x 256 y-z planes (too large for one CTA) run as one plane pass on
+// a cluster of CTAs (two for FP32, four for FP64) instead of a row pass and two
+// y pencil passes (cluster_plane_supported); elsewhere the bit changes nothing.
 enum {
   VARIANT_FUSE_Z = 1,
   VARIANT_FUSE_K = 2,
@@ -93,9 +93,11 @@ enum {
   VARIANT_COUNT = 32
 };
 bool cluster_plane_supported(int prec_bytes, int ny, int nz);
-// The two-CTA cluster plane pass (FP32, ny = nz = 256): grid 2 nx x nworks.
-cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, int nx, const float2* tw_y,
-                                 const float2* tw_zh, const float2* tw_z, cudaStream_t st);
+// The cluster plane pass (ny = nz = 256): grid CL nx x nworks, CL = 2 (FP32)
+// or 4 (FP64) CTAs per plane.
+template <typename T>
+cudaError_t launch_plane_cluster(const PlaneWork<T>* d_works, int nworks, int nx, const c2_t<T>* tw_y,
+                                 const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st);
 
 // The x-y plane design exists for this grid (square x-y planes that fit in
 // shared memory).

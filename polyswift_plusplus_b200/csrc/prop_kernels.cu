@@ -1001,19 +1001,21 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz) {
 }
 
 // ---------------------------------------------------------------------------
-// Plane pass of FP32 256 x 256 y-z planes on a cluster of two CTAs
-// (VARIANT_CLUSTER).  A 256 x 129 half plane (264 KB) does not fit one CTA's
-// shared memory; split over two it does, and the step needs no y pencil passes
-// (two fewer spectrum round trips).  CTA c holds:
-//   y phases: kz columns [64c, 64c + 64) for all y (CTA 0 also kz = 128, which
-//             shares the kz = 0 transform), layout Y[y][slot], 65 slots a row;
-//   z phases: y rows [128c, 128c + 128) for all kz, layout Z[r][kz], 129 a row.
+// Plane pass of 256 x 256 y-z planes on a cluster of CL CTAs
+// (VARIANT_CLUSTER): two for FP32, four for FP64.  A 256 x 129 half plane
+// (264 KB in FP32, 528 KB in FP64) does not fit one CTA's shared memory; split
+// over the cluster it does, and the step needs no y pencil passes (two fewer
+// spectrum round trips).  With CH = 128 / CL and RH = 256 / CL, CTA c holds:
+//   y phases: kz columns [CH c, CH c + CH) for all y (CTA 0 also kz = 128,
+//             which shares the kz = 0 transform), layout Y[y][slot], CH + 1
+//             slots a row;
+//   z phases: y rows [RH c, RH c + RH) for all kz, layout Z[r][kz], 129 a row.
 // Between the phases every thread reads its elements into registers, a cluster
-// barrier makes sure both CTAs have read their buffers, the elements are
-// written to their place in the other layout (this CTA's or the peer's shared
-// memory), and a second cluster barrier publishes them.  Both CTAs of a
-// cluster work on the same plane and mode, so they take the same barriers; no
-// shared memory is touched across the cluster after the last one.
+// barrier makes sure every CTA has read its buffer, the elements are written
+// to their place in the other layout (this CTA's or a peer's shared memory),
+// and a second cluster barrier publishes them.  All CTAs of a cluster work on
+// the same plane and mode, so they take the same barriers; no shared memory is
+// touched across the cluster after the last one.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t cluster_ctarank() {
   uint32_t r;
@@ -1032,28 +1034,48 @@ __device__ __forceinline__ uint32_t peer_smem(const void* p, uint32_t rank) {
 __device__ __forceinline__ void st_peer(uint32_t addr, float2 v) {
   asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
+__device__ __forceinline__ void st_peer(uint32_t addr, double2 v) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y) : "memory");
+}
+// Element i of the buffer `buf` in CTA `rank`: here, or a peer's shared memory.
+template <typename C>
+__device__ __forceinline__ void st_cluster(C* buf, int i, uint32_t rank, uint32_t me, C v) {
+  if (rank == me) buf[i] = v;
+  else st_peer(peer_smem(buf + i, rank), v);
+}
 
-struct PlaneC256 {
-  static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128, TH = 1024;
-  static constexpr int CH = 64;           // y-FFT columns per CTA
-  static constexpr int YS = CH + 1;       // Y row stride (slot CH: kz = 128 in CTA 0)
-  static constexpr int RH = NY / 2;       // z rows per CTA
-  static constexpr int YE = NY * YS;      // 16640
-  static constexpr int ZE = RH * NZH;     // 16512
+template <typename T> struct PlaneCl;
+template <> struct PlaneCl<float> {
+  static constexpr int CL = 2, TH = 1024, UCMAX = 8;
+};
+template <> struct PlaneCl<double> {
+  static constexpr int CL = 4, TH = 512, UCMAX = 4;
+};
+template <typename T> struct PlaneC256 {
+  static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128;
+  static constexpr int CL = PlaneCl<T>::CL, TH = PlaneCl<T>::TH;
+  static constexpr int CH = (NZ / 2) / CL;  // y-FFT columns per CTA
+  static constexpr int YS = CH + 1;         // Y row stride (slot CH: kz = 128 in CTA 0)
+  static constexpr int RH = NY / CL;        // z rows per CTA
+  static constexpr int YE = NY * YS;
+  static constexpr int ZE = RH * NZH;
   static constexpr int BUF = (YE > ZE) ? YE : ZE;
-  static constexpr int UY = NY * CH / TH;            // 32 Y elements per thread (+1 slot-CH element)
-  static constexpr int UZ = (ZE + TH - 1) / TH;      // 33 Z elements per thread
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)BUF + H + NZ + NY);
+  static constexpr int UY = NY * CH / TH;            // Y elements per thread (+1 slot-CH element)
+  static constexpr int UZ = (ZE + TH - 1) / TH;      // Z elements per thread
+  static constexpr size_t SMEM = sizeof(c2_t<T>) * ((size_t)BUF + H + NZ + NY);
+  // the Y -> Z exchange keeps y = e / CH warp-uniform and the slot-CH column
+  // takes one thread per y
+  static_assert(CH % 32 == 0 && (NY * CH) % TH == 0 && NY <= TH, "cluster plane layout");
 };
 
-__global__ void __launch_bounds__(PlaneC256::TH, 1)
-    plane_c256_kernel(const PlaneWork<float>* __restrict__ works, const float2* __restrict__ tw_y,
-                      const float2* __restrict__ tw_zh, const float2* __restrict__ tw_z) {
-  using P = PlaneC256;
-  using T = float;
-  using C = float2;
+template <typename T>
+__global__ void __launch_bounds__(PlaneC256<T>::TH, 1)
+    plane_c256_kernel(const PlaneWork<T>* __restrict__ works, const c2_t<T>* __restrict__ tw_y,
+                      const c2_t<T>* __restrict__ tw_zh, const c2_t<T>* __restrict__ tw_z) {
+  using P = PlaneC256<T>;
+  using C = c2_t<T>;
   constexpr int NY = P::NY, NZ = P::NZ, NZH = P::NZH, H = P::H, TH = P::TH, CH = P::CH, YS = P::YS,
-                RH = P::RH;
+                RH = P::RH, CL = P::CL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
   C* s_tw_zh = buf + P::BUF;
@@ -1061,15 +1083,13 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
   C* s_tw_y = s_tw_z + NZ;
 
   const uint32_t me = cluster_ctarank();
-  const uint32_t peer = me ^ 1u;
   const PlaneWork<T> w = works[blockIdx.y];
-  const int x = blockIdx.x >> 1;
+  const int x = blockIdx.x / CL;
   const int tid = threadIdx.x;
   const size_t soff = (size_t)x * NY * NZH;
-  const int row0 = (int)me * RH, prow0 = (int)peer * RH;
+  const int row0 = (int)me * RH;
   const int col0 = (int)me * CH;
   const size_t roff = ((size_t)x * NY + row0) * NZ;
-  const uint32_t pbase = peer_smem(buf, peer);
   for (int i = tid; i < H; i += TH) s_tw_zh[i] = tw_zh[i];
   for (int i = tid; i < NZ; i += TH) s_tw_z[i] = tw_z[i];
   for (int i = tid; i < NY; i += TH) s_tw_y[i] = tw_y[i];
@@ -1087,7 +1107,7 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
         const int e = tid + u * TH;
         t[u] = __ldg(src + (size_t)(e / CH) * NZH + col0 + (e % CH));
       }
-      C tx = C{0.f, 0.f};
+      C tx = C{T(0), T(0)};
       if (me == 0 && tid < NY) tx = __ldg(src + (size_t)tid * NZH + NZ / 2);
 #pragma unroll
       for (int u = 0; u < P::UY; ++u) {
@@ -1109,41 +1129,38 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
     if (me == 0) {
       for (int y = tid; y < NY; y += TH) {
         const C c = buf[y * YS];
-        buf[y * YS] = C{c.x, 0.f};
-        buf[y * YS + CH] = C{c.y, 0.f};
+        buf[y * YS] = C{c.x, T(0)};
+        buf[y * YS + CH] = C{c.y, T(0)};
       }
     }
     __syncthreads();
-    // Y -> Z: element (y, kz) goes to row y - row0 here or y - prow0 in the peer
+    // Y -> Z: element (y, kz) goes to row y - RH o of CTA o = y / RH
     C v[P::UY];
-    C vx = C{0.f, 0.f};
+    C vx = C{T(0), T(0)};
 #pragma unroll
     for (int u = 0; u < P::UY; ++u) {
       const int e = tid + u * TH;
       v[u] = buf[(e / CH) * YS + (e % CH)];
     }
     if (me == 0 && tid < NY) vx = buf[tid * YS + CH];
-    cluster_sync_all();  // both buffers read
+    cluster_sync_all();  // every buffer read
 #pragma unroll
     for (int u = 0; u < P::UY; ++u) {
       const int e = tid + u * TH;
-      const int y = e / CH, kz = col0 + (e % CH);
-      if (y >= row0 && y < row0 + RH)  // uniform in u: y = tid / 64 + (TH / 64) u
-        buf[(y - row0) * NZH + kz] = v[u];
-      else
-        st_peer(pbase + 8u * (uint32_t)((y - prow0) * NZH + kz), v[u]);
+      const int y = e / CH, kz = col0 + (e % CH);  // y uniform over a warp (CH % 32 == 0)
+      const int o = y / RH;
+      st_cluster(buf, (y - o * RH) * NZH + kz, (uint32_t)o, me, v[u]);
     }
     if (me == 0 && tid < NY) {
-      const int y = tid;
-      if (y < row0 + RH) buf[(y - row0) * NZH + NZ / 2] = vx;
-      else st_peer(pbase + 8u * (uint32_t)((y - prow0) * NZH + NZ / 2), vx);
+      const int y = tid, o = y / RH;
+      st_cluster(buf, (y - o * RH) * NZH + NZ / 2, (uint32_t)o, me, vx);
     }
-    cluster_sync_all();  // both Z layouts complete
+    cluster_sync_all();  // every Z layout complete
     c2r_pre<NZ, RH, TH>(buf, s_tw_z, RH);
     __syncthreads();
     smem_fft<H, RH, TH, true, true>(buf, NZH, 1, s_tw_zh);
   }
-  real_space<T, RH, NZ, TH, 8>(w, reinterpret_cast<T*>(buf), roff, RH);
+  real_space<T, RH, NZ, TH, PlaneCl<T>::UCMAX>(w, reinterpret_cast<T*>(buf), roff, RH);
   if (w.mode == MODE_LAST) return;  // uniform over the cluster
   __syncthreads();
   smem_fft<H, RH, TH, false, true>(buf, NZH, 1, s_tw_zh);
@@ -1157,7 +1174,7 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
       const int e = tid + u * TH;
       if (e < P::ZE) v[u] = buf[e];
     }
-    cluster_sync_all();  // both buffers read
+    cluster_sync_all();  // every buffer read
 #pragma unroll
     for (int u = 0; u < P::UZ; ++u) {
       const int e = tid + u * TH;
@@ -1166,11 +1183,10 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
         const int y = row0 + r;
         const int owner = (kz == NZ / 2) ? 0 : (kz / CH);
         const int slot = (kz == NZ / 2) ? CH : (kz - owner * CH);
-        if (owner == (int)me) buf[y * YS + slot] = v[u];
-        else st_peer(pbase + 8u * (uint32_t)(y * YS + slot), v[u]);
+        st_cluster(buf, y * YS + slot, (uint32_t)owner, me, v[u]);
       }
     }
-    cluster_sync_all();  // both Y layouts complete
+    cluster_sync_all();  // every Y layout complete
   }
   // forward y FFT of the columns (plane_y_forward on this CTA's part)
   if (me == 0) {
@@ -1182,8 +1198,8 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
     for (int k = tid; k <= NY / 2; k += TH) {
       const int km = (NY - k) % NY;
       const C c = buf[k * YS], d = buf[km * YS];
-      const C a0 = {0.5f * (c.x + d.x), 0.5f * (c.y - d.y)};
-      const C ah = {0.5f * (c.y + d.y), 0.5f * (d.x - c.x)};
+      const C a0 = {T(0.5) * (c.x + d.x), T(0.5) * (c.y - d.y)};
+      const C ah = {T(0.5) * (c.y + d.y), T(0.5) * (d.x - c.x)};
       buf[k * YS] = a0;
       buf[k * YS + CH] = ah;
       if (km != k) {
@@ -1200,24 +1216,26 @@ __global__ void __launch_bounds__(PlaneC256::TH, 1)
   }
   if (me == 0)
     for (int y = tid; y < NY; y += TH) dst[(size_t)y * NZH + NZ / 2] = buf[y * YS + CH];
-  // mean-mode carry: a partial per CTA (two per plane), after the barriers above
+  // mean-mode carry: a partial per CTA (CL per plane), after the barriers above
   if (w.dc_out) dc_cta_store(works + blockIdx.y);
 }
 
-cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, int nx, const float2* tw_y,
-                                 const float2* tw_zh, const float2* tw_z, cudaStream_t st) {
-  auto kern = plane_c256_kernel;
+template <typename T>
+cudaError_t launch_plane_cluster(const PlaneWork<T>* d_works, int nworks, int nx, const c2_t<T>* tw_y,
+                                 const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st) {
+  using P = PlaneC256<T>;
+  auto kern = plane_c256_kernel<T>;
   static unsigned attr_mask = 0;
-  cudaError_t e = ensure_smem_attr(kern, PlaneC256::SMEM, &attr_mask);
+  cudaError_t e = ensure_smem_attr(kern, P::SMEM, &attr_mask);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(2 * nx, nworks);
-  cfg.blockDim = dim3(PlaneC256::TH);
-  cfg.dynamicSmemBytes = PlaneC256::SMEM;
+  cfg.gridDim = dim3(P::CL * nx, nworks);
+  cfg.blockDim = dim3(P::TH);
+  cfg.dynamicSmemBytes = P::SMEM;
   cfg.stream = st;
   cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.x = P::CL;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1226,8 +1244,14 @@ cudaError_t launch_plane_cluster(const PlaneWork<float>* d_works, int nworks, in
   cfg.numAttrs = pdl_enabled() ? 2 : 1;
   return cudaLaunchKernelEx(&cfg, kern, d_works, tw_y, tw_zh, tw_z);
 }
+template cudaError_t launch_plane_cluster<float>(const PlaneWork<float>*, int, int, const float2*, const float2*,
+                                                 const float2*, cudaStream_t);
+template cudaError_t launch_plane_cluster<double>(const PlaneWork<double>*, int, int, const double2*,
+                                                  const double2*, const double2*, cudaStream_t);
 
-bool cluster_plane_supported(int prec_bytes, int ny, int nz) { return prec_bytes == 4 && ny == 256 && nz == 256; }
+bool cluster_plane_supported(int prec_bytes, int ny, int nz) {
+  return (prec_bytes == 4 || prec_bytes == 8) && ny == 256 && nz == 256;
+}
 
 #define PSB_PLANE_CASE(T, NY, NZ, TH)                                                      \
   if (ny == NY && nz == NZ)                                                                \

@@ -46,21 +46,17 @@ template <typename T> struct SweepSet {
   const int* junc_cnt = nullptr;
 };
 
-// The two-CTA cluster plane pass exists for FP32 256 x 256 planes only.
+// The cluster plane pass exists for 256 x 256 planes (two CTAs in FP32, four
+// in FP64).
 template <typename T>
 inline bool cluster_path(const SweepSet<T>& s, int variant) {
-  return (variant & VARIANT_CLUSTER) && sizeof(T) == 4 && !s.fused_plane &&
+  return (variant & VARIANT_CLUSTER) && !s.fused_plane &&
          cluster_plane_supported((int)sizeof(T), s.n[1], s.n[2]);
 }
 template <typename T>
-inline cudaError_t launch_plane_cluster_t(const PlaneWork<T>*, int, int, const c2_t<T>*, const c2_t<T>*,
-                                          const c2_t<T>*, cudaStream_t) {
-  return cudaErrorInvalidValue;
-}
-template <>
-inline cudaError_t launch_plane_cluster_t<float>(const PlaneWork<float>* w, int nw, int nx, const float2* ty,
-                                                 const float2* tzh, const float2* tz, cudaStream_t st) {
-  return launch_plane_cluster(w, nw, nx, ty, tzh, tz, st);
+inline cudaError_t launch_plane_cluster_t(const PlaneWork<T>* w, int nw, int nx, const c2_t<T>* ty,
+                                          const c2_t<T>* tzh, const c2_t<T>* tz, cudaStream_t st) {
+  return launch_plane_cluster<T>(w, nw, nx, ty, tzh, tz, st);
 }
 
 template <typename T>

@@ -210,13 +210,15 @@ def test_batch_with_filtered_instances_bit_identical(gpu):
             s.close()
 
 
-def test_batch_class_with_cluster_plane_pass(gpu):
-    """A size class of 8 x 256 x 256 FP32 instances with the cluster plane pass
-    forced (variant 16: one merged plane launch covers every member's sweeps):
-    each instance bit-identical to its single run with the same variant."""
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_class_with_cluster_plane_pass(gpu, precision):
+    """A size class of 8 x 256 x 256 instances with the cluster plane pass forced
+    (variant 16: one merged plane launch covers every member's sweeps; two CTAs
+    per plane in FP32, four in FP64): each instance bit-identical to its single
+    run with the same variant."""
     items = []
     for i in range(3):
-        cfg, _ = W.diblock32(n=16, precision="mixed")
+        cfg, _ = W.diblock32(n=16, precision=precision)
         cfg = dataclasses.replace(cfg, n=(8, 256, 256), cell=(0.5, 0.03125, 0.03125), seed=700 + i)
         items.append((cfg, W.random_fields(cfg, 0.3)))
     iters = 3

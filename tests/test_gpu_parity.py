@@ -239,6 +239,40 @@ def test_cluster_plane_pass_256(gpu, oracle_lib, base):
     assert rel(b[3], a[3]) < 1e-4
 
 
+@pytest.mark.parametrize("base", [0, 8])
+def test_cluster_plane_pass_256_fp64(gpu, oracle_lib, base):
+    """Variant bit 4 in FP64: 256 x 256 y-z planes (528 KB as a half plane) as one
+    plane pass on a cluster of four CTAs (column quarters for the y FFTs, row
+    quarters for the z passes), against the FP64 oracle at the FP64 tolerance
+    over three iterations, and against the row + y-pencil design."""
+    cfg, w = _slab256("fp64")
+    iters = 3
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(iters)
+    runs = {}
+    for v in (base, base | 16):
+        g = ScftSolver(cfg)
+        g.set_variant(v)
+        g.restore(w)
+        hg = []
+        for _ in range(iters):
+            g.update(1)
+            hg.append(g.scalars())
+        assert g.variant()[0] == v
+        if v & 16:
+            assert_parity(cfg, g, o, hg, ho)
+        runs[v] = ([g.w(i) for i in range(2)], g.propagator(0, 1, A.PS_FROM_HEAD, 20),
+                   hg[-1]["free_energy"])
+        g.close()
+    a, b = runs[base], runs[base | 16]
+    print(f"FP64 cluster vs rows: w {max(rel(b[0][i], a[0][i]) for i in range(2)):.2e}, "
+          f"q {rel(b[1], a[1]):.2e}, dF {abs(b[2] - a[2]):.2e}")
+    for i in range(2):
+        assert rel(b[0][i], a[0][i]) < 1e-11
+    assert rel(b[1], a[1]) < 1e-11
+
+
 def test_cluster_variant_only_where_it_exists(gpu):
     for prec, n in (("mixed", 16), ("fp64", 16)):
         cfg, _ = W.diblock32(n=n, precision=prec)
@@ -247,11 +281,12 @@ def test_cluster_variant_only_where_it_exists(gpu):
             g.set_variant(16)
         assert e.value.code == A.PS_ATTRIB_ERR
         g.close()
-    cfg, _ = _slab256("fp64")  # FP64 256 x 256 planes do not fit two CTAs
-    g = ScftSolver(cfg)
-    with pytest.raises(A.PsError):
+    for prec in ("mixed", "fp64"):  # two CTAs per FP32 plane, four per FP64 plane
+        cfg, _ = _slab256(prec)
+        g = ScftSolver(cfg)
         g.set_variant(16)
-    g.close()
+        assert g.variant()[0] == 16
+        g.close()
 
 
 def test_autotune_picks_a_measured_variant(gpu):
