@@ -403,8 +403,14 @@ void* ps_gpu_batch_stream(const ps_batch* b);
 const char* ps_gpu_batch_last_error(const ps_batch* b);
 
 /* --- Adjoint of the propagator sweeps (no reference counterpart) ----------
- * For one linear block copolymer melt (FP64, two distinct sweeps, block 0
- * starting at a free chain end).  ps_adj_forward computes, from the fields
+ * For one linear block copolymer (FP64, uncharged, monodisperse, block 0
+ * starting at a free chain end; mirror-symmetric chains such as homopolymers
+ * and ABA triblocks run both sweeps).  ps_adj_create takes a one-polymer melt;
+ * ps_adj_create_polymer takes polymer `polymer` of any configuration (a blend
+ * with other polymers and solvents) and then computes that polymer's
+ * contribution to phi and its ln Q: the blend's phi is the sum over its
+ * polymers and solvents, and its dL/dw the sum of the polymers' adjoints and
+ * the solvents' closed-form terms.  ps_adj_forward computes, from the fields
  * w (device, n_fields*N doubles), the densities phi (device, n_fields*N) and
  * ln Q exactly as one iteration of ps_gpu_iterate computes them
  * (PsBlockCopolymer::update, pspolymer/PsBlockCopolymer.cpp:189-239).
@@ -417,6 +423,7 @@ const char* ps_gpu_batch_last_error(const ps_batch* b);
  * per sweep, the interval and the bytes of slice storage. */
 typedef struct ps_adj ps_adj;
 int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out);
+int ps_adj_create_polymer(const ps_config* cfg, int polymer, int checkpoint_interval, ps_adj** out);
 int ps_adj_destroy(ps_adj* a);
 int ps_adj_forward(ps_adj* a, const double* w, double* phi, double* log_q);
 int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w, double* g_box,

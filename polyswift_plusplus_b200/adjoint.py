@@ -36,20 +36,29 @@ def _chk(lib, rc, handle):
 
 
 class ChainAdjoint:
-    """Native forward/adjoint pair for one FP64 configuration (fixed box and ds)."""
+    """Native forward/adjoint pair for one FP64 configuration (fixed box and ds).
 
-    def __init__(self, cfg: ScftConfig, checkpoint: int = 0):
+    ``polymer=None``: ``cfg`` is a one-polymer melt.  ``polymer=i``: the chain
+    is polymer i of ``cfg`` (a blend) and ``forward`` gives its contribution
+    to phi and its ln Q."""
+
+    def __init__(self, cfg: ScftConfig, checkpoint: int = 0, polymer: int | None = None):
         if cfg.precision != "fp64":
             cfg = dataclasses.replace(cfg, precision="fp64")
         self.cfg = cfg
         self._lib = A.load_library()
         self._pc = cfg.to_ps_config()
         h = C.c_void_p()
-        _chk(self._lib, self._lib.ps_adj_create(C.byref(self._pc), int(checkpoint), C.byref(h)), None)
+        if polymer is None:
+            rc = self._lib.ps_adj_create(C.byref(self._pc), int(checkpoint), C.byref(h))
+        else:
+            rc = self._lib.ps_adj_create_polymer(C.byref(self._pc), int(polymer), int(checkpoint), C.byref(h))
+        _chk(self._lib, rc, None)
         self._h = h
+        self.polymer = 0 if polymer is None else int(polymer)
         self.N = cfg.n_total
         self.nf = len(cfg.fields)
-        self.nb = len(cfg.polymers[0].blocks)
+        self.nb = len(cfg.polymers[self.polymer].blocks)
         steps, ck, nbytes = C.c_int(), C.c_int(), C.c_size_t()
         _chk(self._lib, self._lib.ps_adj_info(h, C.byref(steps), C.byref(ck), C.byref(nbytes)), h)
         self.contour_steps, self.checkpoint, self.slice_bytes = steps.value, ck.value, nbytes.value
@@ -174,27 +183,130 @@ class DifferentiableChain:
         self._order.clear()
 
 
+class _PolymerFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, w, box, blend, ip):
+        solver = blend.solvers(box)[ip]
+        phi, lnq = solver.forward(w)
+        ctx.solver = solver
+        ctx.token = solver.forward_count
+        ctx.save_for_backward(w)
+        return phi, torch.tensor(lnq, dtype=torch.float64, device=w.device)
+
+    @staticmethod
+    def backward(ctx, g_phi, g_lnq):
+        (w,) = ctx.saved_tensors
+        s = ctx.solver
+        if s.forward_count != ctx.token:
+            s.forward(w)
+        if g_phi is None:
+            g_phi = torch.zeros((s.nf, s.N), dtype=torch.float64, device=w.device)
+        gl = 0.0 if g_lnq is None else float(g_lnq)
+        gw, gbox, _ = s.backward(g_phi, gl)
+        return gw.view_as(w), torch.as_tensor(gbox, dtype=torch.float64), None, None
+
+
+class DifferentiableBlend:
+    """phi, ln Q = blend(w, box) for a blend of linear block copolymers (mirror-symmetric chains
+    and homopolymers included) and simple solvents.
+
+    phi (n_fields, N) is the sum of every species' density and ln Q holds the polymers' ln Q in
+    configuration order, then the solvents'.  Each polymer runs the native adjoint
+    (``ps_adj_create_polymer``); a simple solvent is closed form
+    (pssolvent/PsSimpleSolvent.cpp:86-140): wf = exp(-w_f / L_0), Q_s = mean(wf),
+    phi_f += vf_s wf / Q_s, with L_0 the length of polymer 0, differentiated by torch.  ``box``
+    holds the three box lengths (CPU float64); contour steps are fixed.  Native solvers are built
+    per distinct box and cached.
+    """
+
+    def __init__(self, cfg: ScftConfig, checkpoint: int = 0, cache: int = 4):
+        self.cfg = dataclasses.replace(cfg, precision="fp64")
+        for sv in self.cfg.solvents:
+            if sv.kind != "simpleSolvent":
+                raise ValueError("the blend adjoint takes simple solvents only")
+        self.checkpoint = checkpoint
+        self.scale = float(self.cfg.polymers[0].length)
+        self.box0 = tuple(self.cfg.n[d] * self.cfg.cell[d] for d in range(3))
+        self._cache: dict = {}
+        self._order: list = []
+        self._max = cache
+        self.solvers(self.box0)
+
+    def solvers(self, box) -> list:
+        key = tuple(float(x) for x in box)
+        if key not in self._cache:
+            cell = tuple(key[d] / self.cfg.n[d] for d in range(3))
+            c = dataclasses.replace(self.cfg, cell=cell)
+            self._cache[key] = [ChainAdjoint(c, self.checkpoint, polymer=i) for i in range(len(c.polymers))]
+            self._order.append(key)
+            while len(self._order) > self._max:
+                for s in self._cache.pop(self._order.pop(0)):
+                    s.close()
+        return self._cache[key]
+
+    def __call__(self, w, box=None):
+        box = torch.tensor(self.box0, dtype=torch.float64) if box is None else box
+        phi, lnqs = None, []
+        for ip in range(len(self.cfg.polymers)):
+            p, q = _PolymerFn.apply(w, box, self, ip)
+            phi = p if phi is None else phi + p
+            lnqs.append(q)
+        for sv in self.cfg.solvents:
+            f = self.cfg.field_index(sv.scfield)
+            wf = torch.exp(-w[f] / self.scale)
+            q = wf.mean()
+            add = torch.zeros_like(phi)
+            add[f] = (sv.volfrac / q) * wf
+            phi = phi + add
+            lnqs.append(torch.log(q))
+        return phi, torch.stack(lnqs)
+
+    def species_weights(self) -> tuple[list, list]:
+        """(vf, alpha) per entry of ln Q for free_energy: alpha = L_p / L_0 for a polymer and
+        1 / L_0 for a solvent (pseffhamil/PsPolymerUpdater.cpp:173-226)."""
+        vf = [p.volfrac for p in self.cfg.polymers] + [sv.volfrac for sv in self.cfg.solvents]
+        al = [p.length / self.scale for p in self.cfg.polymers] + [1.0 / self.scale for _ in self.cfg.solvents]
+        return vf, al
+
+    def close(self):
+        for ss in self._cache.values():
+            for s in ss:
+                s.close()
+        self._cache.clear()
+        self._order.clear()
+
+
 def dens_avg(cfg: ScftConfig, f: torch.Tensor | None = None) -> list:
-    """Average density of each field, sum_polymers vf * (length fraction of its blocks)."""
-    p = cfg.polymers[0]
+    """Average density of each field: sum over polymers of vf * (length fraction of its blocks),
+    plus each solvent's vf on its field.  ``f`` overrides polymer 0's block fractions."""
     out = [0.0] * len(cfg.fields)
-    for i, b in enumerate(p.blocks):
-        frac = b.lengthfrac if f is None else f[i]
-        out[cfg.field_index(b.scfield)] = out[cfg.field_index(b.scfield)] + p.volfrac * frac
+    for ip, p in enumerate(cfg.polymers):
+        for i, b in enumerate(p.blocks):
+            frac = b.lengthfrac if (f is None or ip > 0) else f[i]
+            out[cfg.field_index(b.scfield)] = out[cfg.field_index(b.scfield)] + p.volfrac * frac
+    for sv in cfg.solvents:
+        out[cfg.field_index(sv.scfield)] = out[cfg.field_index(sv.scfield)] + sv.volfrac
     return out
 
 
 def free_energy(w, phi, lnq, chin, avg, vf=1.0, alpha=1.0, pairs=None):
-    """F = -vf ln Q / alpha + mean_r[-sum_i phi_i w_i + sum_pairs chiN_ij (phi_i phi_j - avg_i avg_j)]
-    (pseffhamil/PsPolymerUpdater.cpp:173-226, pseffhamil/PsFloryInteraction.cpp:275-321,
-    disorder term subtracted).  Two fields: ``chin`` is the A-B chiN; otherwise ``pairs`` lists
-    (i, j, chiN_ij) and ``chin`` is ignored."""
+    """F = -sum_species vf ln Q / alpha + mean_r[-sum_i phi_i w_i + sum_pairs chiN_ij (phi_i phi_j
+    - avg_i avg_j)] (pseffhamil/PsPolymerUpdater.cpp:173-226, pseffhamil/PsFloryInteraction.cpp:275-321,
+    disorder term subtracted).  One species: scalar ``lnq``, ``vf``, ``alpha``; a blend: ``lnq`` a
+    1-d tensor and ``vf``, ``alpha`` sequences (``DifferentiableBlend.species_weights``).  Two
+    fields: ``chin`` is the A-B chiN; otherwise ``pairs`` lists (i, j, chiN_ij) and ``chin`` is
+    ignored."""
     if pairs is None:
         pairs = [(0, 1, chin)]
     inter = 0.0
     for i, j, c in pairs:
         inter = inter + c * (phi[i] * phi[j] - avg[i] * avg[j])
     field = (-(phi * w).sum(0) + inter).mean()
+    if torch.is_tensor(lnq) and lnq.dim() > 0:
+        species = 0.0
+        for k in range(lnq.shape[0]):
+            species = species - vf[k] * lnq[k] / alpha[k]
+        return species + field
     return -vf * lnq / alpha + field
 
 

@@ -26,6 +26,13 @@
 // (C+1)-slice buffers, and the recomputed slices equal the stored ones bit for
 // bit.  The quadrature and each adjoint sweep recompute the segments once.
 //
+// Branched (tree) chains keep every slice of every sweep (no checkpoints): the
+// forward is the engine's own sweeps with junction products, and the adjoint
+// sweeps run in reverse dependency order.  A sweep that starts at a junction,
+// q_0 = prod_j q^(j)_end, hands its lam_0 back to each arriving sweep's end:
+// lam^(j)_end += lam_0 prod_{j' != j} q^(j')_end, before that sweep's adjoint
+// starts.
+//
 // Every launch and descriptor is fixed at creation; reductions use a fixed
 // grid and are summed on the host in a fixed order, so results are
 // deterministic.
@@ -70,6 +77,16 @@ struct AdjPoint {
   int n_src;
   SrcEntry src[2];
   const double* q_partner;  // Q source partner (nullptr: none at this slice)
+  const double* extra;      // adj_init only: junction contributions to lambda (nullptr: none)
+};
+
+// lam_out[j] += lam0 * prod_{i != j} q_in[i] for the sweeps arriving at a
+// junction (the adjoint of the junction product).
+struct JunctionAdj {
+  const double* lam0;
+  int n;
+  const double* q_in[PS_MAX_JOINS];
+  double* lam_out[PS_MAX_JOINS];
 };
 
 struct BlockFieldMap {
@@ -197,7 +214,21 @@ __global__ void adj_init_kernel(const AdjPoint* __restrict__ pp, long long N, co
     for (int i = 0; i < p.n_src; ++i) s += p.src[i].coef * p.src[i].gphi[r] * p.src[i].partner[r];
     double l = inv_q * s;
     if (p.q_partner) l += gqn * p.q_partner[r];
+    if (p.extra) l += p.extra[r];
     p.lam_out[r] = l;
+  }
+}
+
+__global__ void adj_junction_kernel(const JunctionAdj* __restrict__ jp, long long N) {
+  const JunctionAdj j = *jp;
+  ADJ_LOOP(r, N) {
+    const double l = j.lam0[r];
+    for (int i = 0; i < j.n; ++i) {
+      double v = l;
+      for (int k = 0; k < j.n; ++k)
+        if (k != i) v *= j.q_in[k][r];
+      j.lam_out[i][r] += v;
+    }
   }
 }
 
@@ -261,6 +292,7 @@ using Op = std::function<cudaError_t(cudaStream_t)>;
 struct ps_adj {
   ps_handle* h = nullptr;
   std::string err;
+  int ip = 0;  // the polymer of the configuration this adjoint differentiates
   int M = 0, C = 1, J = 0, nb = 0, nf = 0;
   long long N = 0;
   int n0 = 0;  // sweep-0 index of block 0's head slice (Q = <q_n0 q+_{M-n0}>)
@@ -290,6 +322,14 @@ struct ps_adj {
   std::vector<psb::AccumEntry> h_acc;
   std::vector<psb::AdjPoint> h_pt;
   std::vector<Op> fwd, bwd;
+  // branched chains: the polymer's executed sweeps (h->sweeps indices, in
+  // dependency order), the steps' blocks, junction accumulators, descriptors
+  bool tree = false;
+  std::vector<int> tsw;
+  std::vector<std::vector<int>> tblk;
+  std::vector<double*> jacc;
+  std::vector<psb::JunctionAdj> h_jn;
+  psb::JunctionAdj* d_jn = nullptr;
   size_t storage_bytes = 0;
   size_t E_off = 0, gq_off = 0;  // offsets (in doubles) into part
   bool have_forward = false;
@@ -317,13 +357,13 @@ struct Builder {
   bool fused;
 
   const double* wf(int b) const {
-    const BlockMap& bm = h->blocks[0][b];
+    const BlockMap& bm = h->blocks[a->ip][b];
     for (size_t i = 0; i < h->wfac_keys.size(); ++i)
       if (h->wfac_keys[i].field == bm.field && h->wfac_keys[i].ds == bm.ds) return h->bd.wfac[i];
     return nullptr;
   }
   int ktab(int b) const {
-    const BlockMap& bm = h->blocks[0][b];
+    const BlockMap& bm = h->blocks[a->ip][b];
     for (size_t i = 0; i < h->ktab_keys.size(); ++i)
       if (h->ktab_keys[i].first == bm.ds && h->ktab_keys[i].second == bm.bseg) return (int)i;
     return 0;
@@ -450,7 +490,7 @@ static void fill_sources(ps_adj* a, AdjPoint& p, int sig, int idx, int j) {
   const int n = (sig == 0) ? idx : a->M - idx;
   p.n_src = 0;
   for (auto& e : a->quad[n]) {
-    const int f = a->h->blocks[0][e.first].field;
+    const int f = a->h->blocks[a->ip][e.first].field;
     SrcEntry s;
     s.gphi = a->gphi + (size_t)f * a->N;
     s.partner = slice_ptr(a, 1 - sig, a->M - idx, j);
@@ -461,17 +501,20 @@ static void fill_sources(ps_adj* a, AdjPoint& p, int sig, int idx, int j) {
   p.q_partner = (idx == qslice) ? slice_ptr(a, 1 - sig, a->M - idx, j) : nullptr;
 }
 
-static void adjoint_step(Builder& B, std::vector<Op>& ops, int sig, int s, int j, int cur) {
+// One adjoint step through block b: mu = wf G(wf lam_next), the stress
+// partials of (U, V) = (FFT(wf lam_next), FFT(wf q_s)), dL/dw of the step and,
+// when lam_out is set, lam_s = mu + the explicit sources of slice s (in `src`).
+static void adjoint_step_p(Builder& B, std::vector<Op>& ops, int b, const double* q_s, const double* q_next,
+                           const double* lam_next, double* lam_out, const AdjPoint& src) {
   ps_adj* a = B.a;
   ps_handle* h = B.h;
-  const int b = a->blk[sig][s];
   const double* wfb = B.wf(b);
-  const BlockMap& bm = h->blocks[0][b];
+  const BlockMap& bm = h->blocks[a->ip][b];
   const int slot = (int)a->slot_block.size();
   a->slot_block.push_back(b);
   // U = FFT(wf lam_{s+1}) in spec[0], V = FFT(wf q_s) in spec[1]
-  const size_t p0 = B.plane(B.pw(MODE_FIRST, a->lam[cur], a->spec[0], nullptr, wfb, nullptr));
-  B.plane(B.pw(MODE_FIRST, slice_ptr(a, sig, s, j), a->spec[1], nullptr, wfb, nullptr));
+  const size_t p0 = B.plane(B.pw(MODE_FIRST, lam_next, a->spec[0], nullptr, wfb, nullptr));
+  B.plane(B.pw(MODE_FIRST, q_s, a->spec[1], nullptr, wfb, nullptr));
   const size_t y0 = B.pencil(B.xw(a->spec[0], -1));
   B.pencil(B.xw(a->spec[1], -1));
   B.real_pass(ops, p0, 2, y0, MODE_FIRST);
@@ -497,18 +540,17 @@ static void adjoint_step(Builder& B, std::vector<Op>& ops, int sig, int s, int j
   const size_t p1 = B.plane(B.pw(MODE_LAST, nullptr, a->spec[0], wfb, nullptr, a->mu));
   const size_t y1 = B.pencil(B.xw(a->spec[0], -1));
   B.real_pass(ops, p1, 1, y1, MODE_LAST);
-  AdjPoint p;
-  memset(&p, 0, sizeof(p));
+  AdjPoint p = src;
   p.mu = a->mu;
-  p.lam_next = a->lam[cur];
-  p.q_s = slice_ptr(a, sig, s, j);
-  p.q_next = slice_ptr(a, sig, s + 1, j);
+  p.lam_next = lam_next;
+  p.q_s = q_s;
+  p.q_next = q_next;
   p.w = h->d_w + (size_t)bm.field * a->N;
   p.gwb = a->gwb + (size_t)b * a->N;
-  p.lam_out = (s >= 1) ? a->lam[1 - cur] : nullptr;
+  p.lam_out = lam_out;
   p.dsw_part = a->part + poff + 3 * kAdjRB;
   p.half_ds = 0.5 * bm.ds;
-  if (s >= 1) fill_sources(a, p, sig, s, j);
+  p.extra = nullptr;
   a->h_pt.push_back(p);
   const size_t pi = a->h_pt.size() - 1;
   const long long N = a->N;
@@ -516,6 +558,15 @@ static void adjoint_step(Builder& B, std::vector<Op>& ops, int sig, int s, int j
     adj_point_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->d_pt + pi, N, h->d_sc, a->gq);
     return cudaGetLastError();
   });
+}
+
+static void adjoint_step(Builder& B, std::vector<Op>& ops, int sig, int s, int j, int cur) {
+  ps_adj* a = B.a;
+  AdjPoint src;
+  memset(&src, 0, sizeof(src));
+  if (s >= 1) fill_sources(a, src, sig, s, j);
+  adjoint_step_p(B, ops, a->blk[sig][s], slice_ptr(a, sig, s, j), slice_ptr(a, sig, s + 1, j), a->lam[cur],
+                 (s >= 1) ? a->lam[1 - cur] : nullptr, src);
 }
 
 static void adjoint_init(ps_adj* a, std::vector<Op>& ops, int sig, int j, int cur) {
@@ -545,42 +596,289 @@ static BlockFieldMap field_map(ps_adj* a) {
   memset(&fm, 0, sizeof(fm));
   fm.nb = a->nb;
   fm.nf = a->nf;
-  for (int b = 0; b < a->nb; ++b) fm.field[b] = a->h->blocks[0][b].field;
+  for (int b = 0; b < a->nb; ++b) fm.field[b] = a->h->blocks[a->ip][b].field;
   return fm;
 }
 
-static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
+
+// Branched chain (see the header): every slice stored by the engine's sweeps.
+static int tree_build(ps_adj* a, const ps_config* cfg, int polymer) {
+  ps_handle* h = a->h;
+  const int ip = polymer;
+  a->tree = true;
+  a->C = 1;
+  a->J = 0;
+  a->N = h->N;
+  a->nf = h->nf;
+  a->nb = (int)h->blocks[ip].size();
+  const long long N = a->N;
+  std::vector<int> pos(h->sweeps.size(), -1);  // h->sweeps index -> position in tsw
+  for (int e : h->exec)
+    if (h->sweeps[e].polymer == ip) {
+      pos[e] = (int)a->tsw.size();
+      a->tsw.push_back(e);
+    }
+  const int ns = (int)a->tsw.size();
+  auto S = [h](int sweep, int idx) -> double* {
+    return h->bd.slices[h->sweeps[sweep].storage] + (size_t)idx * h->N;
+  };
+  int steps_total = 0;
+  size_t slice_count = 0;
+  a->tblk.resize(ns);
+  for (int t = 0; t < ns; ++t) {
+    const Sweep& sw = h->sweeps[a->tsw[t]];
+    a->tblk[t].assign(sw.total, 0);
+    for (const Seg& g : sw.segs)
+      for (int k = 0; k < g.steps; ++k) a->tblk[t][g.off + k] = g.block;
+    steps_total += sw.total;
+    slice_count += (size_t)sw.total + 1;
+  }
+  a->M = 0;
+  for (int b = 0; b < a->nb; ++b) a->M += h->blocks[ip][b].steps;
+  // explicit sources per (sweep position, slice): quadrature pairs and Q
+  struct Src {
+    int block;
+    double coef;
+    int psweep, pidx;
+  };
+  std::vector<std::vector<std::vector<Src>>> src(ns);
+  for (int t = 0; t < ns; ++t) src[t].resize(h->sweeps[a->tsw[t]].total + 1);
+  const ps_polymer_config& P = cfg->polymers[ip];
+  const double densfac = 1.0 * P.volfrac / h->alpha[ip];
+  for (int b = 0; b < a->nb; ++b) {
+    const BlockMap& bm = h->blocks[ip][b];
+    const std::vector<double> c = quad_weights(bm.steps);
+    for (int n = 0; n <= bm.steps; ++n) {
+      const double coef = densfac * bm.ds * c[n];
+      const int hi = bm.off_head + n, ti = bm.off_tail + bm.steps - n;
+      src[pos[bm.sweep_head]][hi].push_back({b, coef, bm.sweep_tail, ti});
+      src[pos[bm.sweep_tail]][ti].push_back({b, coef, bm.sweep_head, hi});
+      AccumEntry ae;
+      ae.dst = a->P + (size_t)b * N;
+      ae.x = S(bm.sweep_head, hi);
+      ae.y = S(bm.sweep_tail, ti);
+      ae.coef = coef;
+      a->h_acc.push_back(ae);
+    }
+  }
+  for (auto& v : src)
+    for (auto& e : v)
+      if (e.size() > 2) {
+        a->err = "more than two quadrature pairs on one contour slice";
+        return PS_INPUT_ERR;
+      }
+  const BlockMap& b0 = h->blocks[ip][0];
+  const int qh_sw = b0.sweep_head, qh_i = b0.off_head;
+  const int qt_sw = b0.sweep_tail, qt_i = b0.off_tail + b0.steps;
+  auto fill = [&](AdjPoint& p, int t, int i) {
+    p.n_src = 0;
+    for (const Src& e : src[t][i]) {
+      SrcEntry se;
+      se.gphi = a->gphi + (size_t)h->blocks[ip][e.block].field * N;
+      se.partner = S(e.psweep, e.pidx);
+      se.coef = e.coef;
+      p.src[p.n_src++] = se;
+    }
+    const int sw = a->tsw[t];
+    p.q_partner = (sw == qh_sw && i == qh_i) ? S(qt_sw, qt_i) : (sw == qt_sw && i == qt_i) ? S(qh_sw, qh_i) : nullptr;
+  };
+  // junction accumulators: one per sweep whose end feeds a junction
+  a->jacc.assign(ns, nullptr);
+  const size_t NB = sizeof(double) * (size_t)N;
+  PA_CUDA(a, cudaSetDevice(h->dev));
+  for (int t = 0; t < ns; ++t)
+    for (auto& in : h->sweeps[a->tsw[t]].jin) {
+      const int u = pos[in.first];
+      if (u < 0 || in.second != h->sweeps[in.first].total) {
+        a->err = "junction input is not the end of one of this polymer's sweeps";
+        return PS_INPUT_ERR;
+      }
+      if (!a->jacc[u]) PA_CUDA(a, cudaMalloc((void**)&a->jacc[u], NB));
+    }
+  for (int sg = 0; sg < 2; ++sg) {
+    PA_CUDA(a, cudaMalloc((void**)&a->lam[sg], NB));
+    PA_CUDA(a, cudaMalloc((void**)&a->spec[sg], sizeof(double2) * (size_t)h->n[0] * h->n[1] * h->nzh));
+  }
+  a->storage_bytes = NB * slice_count;
+  PA_CUDA(a, cudaMalloc((void**)&a->mu, NB));
+  PA_CUDA(a, cudaMalloc((void**)&a->gwb, NB * a->nb));
+  PA_CUDA(a, cudaMalloc((void**)&a->gphi, NB * a->nf));
+  PA_CUDA(a, cudaMemset(a->gphi, 0, NB * a->nf));
+  PA_CUDA(a, cudaMalloc((void**)&a->gq, sizeof(double)));
+  a->E_off = (size_t)steps_total * 4 * kAdjRB;
+  a->gq_off = a->E_off + (size_t)a->nb * kAdjRB;
+  a->part_len = a->gq_off + kAdjRB;
+  PA_CUDA(a, cudaMalloc((void**)&a->part, sizeof(double) * a->part_len));
+  PA_CUDA(a, cudaMemset(a->part, 0, sizeof(double) * a->part_len));
+  PA_CUDA(a, cudaMallocHost((void**)&a->h_part, sizeof(double) * a->part_len));
+  // a->P was sized before the accumulation entries pointed at it
+  Builder B;
+  B.a = a;
+  B.h = h;
+  B.nx = h->n[0];
+  B.ny = h->n[1];
+  B.nz = h->n[2];
+  B.nzh = h->nzh;
+  B.fused = plane_fused_supported(8, h->n[1], h->n[2]);
+  const BlockFieldMap fm = field_map(a);
+
+  // ---- forward: the engine's sweeps (every slice stored), Q, quadrature
+  a->fwd.push_back([h](cudaStream_t) {
+    long long nl = 0;
+    return engine_sweeps(h, &nl, 0) == PS_OK ? cudaSuccess : cudaErrorLaunchFailure;
+  });
+  {
+    const double* qx = S(qh_sw, qh_i);
+    const double* qy = S(qt_sw, qt_i);
+    a->fwd.push_back([=](cudaStream_t st) {
+      cudaError_t e = launch_dot_partials<double>(qx, qy, N, h->d_qpart, st);
+      if (e == cudaSuccess) e = launch_finalize_q(h->d_qpart, (double)N, 0, h->d_sc, st);
+      return e;
+    });
+    a->fwd.push_back([=](cudaStream_t st) { return cudaMemsetAsync(a->P, 0, sizeof(double) * N * a->nb, st); });
+    const int ne = (int)a->h_acc.size();
+    a->fwd.push_back([=](cudaStream_t st) {
+      adj_accum_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->d_acc, ne, N);
+      return cudaGetLastError();
+    });
+    a->fwd.push_back([=](cudaStream_t st) {
+      adj_normalize_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->P, h->d_phi, fm, N, h->d_sc);
+      return cudaGetLastError();
+    });
+  }
+  // ---- backward (bwd[0]: the <g_phi, phi> reduction, as for linear chains)
+  {
+    const long long nfN = (long long)a->nf * N;
+    a->bwd.push_back([=](cudaStream_t st) {
+      adj_dot_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->gphi, h->d_phi, nfN, a->part + a->gq_off);
+      return cudaGetLastError();
+    });
+    for (int b = 0; b < a->nb; ++b) {
+      const int f = h->blocks[ip][b].field;
+      a->bwd.push_back([=](cudaStream_t st) {
+        adj_dot_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->gphi + (size_t)f * N, a->P + (size_t)b * N, N,
+                                                  a->part + a->E_off + (size_t)b * kAdjRB);
+        return cudaGetLastError();
+      });
+    }
+    a->bwd.push_back([=](cudaStream_t st) { return cudaMemsetAsync(a->gwb, 0, sizeof(double) * N * a->nb, st); });
+    for (int t = 0; t < ns; ++t)
+      if (a->jacc[t]) {
+        double* jb = a->jacc[t];
+        a->bwd.push_back([=](cudaStream_t st) { return cudaMemsetAsync(jb, 0, NB, st); });
+      }
+    for (int t = ns - 1; t >= 0; --t) {
+      const int sw = a->tsw[t];
+      const Sweep& swp = h->sweeps[sw];
+      const int T = swp.total;
+      const bool junction = !swp.jin.empty();
+      int cur = 0;
+      {
+        AdjPoint p;
+        memset(&p, 0, sizeof(p));
+        p.lam_out = a->lam[cur];
+        fill(p, t, T);
+        p.extra = a->jacc[t];
+        a->h_pt.push_back(p);
+        const size_t pi = a->h_pt.size() - 1;
+        a->bwd.push_back([=](cudaStream_t st) {
+          adj_init_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->d_pt + pi, N, h->d_sc, a->gq);
+          return cudaGetLastError();
+        });
+      }
+      for (int st_ = T - 1; st_ >= 0; --st_) {
+        AdjPoint p;
+        memset(&p, 0, sizeof(p));
+        const bool out = (st_ >= 1) || junction;
+        if (out) fill(p, t, st_);
+        adjoint_step_p(B, a->bwd, a->tblk[t][st_], S(sw, st_), S(sw, st_ + 1), a->lam[cur],
+                       out ? a->lam[1 - cur] : nullptr, p);
+        if (out) cur = 1 - cur;
+      }
+      if (junction) {
+        JunctionAdj jn;
+        memset(&jn, 0, sizeof(jn));
+        jn.lam0 = a->lam[cur];
+        jn.n = (int)swp.jin.size();
+        for (int i = 0; i < jn.n; ++i) {
+          jn.q_in[i] = S(swp.jin[i].first, swp.jin[i].second);
+          jn.lam_out[i] = a->jacc[pos[swp.jin[i].first]];
+        }
+        a->h_jn.push_back(jn);
+        const size_t ji = a->h_jn.size() - 1;
+        a->bwd.push_back([=](cudaStream_t st) {
+          adj_junction_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->d_jn + ji, N);
+          return cudaGetLastError();
+        });
+      }
+    }
+  }
+  int r2 = adj_upload(a, &a->d_pw, a->h_pw);
+  if (!r2) r2 = adj_upload(a, &a->d_xw, a->h_xw);
+  if (!r2) r2 = adj_upload(a, &a->d_acc, a->h_acc);
+  if (!r2) r2 = adj_upload(a, &a->d_pt, a->h_pt);
+  if (!r2) r2 = adj_upload(a, &a->d_jn, a->h_jn);
+  return r2;
+}
+
+// polymer: the linear chain of cfg to differentiate (its phi contribution and
+// ln Q); single: the configuration must be a one-polymer melt (ps_adj_create).
+static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, int checkpoint) {
   if (cfg->precision != PS_PREC_FP64) {
     a->err = "the adjoint runs in FP64 (precision must be PS_PREC_FP64)";
     return PS_ATTRIB_ERR;
   }
-  if (cfg->n_polymers != 1 || cfg->n_solvents != 0 || cfg->n_charges != 0 ||
-      cfg->polydisperse[0].enabled) {
-    a->err = "the adjoint takes one polymer (a linear block copolymer melt) and no solvent";
+  if (polymer < 0 || polymer >= cfg->n_polymers) {
+    a->err = "polymer index out of range";
+    return PS_ATTRIB_ERR;
+  }
+  if (single && (cfg->n_polymers != 1 || cfg->n_solvents != 0)) {
+    a->err = "ps_adj_create takes one polymer and no solvent (ps_adj_create_polymer takes a blend)";
     return PS_INPUT_ERR;
   }
+  if (cfg->n_charges != 0 || cfg->polydisperse[polymer].enabled) {
+    a->err = "the adjoint takes uncharged, monodisperse chains";
+    return PS_INPUT_ERR;
+  }
+  a->ip = polymer;
   a->h = new ps_handle();
   a->h->no_slices = true;
+  a->h->no_alias = true;  // mirror-symmetric chains: both sweeps run and are differentiated
   int rc = engine_create(a->h, cfg);
   if (rc) {
     a->err = a->h->err;
     return rc;
   }
   ps_handle* h = a->h;
-  if (h->branched) {
-    a->err = "the adjoint takes a linear chain (this polymer is branched)";
+  std::vector<int> own;  // this polymer's sweeps
+  for (int k = 0; k < (int)h->sweeps.size(); ++k)
+    if (h->sweeps[k].polymer == polymer) own.push_back(k);
+  bool linear = (own.size() == 2);
+  for (int k : own) linear = linear && h->sweeps[k].jin.empty();
+  if (!linear) {
+    // a branched chain: rebuild the engine with slice storage
+    engine_free(a->h);
+    delete a->h;
+    a->h = new ps_handle();
+    a->h->no_slices = false;
+    rc = engine_create(a->h, cfg);
+    if (rc) {
+      a->err = a->h->err;
+      return rc;
+    }
+    PA_CUDA(a, cudaMalloc((void**)&a->P, sizeof(double) * (size_t)a->h->N * a->h->blocks[polymer].size()));
+    return tree_build(a, cfg, polymer);
+  }
+  const Sweep& s0 = h->sweeps[own[0]];
+  const Sweep& s1 = h->sweeps[own[1]];
+  if (s0.storage < 0 || s1.storage < 0 || s0.storage == s1.storage) {
+    a->err = "the adjoint needs two executed sweeps";
     return PS_INPUT_ERR;
   }
-  if (h->exec.size() != 2) {
-    a->err = "the adjoint needs two distinct sweeps (mirror-symmetric chains are not supported)";
-    return PS_INPUT_ERR;
-  }
-  const Sweep& s0 = h->sweeps[h->exec[0]];
-  const Sweep& s1 = h->sweeps[h->exec[1]];
   a->M = s0.total;
   a->N = h->N;
   a->nf = h->nf;
-  a->nb = (int)h->blocks[0].size();
+  a->nb = (int)h->blocks[a->ip].size();
   const int M = a->M;
   for (int sg = 0; sg < 2; ++sg) {
     const Sweep& sw = sg ? s1 : s0;
@@ -590,12 +888,12 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
   }
   // quadrature pairs in sweep-0 indexing: (q_n, q+_{M-n})
   a->quad.assign(M + 1, {});
-  const ps_polymer_config& P = cfg->polymers[0];
-  const double densfac = 1.0 * P.volfrac / h->alpha[0];
+  const ps_polymer_config& P = cfg->polymers[polymer];
+  const double densfac = 1.0 * P.volfrac / h->alpha[polymer];
   for (int b = 0; b < a->nb; ++b) {
-    const BlockMap& bm = h->blocks[0][b];
+    const BlockMap& bm = h->blocks[a->ip][b];
     const std::vector<double> c = quad_weights(bm.steps);
-    const bool head0 = (h->sweeps[bm.sweep_head].storage == 0);
+    const bool head0 = (h->sweeps[bm.sweep_head].storage == s0.storage);
     const int o = head0 ? bm.off_head : M - bm.off_head - bm.steps;  // block start in sweep 0
     for (int n = o; n <= o + bm.steps; ++n) {
       const int loc = head0 ? n - o : o + bm.steps - n;
@@ -608,8 +906,8 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
       return PS_INPUT_ERR;
     }
   {
-    const BlockMap& b0 = h->blocks[0][0];
-    const bool head0 = (h->sweeps[b0.sweep_head].storage == 0);
+    const BlockMap& b0 = h->blocks[a->ip][0];
+    const bool head0 = (h->sweeps[b0.sweep_head].storage == s0.storage);
     a->n0 = head0 ? b0.off_head : M - b0.off_head;
     if (a->n0 != 0 && a->n0 != M) {
       a->err = "the adjoint needs block 0 to start at a free chain end";
@@ -717,7 +1015,7 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int checkpoint) {
       return cudaGetLastError();
     });
     for (int b = 0; b < a->nb; ++b) {
-      const int f = h->blocks[0][b].field;
+      const int f = h->blocks[a->ip][b].field;
       a->bwd.push_back([=](cudaStream_t st) {
         adj_dot_kernel<<<kAdjRB, kAdjRT, 0, st>>>(a->gphi + (size_t)f * N, a->P + (size_t)b * N, N,
                                                   a->part + a->E_off + (size_t)b * kAdjRB);
@@ -777,6 +1075,8 @@ static void adj_free(ps_adj* a) {
   f(a->d_xw);
   f(a->d_acc);
   f(a->d_pt);
+  f(a->d_jn);
+  for (auto p : a->jacc) f(p);
   if (a->h) {
     engine_free(a->h);
     delete a->h;
@@ -794,14 +1094,14 @@ using namespace psb;
 
 extern "C" {
 
-int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out) {
+static int adj_create(const ps_config* cfg, int polymer, bool single, int checkpoint_interval, ps_adj** out) {
   if (!cfg || !out) {
     g_adj_err = "null argument";
     return PS_ATTRIB_ERR;
   }
   *out = nullptr;
   ps_adj* a = new ps_adj();
-  int rc = adj_build(a, cfg, checkpoint_interval);
+  int rc = adj_build(a, cfg, polymer, single, checkpoint_interval);
   if (rc) {
     g_adj_err = a->err;
     adj_free(a);
@@ -811,6 +1111,14 @@ int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out) {
   }
   *out = a;
   return PS_OK;
+}
+
+int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out) {
+  return adj_create(cfg, 0, true, checkpoint_interval, out);
+}
+
+int ps_adj_create_polymer(const ps_config* cfg, int polymer, int checkpoint_interval, ps_adj** out) {
+  return adj_create(cfg, polymer, false, checkpoint_interval, out);
 }
 
 int ps_adj_destroy(ps_adj* a) {
@@ -883,7 +1191,7 @@ int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w,
   const double L[3] = {h->n[0] * h->cfg.cell[0], h->n[1] * h->cfg.cell[1], h->n[2] * h->cfg.cell[2]};
   for (size_t slot = 0; slot < a->slot_block.size(); ++slot) {
     const int b = a->slot_block[slot];
-    const BlockMap& bm = h->blocks[0][b];
+    const BlockMap& bm = h->blocks[a->ip][b];
     const double* p = a->h_part + slot * 4 * kAdjRB;
     double R[4] = {0.0, 0.0, 0.0, 0.0};
     for (int q = 0; q < 4; ++q)
@@ -895,7 +1203,7 @@ int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w,
   for (int b = 0; b < a->nb; ++b) {
     double E = 0.0;
     for (int i = 0; i < kAdjRB; ++i) E += a->h_part[a->E_off + (size_t)b * kAdjRB + i];
-    gds[b] += E / h->blocks[0][b].ds;
+    gds[b] += E / h->blocks[a->ip][b].ds;
   }
   if (g_box)
     for (int d = 0; d < 3; ++d) g_box[d] = gbox[d];

@@ -66,8 +66,11 @@ __device__ __forceinline__ C mul_mi(C a) {
 // tables, work descriptors), then pdl_wait() blocks until that kernel has
 // completed and its writes are visible; without the attribute pdl_wait() is a
 // no-op.  No kernel triggers its dependents early: blocks of the next sweep
-// kernel parked on pdl_wait() would hold shared memory that the concurrent
-// sweep's kernels need (measured 4% slower at 128^3).
+// kernel parked on pdl_wait() hold shared memory and registers that the
+// concurrent sweep's kernels need.  At 128^3 a trigger after the loads was 4%
+// slower, and a late one (plane pass after its real-space step, pencil pass
+// after its k^2 pass) 2-3% slower, although it cut the time from the last
+// block's exit to the next kernel's release from about 2.5 to 1.6 us.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 }  // namespace psb

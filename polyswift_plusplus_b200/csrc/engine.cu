@@ -939,7 +939,7 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
     a.storage = (int)h->exec.size();
     h->exec.push_back(ia);
     h->sweeps.push_back(a);
-    if (same) {
+    if (same && !h->no_alias) {
       b.storage = a.storage;
     } else {
       b.storage = (int)h->exec.size();

@@ -159,6 +159,7 @@ struct ps_handle {
   bool branched = false;  // a branched polymer: its sweeps run as dependent launch chains only
   int n_jbuf = 0;
   bool no_slices = false; // tables only, no slice storage (the adjoint keeps its own)
+  bool no_alias = false;  // mirror-symmetric chains keep both sweeps (the adjoint differentiates each)
   void* filter = nullptr;  // spectral filter updater (filter.cu), or nullptr
   void* poisson = nullptr; // Poisson updater (poisson.cu), or nullptr
   std::vector<int> post_order;  // updaters after the field update, in run order (POST_*)

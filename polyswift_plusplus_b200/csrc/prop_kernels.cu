@@ -339,6 +339,9 @@ template <> struct PlanY<128> { using type = RadixList<16, 8>; };
 // the forward transform of x_0 + i x_h is split by Hermitian symmetry,
 // A_0[k] = (C[k] + conj(C[-k]))/2, A_h[k] = -i (C[k] - conj(C[-k]))/2.  The y
 // FFT then runs over nz/2 columns instead of nz/2 + 1.
+// The packing and unpacking are loops of their own: folded into the first and
+// last Stockham passes (pencil 0's reads and writes) they made one thread in
+// every other warp diverge, and the 128^3 step took 16.1 instead of 15.4 us.
 template <int ROWS, int NZH, int TH, typename C>
 __device__ __forceinline__ void plane_y_inverse(C* buf, const C* tw) {
   if constexpr (NZH > 1 && ROWS > 1) {

@@ -250,3 +250,234 @@ def test_adjoint_on_split_plane_grid(gpu):
         an = float((gw2 * d).sum())
         print(f"split-plane dL/dw: adjoint {an:.12e} central difference {fd:.12e}")
         assert abs(an - fd) <= TOL * abs(fd), (an, fd)
+
+
+def blend_case(n=16, ns=32):
+    """AB diblock (vf 0.75, f_A = 12/32) + A homopolymer (vf 0.15, half length: a
+    mirror-symmetric chain) + simple solvent on B (vf 0.1), FP64."""
+    from polyswift_plusplus_b200.config import Solvent
+    cfg = W.blend(n, 18.0, 0.375, 0.15, precision="fp64", ns=ns, anderson=False)
+    cfg.polymers[0].volfrac = 0.75
+    cfg = dataclasses.replace(cfg, cell=(0.13, 0.12, 0.125), solvents=[Solvent("solv", "B", 0.1)])
+    _, _, z = W.coords(cfg)
+    c = np.cos(2 * math.pi * z / cfg.box[2]).reshape(-1)
+    w = W.random_fields(cfg, 0.5)
+    return cfg, np.stack([w[0] + c, w[1] - c])
+
+
+def blend_loss(cfg, seed=5):
+    rng = np.random.default_rng(seed)
+    t = torch.tensor(rng.uniform(0.2, 0.8, cfg.n_total), device=DEV)
+    r = torch.tensor(rng.standard_normal(cfg.n_total), device=DEV)
+    c = torch.tensor([0.3, -0.2, 0.1], dtype=torch.float64, device=DEV)
+
+    def L(phi, lnq):
+        return ((phi[0] - t) ** 2).sum() + 0.5 * (phi[1] * r).sum() + (c * lnq).sum()
+    return L
+
+
+def test_blend_adjoint_forward_matches_engine(gpu):
+    """DifferentiableBlend's phi (sum of the diblock's and the homopolymer's native adjoint
+    forwards and the solvent's closed form) and the polymers' ln Q against one engine
+    iteration."""
+    from polyswift_plusplus_b200.adjoint import DifferentiableBlend
+    cfg, w = blend_case()
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.update(1)
+    blend = DifferentiableBlend(cfg, checkpoint=1)
+    with torch.no_grad():
+        phi, lnq = blend(torch.tensor(w, device=DEV))
+    for i in range(2):
+        ref = s.phi(i)
+        assert np.abs(phi[i].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    for ip in range(2):
+        assert float(lnq[ip]) == pytest.approx(s.scalars()["log_q"][ip], rel=1e-13, abs=1e-13)
+    blend.close()
+
+
+def test_blend_adjoint_gradients_match_finite_differences(gpu):
+    """dL/dw and dL/dL_box of a loss over the blend's phi and every species' ln Q, and the
+    stress dF/dL_box of its free energy, against central differences."""
+    from polyswift_plusplus_b200.adjoint import DifferentiableBlend
+    cfg, w = blend_case()
+    L = blend_loss(cfg)
+    blend = DifferentiableBlend(cfg)  # square-root checkpointing
+    wt = torch.tensor(w, device=DEV, requires_grad=True)
+    box = torch.tensor(blend.box0, dtype=torch.float64, requires_grad=True)
+    phi, lnq = blend(wt, box)
+    L(phi, lnq).backward()
+    gw, gbox = wt.grad.detach(), box.grad.detach().clone()
+
+    def at(wv, b):
+        with torch.no_grad():
+            p, q = blend(wv, torch.tensor(b, dtype=torch.float64))
+            return float(L(p, q))
+    w0 = wt.detach()
+    rng = np.random.default_rng(11)
+    for k in range(3):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        if k == 2:
+            d = torch.zeros_like(w0)
+            d[0, 1234] = 1.0
+            d[1, 77] = -0.5
+        eps = 1e-6
+        fd = (at(w0 + eps * d, blend.box0) - at(w0 - eps * d, blend.box0)) / (2 * eps)
+        an = float((gw * d).sum())
+        print(f"blend dL/dw direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    for dim in range(3):
+        h = 1e-6 * blend.box0[dim]
+        bp, bm = list(blend.box0), list(blend.box0)
+        bp[dim] += h
+        bm[dim] -= h
+        fd = (at(w0, bp) - at(w0, bm)) / (2 * h)
+        print(f"blend dL/dL_{dim}: adjoint {gbox[dim].item():.12e} central difference {fd:.12e}")
+        assert abs(gbox[dim].item() - fd) <= TOL * abs(fd), (dim, gbox[dim].item(), fd)
+    # stress of the free energy (fields fixed): F over every species
+    from polyswift_plusplus_b200.adjoint import dens_avg, free_energy
+    avg = dens_avg(cfg)
+    vf, al = blend.species_weights()
+    chin = cfg.interactions[0].chi * cfg.polymers[0].length
+    box = torch.tensor(blend.box0, dtype=torch.float64, requires_grad=True)
+    phi, lnq = blend(w0, box)
+    free_energy(w0, phi, lnq, chin, avg, vf, al).backward()
+
+    def F_at(b):
+        with torch.no_grad():
+            p, q = blend(w0, torch.tensor(b, dtype=torch.float64))
+            return float(free_energy(w0, p, q, chin, avg, vf, al))
+    fds = []
+    for dim in range(3):
+        h = 1e-6 * blend.box0[dim]
+        bp, bm = list(blend.box0), list(blend.box0)
+        bp[dim] += h
+        bm[dim] -= h
+        fds.append((F_at(bp) - F_at(bm)) / (2 * h))
+        print(f"blend dF/dL_{dim}: adjoint {box.grad[dim].item():.12e} central difference {fds[-1]:.12e}")
+    # the stress across the pattern (z) is the large component; the others sit at the
+    # resolution of a central difference of F and are checked against it
+    big = max(abs(x) for x in fds)
+    for dim in range(3):
+        assert abs(box.grad[dim].item() - fds[dim]) <= TOL * big, (dim, box.grad[dim].item(), fds[dim])
+    blend.close()
+
+
+def test_adjoint_mirror_symmetric_chain(gpu):
+    """A symmetric ABA triblock melt (identical sweeps from both ends, aliased in the engine)
+    through ps_adj_create: forward against the engine, dL/dw against central differences."""
+    from polyswift_plusplus_b200.config import Block, Polymer
+    cfg, w = small_case()
+    ds = cfg.polymers[0].blocks[0].ds
+    cfg.polymers[0] = Polymer(name="aba", volfrac=1.0, length=cfg.polymers[0].length, blocks=[
+        Block("aba_A1", "A", ds, 0.25, ["freeEnd"], ["aba_B"], force_block_steps=True),
+        Block("aba_B", "B", ds, 0.5, ["aba_A1"], ["aba_A2"], force_block_steps=True),
+        Block("aba_A2", "A", ds, 0.25, ["aba_B"], ["freeEnd"], force_block_steps=True)])
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.update(1)
+    adj = ChainAdjoint(cfg)
+    wt = torch.tensor(w, device=DEV)
+    phi, lnq = adj.forward(wt)
+    for i in range(2):
+        ref = s.phi(i)
+        assert np.abs(phi[i].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert lnq == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    L = loss_terms(cfg, seed=9)
+    gw, _, _ = grads(adj, wt, L)
+    rng = np.random.default_rng(3)
+    for k in range(2):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        eps = 1e-6
+        fd = (eval_loss(adj, wt + eps * d, L) - eval_loss(adj, wt - eps * d, L)) / (2 * eps)
+        an = float((gw * d).sum())
+        print(f"ABA dL/dw direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    adj.close()
+
+
+def branched_case(kind):
+    """A three-arm ABC star, or the two-junction H-shaped tree (arms A, B and backbone C at one
+    junction, C, D, E at the other), FP64 at 16^3."""
+    from polyswift_plusplus_b200.config import Block, Interaction, Polymer, ScftConfig
+    if kind == "star3":
+        return W.star_abc(n=16)
+    ds = 0.01
+    blocks = [Block("a", "A", ds, 0.15, ["freeEnd"], ["b", "c"]),
+              Block("b", "B", ds, 0.15, ["freeEnd"], ["a", "c"]),
+              Block("c", "C", ds, 0.40, ["a", "b"], ["d", "e"]),
+              Block("d", "A", ds, 0.15, ["freeEnd"], ["c", "e"]),
+              Block("e", "B", ds, 0.15, ["freeEnd"], ["c", "d"])]
+    cfg = ScftConfig(n=(16, 16, 16), cell=(0.2, 0.19, 0.21), fields=["A", "B", "C"],
+                     polymers=[Polymer("h", 1.0, 100, blocks)],
+                     interactions=[Interaction("AB", 0.12, ["A", "B"]), Interaction("BC", 0.12, ["B", "C"]),
+                                   Interaction("AC", 0.15, ["A", "C"])],
+                     updater=Updater(relaxlambdas=(0.05, 0.025)), seed=77, precision="fp64")
+    return cfg, W.random_fields(cfg, 0.4)
+
+
+@pytest.mark.parametrize("kind", ["star3", "tree_h"])
+def test_adjoint_branched_chain(gpu, kind):
+    """Branched chains (every slice stored; junction products differentiated back to the
+    arriving sweeps): forward against the engine, dL/dw, dL/dL_box and dL/d(ds) against
+    central differences."""
+    cfg, w = branched_case(kind)
+    w = np.stack(w)
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.update(1)
+    adj = ChainAdjoint(cfg)
+    assert adj.checkpoint == 1
+    wt = torch.tensor(w, device=DEV)
+    phi, lnq = adj.forward(wt)
+    for i in range(len(cfg.fields)):
+        ref = s.phi(i)
+        assert np.abs(phi[i].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert lnq == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    L = loss_terms(cfg, seed=13)
+    gw, _, _ = grads(adj, wt, L)
+    rng = np.random.default_rng(17)
+    n = cfg.n
+    for k in range(3):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        if k == 2:
+            # localised: a 4^3 patch of field A and one of field C (a single point's derivative is
+            # at the roundoff floor of a central difference of this loss)
+            d = torch.zeros((len(cfg.fields),) + tuple(n), dtype=torch.float64, device=DEV)
+            d[0, 2:6, 3:7, 4:8] = 1.0
+            d[2, 9:13, 10:14, 1:5] = -0.5
+            d = d.reshape(len(cfg.fields), -1)
+        an = float((gw * d).sum())
+        for eps in (1e-6, 1e-5):
+            fd = (eval_loss(adj, wt + eps * d, L) - eval_loss(adj, wt - eps * d, L)) / (2 * eps)
+            print(f"{kind} dL/dw direction {k} (step {eps:g}): adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    adj.close()
+    chain = DifferentiableChain(cfg)
+    box = torch.tensor(chain.box0, dtype=torch.float64, requires_grad=True)
+    ds = torch.tensor(chain.ds0, dtype=torch.float64, requires_grad=True)
+    phi, lnq = chain(wt, box, ds)
+    L(phi, lnq).backward()
+
+    def at(b, dd):
+        with torch.no_grad():
+            p, q = chain(wt, torch.tensor(b, dtype=torch.float64), torch.tensor(dd, dtype=torch.float64))
+            return float(L(p, q))
+    # relative steps of 1e-5: with 1e-6 the roundoff of L (about 400) is 5e-7 in a difference
+    for dim in range(3):
+        h = 1e-5 * chain.box0[dim]
+        bp, bm = list(chain.box0), list(chain.box0)
+        bp[dim] += h
+        bm[dim] -= h
+        fd = (at(bp, chain.ds0) - at(bm, chain.ds0)) / (2 * h)
+        print(f"{kind} dL/dL_{dim}: adjoint {box.grad[dim].item():.12e} central difference {fd:.12e}")
+        assert abs(box.grad[dim].item() - fd) <= TOL * abs(fd), (dim, box.grad[dim].item(), fd)
+    for b in (0, len(chain.ds0) - 1):
+        h = 1e-5 * chain.ds0[b]
+        dp, dm = list(chain.ds0), list(chain.ds0)
+        dp[b] += h
+        dm[b] -= h
+        fd = (at(chain.box0, dp) - at(chain.box0, dm)) / (2 * h)
+        print(f"{kind} dL/dds_{b}: adjoint {ds.grad[b].item():.12e} central difference {fd:.12e}")
+        assert abs(ds.grad[b].item() - fd) <= TOL * abs(fd), (b, ds.grad[b].item(), fd)
+    chain.close()
