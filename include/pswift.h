@@ -403,14 +403,19 @@ void* ps_gpu_batch_stream(const ps_batch* b);
 const char* ps_gpu_batch_last_error(const ps_batch* b);
 
 /* --- Adjoint of the propagator sweeps (no reference counterpart) ----------
- * For one linear block copolymer (FP64, uncharged, monodisperse, block 0
- * starting at a free chain end; mirror-symmetric chains such as homopolymers
- * and ABA triblocks run both sweeps).  ps_adj_create takes a one-polymer melt;
- * ps_adj_create_polymer takes polymer `polymer` of any configuration (a blend
- * with other polymers and solvents) and then computes that polymer's
- * contribution to phi and its ln Q: the blend's phi is the sum over its
- * polymers and solvents, and its dL/dw the sum of the polymers' adjoints and
- * the solvents' closed-form terms.  ps_adj_forward computes, from the fields
+ * For one block copolymer chain (FP64, uncharged): linear chains with block 0
+ * starting at a free end are checkpointed (mirror-symmetric chains such as
+ * homopolymers and ABA triblocks run both sweeps); branched chains keep every
+ * slice.  ps_adj_create takes a one-polymer melt; ps_adj_create_polymer takes
+ * quadrature chain `chain` (0 unless the polymer is a polyDisperseBCP, then
+ * 0..n_g-1) of polymer `polymer` of any configuration (a blend with other
+ * polymers and solvents) and computes that chain's contribution to phi and
+ * its ln Q: the blend's phi is the sum over its chains and solvents, and its
+ * dL/dw the sum of the chains' adjoints and the solvents' closed-form terms.
+ * ps_adj_species reports the chain's free-energy weight (volfrac times the
+ * polydisperse density weight), its length ratio and the configuration's
+ * average density per field (n_fields doubles), for the free energy
+ * F = -sum weight ln Q / ratio + ...  ps_adj_forward computes, from the fields
  * w (device, n_fields*N doubles), the densities phi (device, n_fields*N) and
  * ln Q exactly as one iteration of ps_gpu_iterate computes them
  * (PsBlockCopolymer::update, pspolymer/PsBlockCopolymer.cpp:189-239).
@@ -423,7 +428,9 @@ const char* ps_gpu_batch_last_error(const ps_batch* b);
  * per sweep, the interval and the bytes of slice storage. */
 typedef struct ps_adj ps_adj;
 int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out);
-int ps_adj_create_polymer(const ps_config* cfg, int polymer, int checkpoint_interval, ps_adj** out);
+int ps_adj_create_polymer(const ps_config* cfg, int polymer, int chain, int checkpoint_interval,
+                          ps_adj** out);
+int ps_adj_species(const ps_adj* a, double* f_weight, double* length_ratio, double* dens_avg);
 int ps_adj_destroy(ps_adj* a);
 int ps_adj_forward(ps_adj* a, const double* w, double* phi, double* log_q);
 int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w, double* g_box,

@@ -39,10 +39,11 @@ class ChainAdjoint:
     """Native forward/adjoint pair for one FP64 configuration (fixed box and ds).
 
     ``polymer=None``: ``cfg`` is a one-polymer melt.  ``polymer=i``: the chain
-    is polymer i of ``cfg`` (a blend) and ``forward`` gives its contribution
-    to phi and its ln Q."""
+    is polymer i of ``cfg`` (a blend; quadrature chain ``chain`` of a
+    polyDisperseBCP) and ``forward`` gives its contribution to phi and its
+    ln Q."""
 
-    def __init__(self, cfg: ScftConfig, checkpoint: int = 0, polymer: int | None = None):
+    def __init__(self, cfg: ScftConfig, checkpoint: int = 0, polymer: int | None = None, chain: int = 0):
         if cfg.precision != "fp64":
             cfg = dataclasses.replace(cfg, precision="fp64")
         self.cfg = cfg
@@ -52,7 +53,8 @@ class ChainAdjoint:
         if polymer is None:
             rc = self._lib.ps_adj_create(C.byref(self._pc), int(checkpoint), C.byref(h))
         else:
-            rc = self._lib.ps_adj_create_polymer(C.byref(self._pc), int(polymer), int(checkpoint), C.byref(h))
+            rc = self._lib.ps_adj_create_polymer(C.byref(self._pc), int(polymer), int(chain), int(checkpoint),
+                                                 C.byref(h))
         _chk(self._lib, rc, None)
         self._h = h
         self.polymer = 0 if polymer is None else int(polymer)
@@ -88,6 +90,13 @@ class ChainAdjoint:
                                                   C.c_void_p(gw.data_ptr()), gbox, gds), self._h)
         return (gw.view(self.nf, self.N), np.array([gbox[i] for i in range(3)]),
                 np.array([gds[i] for i in range(self.nb)]))
+
+    def species(self) -> tuple[float, float, list]:
+        """(free-energy weight, length ratio, average density of each field of the configuration)."""
+        wt, lr = C.c_double(), C.c_double()
+        avg = (C.c_double * self.nf)()
+        _chk(self._lib, self._lib.ps_adj_species(self._h, C.byref(wt), C.byref(lr), avg), self._h)
+        return wt.value, lr.value, [avg[i] for i in range(self.nf)]
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -207,12 +216,12 @@ class _PolymerFn(torch.autograd.Function):
 
 
 class DifferentiableBlend:
-    """phi, ln Q = blend(w, box) for a blend of linear block copolymers (mirror-symmetric chains
-    and homopolymers included) and simple solvents.
+    """phi, ln Q = blend(w, box) for a blend of block copolymers (linear, mirror-symmetric,
+    branched or polydisperse) and simple solvents.
 
-    phi (n_fields, N) is the sum of every species' density and ln Q holds the polymers' ln Q in
-    configuration order, then the solvents'.  Each polymer runs the native adjoint
-    (``ps_adj_create_polymer``); a simple solvent is closed form
+    phi (n_fields, N) is the sum of every species' density and ln Q holds the polymers' chains'
+    ln Q in configuration order (n_g entries for a polyDisperseBCP), then the solvents'.  Each
+    chain runs the native adjoint (``ps_adj_create_polymer``); a simple solvent is closed form
     (pssolvent/PsSimpleSolvent.cpp:86-140): wf = exp(-w_f / L_0), Q_s = mean(wf),
     phi_f += vf_s wf / Q_s, with L_0 the length of polymer 0, differentiated by torch.  ``box``
     holds the three box lengths (CPU float64); contour steps are fixed.  Native solvers are built
@@ -232,12 +241,16 @@ class DifferentiableBlend:
         self._max = cache
         self.solvers(self.box0)
 
+    def chains(self) -> list:
+        """(polymer, quadrature chain) of each entry of the polymers' part of ln Q."""
+        return [(i, k) for i, p in enumerate(self.cfg.polymers) for k in range(p.n_chains)]
+
     def solvers(self, box) -> list:
         key = tuple(float(x) for x in box)
         if key not in self._cache:
             cell = tuple(key[d] / self.cfg.n[d] for d in range(3))
             c = dataclasses.replace(self.cfg, cell=cell)
-            self._cache[key] = [ChainAdjoint(c, self.checkpoint, polymer=i) for i in range(len(c.polymers))]
+            self._cache[key] = [ChainAdjoint(c, self.checkpoint, polymer=i, chain=k) for i, k in self.chains()]
             self._order.append(key)
             while len(self._order) > self._max:
                 for s in self._cache.pop(self._order.pop(0)):
@@ -247,7 +260,7 @@ class DifferentiableBlend:
     def __call__(self, w, box=None):
         box = torch.tensor(self.box0, dtype=torch.float64) if box is None else box
         phi, lnqs = None, []
-        for ip in range(len(self.cfg.polymers)):
+        for ip in range(len(self.chains())):
             p, q = _PolymerFn.apply(w, box, self, ip)
             phi = p if phi is None else phi + p
             lnqs.append(q)
@@ -262,11 +275,17 @@ class DifferentiableBlend:
         return phi, torch.stack(lnqs)
 
     def species_weights(self) -> tuple[list, list]:
-        """(vf, alpha) per entry of ln Q for free_energy: alpha = L_p / L_0 for a polymer and
-        1 / L_0 for a solvent (pseffhamil/PsPolymerUpdater.cpp:173-226)."""
-        vf = [p.volfrac for p in self.cfg.polymers] + [sv.volfrac for sv in self.cfg.solvents]
-        al = [p.length / self.scale for p in self.cfg.polymers] + [1.0 / self.scale for _ in self.cfg.solvents]
+        """(vf, alpha) per entry of ln Q for free_energy: a chain's volfrac times its polydisperse
+        density weight and its length ratio L / L_0; vf and 1 / L_0 for a solvent
+        (pseffhamil/PsPolymerUpdater.cpp:173-226)."""
+        sp = [s.species() for s in self.solvers(self.box0)]
+        vf = [x[0] for x in sp] + [sv.volfrac for sv in self.cfg.solvents]
+        al = [x[1] for x in sp] + [1.0 / self.scale for _ in self.cfg.solvents]
         return vf, al
+
+    def dens_avg(self) -> list:
+        """The configuration's average density of each field (the disorder reference of F)."""
+        return self.solvers(self.box0)[0].species()[2]
 
     def close(self):
         for ss in self._cache.values():

@@ -602,9 +602,9 @@ static BlockFieldMap field_map(ps_adj* a) {
 
 
 // Branched chain (see the header): every slice stored by the engine's sweeps.
-static int tree_build(ps_adj* a, const ps_config* cfg, int polymer) {
+static int tree_build(ps_adj* a, int ec) {
   ps_handle* h = a->h;
-  const int ip = polymer;
+  const int ip = ec;  // the engine's (expanded) polymer index
   a->tree = true;
   a->C = 1;
   a->J = 0;
@@ -643,8 +643,7 @@ static int tree_build(ps_adj* a, const ps_config* cfg, int polymer) {
   };
   std::vector<std::vector<std::vector<Src>>> src(ns);
   for (int t = 0; t < ns; ++t) src[t].resize(h->sweeps[a->tsw[t]].total + 1);
-  const ps_polymer_config& P = cfg->polymers[ip];
-  const double densfac = 1.0 * P.volfrac / h->alpha[ip];
+  const double densfac = h->chain_dwt[ip] * h->chain_vf[ip] / h->alpha[ip];
   for (int b = 0; b < a->nb; ++b) {
     const BlockMap& bm = h->blocks[ip][b];
     const std::vector<double> c = quad_weights(bm.steps);
@@ -821,9 +820,10 @@ static int tree_build(ps_adj* a, const ps_config* cfg, int polymer) {
   return r2;
 }
 
-// polymer: the linear chain of cfg to differentiate (its phi contribution and
-// ln Q); single: the configuration must be a one-polymer melt (ps_adj_create).
-static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, int checkpoint) {
+// polymer: the caller's polymer of cfg to differentiate (its phi contribution
+// and ln Q), chain: its quadrature chain (0 unless polyDisperseBCP); single:
+// the configuration must be a one-polymer melt (ps_adj_create).
+static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, int chain, bool single, int checkpoint) {
   if (cfg->precision != PS_PREC_FP64) {
     a->err = "the adjoint runs in FP64 (precision must be PS_PREC_FP64)";
     return PS_ATTRIB_ERR;
@@ -836,11 +836,10 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, 
     a->err = "ps_adj_create takes one polymer and no solvent (ps_adj_create_polymer takes a blend)";
     return PS_INPUT_ERR;
   }
-  if (cfg->n_charges != 0 || cfg->polydisperse[polymer].enabled) {
-    a->err = "the adjoint takes uncharged, monodisperse chains";
+  if (cfg->n_charges != 0) {
+    a->err = "the adjoint takes uncharged chains";
     return PS_INPUT_ERR;
   }
-  a->ip = polymer;
   a->h = new ps_handle();
   a->h->no_slices = true;
   a->h->no_alias = true;  // mirror-symmetric chains: both sweeps run and are differentiated
@@ -850,9 +849,15 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, 
     return rc;
   }
   ps_handle* h = a->h;
-  std::vector<int> own;  // this polymer's sweeps
+  if (chain < 0 || chain >= h->user_ng[polymer]) {
+    a->err = "chain index out of range (a polyDisperseBCP polymer has n_g chains, any other one)";
+    return PS_ATTRIB_ERR;
+  }
+  const int ec = h->user_first[polymer] + chain;  // the engine's (expanded) polymer index
+  a->ip = ec;
+  std::vector<int> own;  // this chain's sweeps
   for (int k = 0; k < (int)h->sweeps.size(); ++k)
-    if (h->sweeps[k].polymer == polymer) own.push_back(k);
+    if (h->sweeps[k].polymer == ec) own.push_back(k);
   bool linear = (own.size() == 2);
   for (int k : own) linear = linear && h->sweeps[k].jin.empty();
   if (!linear) {
@@ -866,8 +871,8 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, 
       a->err = a->h->err;
       return rc;
     }
-    PA_CUDA(a, cudaMalloc((void**)&a->P, sizeof(double) * (size_t)a->h->N * a->h->blocks[polymer].size()));
-    return tree_build(a, cfg, polymer);
+    PA_CUDA(a, cudaMalloc((void**)&a->P, sizeof(double) * (size_t)a->h->N * a->h->blocks[ec].size()));
+    return tree_build(a, ec);
   }
   const Sweep& s0 = h->sweeps[own[0]];
   const Sweep& s1 = h->sweeps[own[1]];
@@ -888,8 +893,7 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, bool single, 
   }
   // quadrature pairs in sweep-0 indexing: (q_n, q+_{M-n})
   a->quad.assign(M + 1, {});
-  const ps_polymer_config& P = cfg->polymers[polymer];
-  const double densfac = 1.0 * P.volfrac / h->alpha[polymer];
+  const double densfac = h->chain_dwt[ec] * h->chain_vf[ec] / h->alpha[ec];
   for (int b = 0; b < a->nb; ++b) {
     const BlockMap& bm = h->blocks[a->ip][b];
     const std::vector<double> c = quad_weights(bm.steps);
@@ -1094,14 +1098,15 @@ using namespace psb;
 
 extern "C" {
 
-static int adj_create(const ps_config* cfg, int polymer, bool single, int checkpoint_interval, ps_adj** out) {
+static int adj_create(const ps_config* cfg, int polymer, int chain, bool single, int checkpoint_interval,
+                      ps_adj** out) {
   if (!cfg || !out) {
     g_adj_err = "null argument";
     return PS_ATTRIB_ERR;
   }
   *out = nullptr;
   ps_adj* a = new ps_adj();
-  int rc = adj_build(a, cfg, polymer, single, checkpoint_interval);
+  int rc = adj_build(a, cfg, polymer, chain, single, checkpoint_interval);
   if (rc) {
     g_adj_err = a->err;
     adj_free(a);
@@ -1114,11 +1119,22 @@ static int adj_create(const ps_config* cfg, int polymer, bool single, int checkp
 }
 
 int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out) {
-  return adj_create(cfg, 0, true, checkpoint_interval, out);
+  return adj_create(cfg, 0, 0, true, checkpoint_interval, out);
 }
 
-int ps_adj_create_polymer(const ps_config* cfg, int polymer, int checkpoint_interval, ps_adj** out) {
-  return adj_create(cfg, polymer, false, checkpoint_interval, out);
+int ps_adj_create_polymer(const ps_config* cfg, int polymer, int chain, int checkpoint_interval,
+                          ps_adj** out) {
+  return adj_create(cfg, polymer, chain, false, checkpoint_interval, out);
+}
+
+int ps_adj_species(const ps_adj* a, double* f_weight, double* length_ratio, double* dens_avg) {
+  if (!a || !a->h) return PS_ATTRIB_ERR;
+  const ps_handle* h = a->h;
+  if (f_weight) *f_weight = h->chain_dwt[a->ip] * h->chain_vf[a->ip];
+  if (length_ratio) *length_ratio = h->alpha[a->ip];
+  if (dens_avg)
+    for (int i = 0; i < h->nf; ++i) dens_avg[i] = h->fm.dens_avg[i];
+  return PS_OK;
 }
 
 int ps_adj_destroy(ps_adj* a) {

@@ -336,7 +336,8 @@ def test_blend_adjoint_gradients_match_finite_differences(gpu):
         assert abs(gbox[dim].item() - fd) <= TOL * abs(fd), (dim, gbox[dim].item(), fd)
     # stress of the free energy (fields fixed): F over every species
     from polyswift_plusplus_b200.adjoint import dens_avg, free_energy
-    avg = dens_avg(cfg)
+    avg = blend.dens_avg()
+    assert avg == pytest.approx(dens_avg(cfg), rel=1e-15, abs=1e-15)
     vf, al = blend.species_weights()
     chin = cfg.interactions[0].chi * cfg.polymers[0].length
     box = torch.tensor(blend.box0, dtype=torch.float64, requires_grad=True)
@@ -481,3 +482,66 @@ def test_adjoint_branched_chain(gpu, kind):
         print(f"{kind} dL/dds_{b}: adjoint {ds.grad[b].item():.12e} central difference {fd:.12e}")
         assert abs(ds.grad[b].item() - fd) <= TOL * abs(fd), (b, ds.grad[b].item(), fd)
     chain.close()
+
+
+def test_blend_adjoint_polydisperse(gpu):
+    """An A homopolymer (first, so the polydisperse polymer's quadrature chains sit at shifted
+    engine indices) blended with a polyDisperseBCP diblock of three Gauss-Laguerre chains: the
+    blend's phi against the engine, dL/dw against central differences, and F against the
+    engine's free-energy formula through the chains' weights."""
+    from polyswift_plusplus_b200.adjoint import DifferentiableBlend, free_energy
+    from polyswift_plusplus_b200.config import Block, Polymer
+    cfg, w = W.polydisperse_diblock(n=(16, 16, 16), n_g=3)
+    pd = dataclasses.replace(cfg.polymers[0], volfrac=0.85)
+    homo = Polymer(name="homoA", volfrac=0.15, length=50,
+                   blocks=[Block(name="hA", scfield="A", ds=0.02, lengthfrac=1.0)])
+    cfg = dataclasses.replace(cfg, polymers=[homo, pd])
+    w = np.stack(w)
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.update(1)
+    blend = DifferentiableBlend(cfg)
+    assert blend.chains() == [(0, 0), (1, 0), (1, 1), (1, 2)]
+    wt = torch.tensor(w, device=DEV, requires_grad=True)
+    phi, lnq = blend(wt)
+    for i in range(2):
+        ref = s.phi(i)
+        assert np.abs(phi[i].detach().cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert float(lnq[0]) == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    L = blend_loss(cfg, seed=21)
+    c = torch.tensor([0.3, -0.2, 0.1, 0.25], dtype=torch.float64, device=DEV)
+    rng = np.random.default_rng(5)
+    t = torch.tensor(rng.uniform(0.2, 0.8, cfg.n_total), device=DEV)
+
+    def Lp(p, q):
+        return ((p[0] - t) ** 2).sum() + 0.5 * p[1].sum() + (c * q).sum()
+    Lp(phi, lnq).backward()
+    gw = wt.grad.detach()
+    w0 = wt.detach()
+
+    def at(wv):
+        with torch.no_grad():
+            p, q = blend(wv)
+            return float(Lp(p, q))
+    for k in range(2):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        if k == 1:
+            d = torch.zeros((2, 16, 16, 16), dtype=torch.float64, device=DEV)
+            d[0, 2:6, 3:7, 4:8] = 1.0
+            d[1, 9:13, 10:14, 1:5] = -0.5
+            d = d.reshape(2, -1)
+        eps = 1e-5
+        fd = (at(w0 + eps * d) - at(w0 - eps * d)) / (2 * eps)
+        an = float((gw * d).sum())
+        print(f"polydisperse blend dL/dw direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    # the chains' free-energy weights reproduce the engine's -vf sum_k (w_k / Gamma) ln Q_k / alpha
+    # term: F of the blend's phi and ln Q at the engine's post-update fields equals the engine's F
+    vf, al = blend.species_weights()
+    wn = torch.tensor(np.stack([s.w(0), s.w(1)]), device=DEV)
+    with torch.no_grad():
+        F = float(free_energy(wn, phi.detach(), lnq.detach(), cfg.interactions[0].chi * cfg.polymers[0].length,
+                              blend.dens_avg(), vf, al))
+    print(f"polydisperse blend F: torch {F:.15f} engine {s.scalars()['free_energy']:.15f}")
+    assert F == pytest.approx(s.scalars()["free_energy"], rel=1e-12, abs=1e-12)
+    blend.close()
