@@ -403,7 +403,7 @@ void* ps_gpu_batch_stream(const ps_batch* b);
 const char* ps_gpu_batch_last_error(const ps_batch* b);
 
 /* --- Adjoint of the propagator sweeps (no reference counterpart) ----------
- * For one block copolymer chain (FP64, uncharged): linear chains with block 0
+ * For one block copolymer chain (FP64): linear chains with block 0
  * starting at a free end are checkpointed (mirror-symmetric chains such as
  * homopolymers and ABA triblocks run both sweeps); branched chains keep every
  * slice.  ps_adj_create takes a one-polymer melt; ps_adj_create_polymer takes
@@ -431,6 +431,13 @@ int ps_adj_create(const ps_config* cfg, int checkpoint_interval, ps_adj** out);
 int ps_adj_create_polymer(const ps_config* cfg, int polymer, int chain, int checkpoint_interval,
                           ps_adj** out);
 int ps_adj_species(const ps_adj* a, double* f_weight, double* length_ratio, double* dens_avg);
+/* Charged systems (chargeFlexPseudoSpec blocks): the potential psi (device,
+ * n_charges*N doubles) enters a charged block's Boltzmann factor next to w
+ * and is held fixed by the adjoint; ps_adj_set_potential sets it (zero at
+ * creation) and ps_adj_potential_grad returns dL/dpsi (device, n_charges*N)
+ * for the last ps_adj_backward. */
+int ps_adj_set_potential(ps_adj* a, const double* psi);
+int ps_adj_potential_grad(ps_adj* a, double* g_psi);
 int ps_adj_destroy(ps_adj* a);
 int ps_adj_forward(ps_adj* a, const double* w, double* phi, double* log_q);
 int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w, double* g_box,

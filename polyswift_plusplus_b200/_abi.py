@@ -167,6 +167,8 @@ SIGNATURES = {
     "ps_adj_create": (C.c_int, [C.POINTER(ps_config), C.c_int, C.POINTER(_vp)]),
     "ps_adj_create_polymer": (C.c_int, [C.POINTER(ps_config), C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
     "ps_adj_species": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ps_adj_set_potential": (C.c_int, [_vp, _vp]),
+    "ps_adj_potential_grad": (C.c_int, [_vp, _vp]),
     "ps_adj_destroy": (C.c_int, [_vp]),
     "ps_adj_forward": (C.c_int, [_vp, _vp, _vp, _dbl_p]),
     "ps_adj_backward": (C.c_int, [_vp, _vp, C.c_double, _vp, _dbl_p, _dbl_p]),

@@ -91,6 +91,20 @@ class ChainAdjoint:
         return (gw.view(self.nf, self.N), np.array([gbox[i] for i in range(3)]),
                 np.array([gds[i] for i in range(self.nb)]))
 
+    def set_potential(self, psi: torch.Tensor) -> None:
+        """Charged systems: the potential (n_charges, N) float64 CUDA tensor, held fixed."""
+        psi = psi.detach().to(torch.float64).contiguous()
+        torch.cuda.current_stream(psi.device).synchronize()
+        _chk(self._lib, self._lib.ps_adj_set_potential(self._h, C.c_void_p(psi.data_ptr())), self._h)
+        self._psi = psi  # kept alive until the copy on the handle's stream has run
+        self.forward_count += 1
+
+    def potential_grad(self, n_charges: int) -> torch.Tensor:
+        """dL/dpsi of the last backward, (n_charges, N)."""
+        g = torch.empty((n_charges, self.N), dtype=torch.float64, device="cuda")
+        _chk(self._lib, self._lib.ps_adj_potential_grad(self._h, C.c_void_p(g.data_ptr())), self._h)
+        return g
+
     def species(self) -> tuple[float, float, list]:
         """(free-energy weight, length ratio, average density of each field of the configuration)."""
         wt, lr = C.c_double(), C.c_double()

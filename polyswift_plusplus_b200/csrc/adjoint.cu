@@ -78,6 +78,8 @@ struct AdjPoint {
   SrcEntry src[2];
   const double* q_partner;  // Q source partner (nullptr: none at this slice)
   const double* extra;      // adj_init only: junction contributions to lambda (nullptr: none)
+  const double* psi;        // charged block: the exponent is w + facz psi (nullptr: w alone)
+  double facz;
 };
 
 // lam_out[j] += lam0 * prod_{i != j} q_in[i] for the sweeps arriving at a
@@ -219,6 +221,10 @@ __global__ void adj_init_kernel(const AdjPoint* __restrict__ pp, long long N, co
   }
 }
 
+__global__ void adj_axpy_kernel(double* __restrict__ dst, const double* __restrict__ x, double coef, long long N) {
+  ADJ_LOOP(r, N) dst[r] += coef * x[r];
+}
+
 __global__ void adj_junction_kernel(const JunctionAdj* __restrict__ jp, long long N) {
   const JunctionAdj j = *jp;
   ADJ_LOOP(r, N) {
@@ -242,7 +248,8 @@ __global__ void adj_point_kernel(const AdjPoint* __restrict__ pp, long long N, c
   ADJ_LOOP(r, N) {
     const double t = p.lam_next[r] * p.q_next[r] + p.q_s[r] * p.mu[r];
     p.gwb[r] += -p.half_ds * t;
-    acc += p.w[r] * (-0.5 * t);
+    const double x = p.psi ? p.w[r] + p.facz * p.psi[r] : p.w[r];
+    acc += x * (-0.5 * t);
     if (p.lam_out) {
       double s = 0.0;
       for (int i = 0; i < p.n_src; ++i) s += p.src[i].coef * p.src[i].gphi[r] * p.src[i].partner[r];
@@ -333,6 +340,7 @@ struct ps_adj {
   size_t storage_bytes = 0;
   size_t E_off = 0, gq_off = 0;  // offsets (in doubles) into part
   bool have_forward = false;
+  bool have_backward = false;
 };
 
 namespace psb {
@@ -358,8 +366,12 @@ struct Builder {
 
   const double* wf(int b) const {
     const BlockMap& bm = h->blocks[a->ip][b];
-    for (size_t i = 0; i < h->wfac_keys.size(); ++i)
-      if (h->wfac_keys[i].field == bm.field && h->wfac_keys[i].ds == bm.ds) return h->bd.wfac[i];
+    for (size_t i = 0; i < h->wfac_keys.size(); ++i) {
+      const WfacKey& k = h->wfac_keys[i];
+      if (k.field == bm.field && k.ds == bm.ds && k.charge_field == bm.charge_field &&
+          (bm.charge_field < 0 || k.facz == bm.facz))
+        return h->bd.wfac[i];
+    }
     return nullptr;
   }
   int ktab(int b) const {
@@ -551,6 +563,8 @@ static void adjoint_step_p(Builder& B, std::vector<Op>& ops, int b, const double
   p.dsw_part = a->part + poff + 3 * kAdjRB;
   p.half_ds = 0.5 * bm.ds;
   p.extra = nullptr;
+  p.psi = (bm.charge_field >= 0) ? h->d_psi + (size_t)bm.charge_field * a->N : nullptr;
+  p.facz = bm.facz;
   a->h_pt.push_back(p);
   const size_t pi = a->h_pt.size() - 1;
   const long long N = a->N;
@@ -834,10 +848,6 @@ static int adj_build(ps_adj* a, const ps_config* cfg, int polymer, int chain, bo
   }
   if (single && (cfg->n_polymers != 1 || cfg->n_solvents != 0)) {
     a->err = "ps_adj_create takes one polymer and no solvent (ps_adj_create_polymer takes a blend)";
-    return PS_INPUT_ERR;
-  }
-  if (cfg->n_charges != 0) {
-    a->err = "the adjoint takes uncharged chains";
     return PS_INPUT_ERR;
   }
   a->h = new ps_handle();
@@ -1127,6 +1137,46 @@ int ps_adj_create_polymer(const ps_config* cfg, int polymer, int chain, int chec
   return adj_create(cfg, polymer, chain, false, checkpoint_interval, out);
 }
 
+int ps_adj_set_potential(ps_adj* a, const double* psi) {
+  if (!a || !a->h || !psi) return PS_ATTRIB_ERR;
+  ps_handle* h = a->h;
+  if (h->nq == 0) {
+    a->err = "the configuration has no chargeDens field";
+    return PS_ATTRIB_ERR;
+  }
+  PA_CUDA(a, cudaSetDevice(h->dev));
+  PA_CUDA(a, cudaMemcpyAsync(h->d_psi, psi, sizeof(double) * (size_t)h->nq * a->N, cudaMemcpyDeviceToDevice,
+                             h->st));
+  a->have_forward = false;
+  return PS_OK;
+}
+
+int ps_adj_potential_grad(ps_adj* a, double* g_psi) {
+  if (!a || !a->h || !g_psi) return PS_ATTRIB_ERR;
+  ps_handle* h = a->h;
+  if (h->nq == 0) {
+    a->err = "the configuration has no chargeDens field";
+    return PS_ATTRIB_ERR;
+  }
+  if (!a->have_backward) {
+    a->err = "ps_adj_potential_grad needs a ps_adj_backward first";
+    return PS_ATTRIB_ERR;
+  }
+  const long long N = a->N;
+  PA_CUDA(a, cudaSetDevice(h->dev));
+  PA_CUDA(a, cudaMemsetAsync(g_psi, 0, sizeof(double) * (size_t)h->nq * N, h->st));
+  // psi enters a charged block's exponent as facz psi next to w: dL/dpsi = facz dL/dw of the block
+  for (int b = 0; b < a->nb; ++b) {
+    const BlockMap& bm = h->blocks[a->ip][b];
+    if (bm.charge_field < 0) continue;
+    adj_axpy_kernel<<<kAdjRB, kAdjRT, 0, h->st>>>(g_psi + (size_t)bm.charge_field * N, a->gwb + (size_t)b * N,
+                                                  bm.facz, N);
+    PA_CUDA(a, cudaGetLastError());
+  }
+  PA_CUDA(a, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
 int ps_adj_species(const ps_adj* a, double* f_weight, double* length_ratio, double* dens_avg) {
   if (!a || !a->h) return PS_ATTRIB_ERR;
   const ps_handle* h = a->h;
@@ -1177,6 +1227,7 @@ int ps_adj_forward(ps_adj* a, const double* w, double* phi, double* log_q) {
   }
   if (log_q) *log_q = h->h_sc->log_q[0];
   a->have_forward = true;
+  a->have_backward = false;
   return PS_OK;
 }
 
@@ -1225,6 +1276,7 @@ int ps_adj_backward(ps_adj* a, const double* g_phi, double g_log_q, double* g_w,
     for (int d = 0; d < 3; ++d) g_box[d] = gbox[d];
   if (g_ds)
     for (int b = 0; b < a->nb; ++b) g_ds[b] = gds[b];
+  a->have_backward = true;
   return PS_OK;
 }
 

@@ -507,7 +507,7 @@ def test_blend_adjoint_polydisperse(gpu):
     for i in range(2):
         ref = s.phi(i)
         assert np.abs(phi[i].detach().cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
-    assert float(lnq[0]) == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    assert float(lnq[0].detach()) == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
     L = blend_loss(cfg, seed=21)
     c = torch.tensor([0.3, -0.2, 0.1, 0.25], dtype=torch.float64, device=DEV)
     rng = np.random.default_rng(5)
@@ -545,3 +545,51 @@ def test_blend_adjoint_polydisperse(gpu):
     print(f"polydisperse blend F: torch {F:.15f} engine {s.scalars()['free_energy']:.15f}")
     assert F == pytest.approx(s.scalars()["free_energy"], rel=1e-12, abs=1e-12)
     blend.close()
+
+
+def test_adjoint_charged_chain_at_fixed_potential(gpu):
+    """A charged diblock (chargeFlexPseudoSpec block A, counter-ions): with the potential psi set,
+    the adjoint's phi against the engine's first iteration, and dL/dw and dL/dpsi against
+    central differences (psi enters the charged block's Boltzmann factor next to w)."""
+    from polyswift_plusplus_b200 import _abi as A
+    cfg, w, psi = W.charged_diblock(n=(16, 16, 16), poisson_every=5)
+    w = np.stack(w)
+    s = ScftSolver(cfg)
+    s.restore(list(w))
+    s.set_field(A.PS_FIELD_POTENTIAL, 0, psi)
+    s.update(1)
+    adj = ChainAdjoint(cfg, polymer=0)
+    nq = 2
+    pt = torch.zeros((nq, cfg.n_total), dtype=torch.float64, device=DEV)
+    pt[0] = torch.tensor(psi, device=DEV)
+    adj.set_potential(pt)
+    wt = torch.tensor(w, device=DEV)
+    phi, lnq = adj.forward(wt)
+    for i in range(2):
+        ref = s.phi(i)
+        assert np.abs(phi[i].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert lnq == pytest.approx(s.scalars()["log_q"][0], rel=1e-13, abs=1e-13)
+    L = loss_terms(cfg, seed=23)
+    gw, _, _ = grads(adj, wt, L)
+    gpsi = adj.potential_grad(nq)
+    assert float(gpsi[1].abs().max()) == 0.0  # no block is charged through the counter-ion field
+    rng = np.random.default_rng(29)
+    eps = 1e-5
+    for k in range(2):
+        d = torch.tensor(rng.standard_normal(w.shape), device=DEV)
+        fd = (eval_loss(adj, wt + eps * d, L) - eval_loss(adj, wt - eps * d, L)) / (2 * eps)
+        an = float((gw * d).sum())
+        print(f"charged dL/dw direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    for k in range(2):
+        d = torch.zeros_like(pt)
+        d[0] = torch.tensor(rng.standard_normal(cfg.n_total), device=DEV)
+
+        def at(p):
+            adj.set_potential(p)
+            return eval_loss(adj, wt, L)
+        fd = (at(pt + eps * d) - at(pt - eps * d)) / (2 * eps)
+        an = float((gpsi * d).sum())
+        print(f"charged dL/dpsi direction {k}: adjoint {an:.12e} central difference {fd:.12e}")
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+    adj.close()
