@@ -247,6 +247,16 @@ int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_d
  * read of the same field waits (on the device) for the first one's host copy
  * before its snapshot is taken. */
 int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host);
+/* Copy a field in from host memory without waiting (no reference counterpart).
+ * A field w_i goes up on the handle's stream, ahead of the next iteration.
+ * The pressure field goes up on its own stream after the work enqueued so
+ * far, and only the next iteration's field update (its first reader) waits
+ * for it, so the copy overlaps that iteration's sweeps.  `host` should be
+ * pinned memory, and must stay unchanged until ps_gpu_fields_wait,
+ * ps_gpu_synchronize or ps_gpu_get_scalars returns.  Batch instances copy
+ * synchronously. */
+int ps_gpu_set_fields_async(ps_handle* h, int which, int index, const double* host);
+/* Wait for every asynchronous read-back and upload of the handle. */
 int ps_gpu_fields_wait(ps_handle* h);
 
 /* Reference initialisation: every monomerDens w_i = U[0,1) - 0.5 drawn from

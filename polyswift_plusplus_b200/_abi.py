@@ -180,6 +180,7 @@ SIGNATURES = {
     "ps_fft_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "ps_gpu_set_bulk_wait_limit": (C.c_int, [C.c_uint]),
     "ps_gpu_get_fields_async": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "ps_gpu_set_fields_async": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "ps_gpu_fields_wait": (C.c_int, [_vp]),
     "ps_fft_get_grid": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "ps_fft_scaled_pair": (C.c_int, [_vp, _vp, _vp, _vp]),

@@ -543,6 +543,14 @@ static int launch_post(ps_handle* h, long long* nlaunch) {
       }
     }
   }
+  // the field update is the first reader of p: wait for an asynchronous upload
+  // of it (an external event-wait node when this is being captured)
+  if (h->p_ready) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PS_CUDA(h, cudaStreamIsCapturing(h->st, &cs));
+    PS_CUDA(h, cudaStreamWaitEvent(h->st, h->p_ready,
+                                   cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0));
+  }
   FieldPtrs fp;
   memset(&fp, 0, sizeof(fp));
   for (int i = 0; i < h->nf; ++i) {
@@ -704,6 +712,10 @@ static void free_all(ps_handle* h) {
   }
   h->read_slots.clear();
   if (h->io_st) cudaStreamDestroy(h->io_st);
+  if (h->up_st) cudaStreamSynchronize(h->up_st);
+  if (h->up_st) cudaStreamDestroy(h->up_st);
+  if (h->up_ev) cudaEventDestroy(h->up_ev);
+  if (h->p_ready) cudaEventDestroy(h->p_ready);
   if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -1050,6 +1062,8 @@ static int create_impl(ps_handle* h, const ps_config* ucfg) {
   PS_CUDA(h, cudaMemset(h->d_w, 0, sizeof(double) * nfN));
   PS_CUDA(h, cudaMemset(h->d_phi, 0, sizeof(double) * nfN));
   PS_CUDA(h, cudaMemset(h->d_p, 0, sizeof(double) * (size_t)h->N));
+  PS_CUDA(h, cudaEventCreateWithFlags(&h->p_ready, cudaEventDisableTiming));
+  PS_CUDA(h, cudaEventRecord(h->p_ready, h->st));
   if (h->nq > 0) {
     const size_t qN = (size_t)h->nq * h->N;
     PS_CUDA(h, cudaMalloc((void**)&h->d_rho, sizeof(double) * qN));
@@ -1279,6 +1293,12 @@ static double* field_ptr(ps_handle* h, int which, int index) {
   return nullptr;
 }
 
+// Work on st that touches p goes after an asynchronous upload of it.
+static int order_uploads(ps_handle* h) {
+  if (h->up_st) PS_CUDA(h, cudaStreamWaitEvent(h->st, h->p_ready, 0));
+  return PS_OK;
+}
+
 int ps_gpu_set_fields(ps_handle* h, int which, int index, const double* data, int on_device) {
   if (!h || !data) return PS_ATTRIB_ERR;
   double* dst = field_ptr(h, which, index);
@@ -1287,9 +1307,38 @@ int ps_gpu_set_fields(ps_handle* h, int which, int index, const double* data, in
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));
+  int rc = order_uploads(h);
+  if (rc) return rc;
   PS_CUDA(h, cudaMemcpyAsync(dst, data, sizeof(double) * (size_t)h->N,
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->st));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
+  return PS_OK;
+}
+
+int ps_gpu_set_fields_async(ps_handle* h, int which, int index, const double* host) {
+  if (!h || !host) return PS_ATTRIB_ERR;
+  double* dst = field_ptr(h, which, index);
+  if (!dst) {
+    h->err = "bad field selector";
+    return PS_ATTRIB_ERR;
+  }
+  if (h->in_batch) return ps_gpu_set_fields(h, which, index, host, 0);  // the batch owns the launches
+  PS_CUDA(h, cudaSetDevice(h->dev));
+  const size_t bytes = sizeof(double) * (size_t)h->N;
+  if (which != PS_FIELD_PRES) {
+    PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, h->st));
+    return PS_OK;
+  }
+  if (!h->up_st) {
+    PS_CUDA(h, cudaStreamCreateWithFlags(&h->up_st, cudaStreamNonBlocking));
+    PS_CUDA(h, cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming));
+  }
+  // after the work enqueued so far (the last update, read-back snapshots of p),
+  // before the next update, overlapping the next iteration's sweeps
+  PS_CUDA(h, cudaEventRecord(h->up_ev, h->st));
+  PS_CUDA(h, cudaStreamWaitEvent(h->up_st, h->up_ev, 0));
+  PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, h->up_st));
+  PS_CUDA(h, cudaEventRecord(h->p_ready, h->up_st));
   return PS_OK;
 }
 
@@ -1301,6 +1350,8 @@ int ps_gpu_get_fields(ps_handle* h, int which, int index, double* data, int on_d
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));
+  int rc = order_uploads(h);
+  if (rc) return rc;
   PS_CUDA(h, cudaMemcpyAsync(data, src, sizeof(double) * (size_t)h->N,
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->st));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
@@ -1315,6 +1366,8 @@ int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host) {
     return PS_ATTRIB_ERR;
   }
   PS_CUDA(h, cudaSetDevice(h->dev));
+  int rc = order_uploads(h);
+  if (rc) return rc;
   if (!h->io_st) PS_CUDA(h, cudaStreamCreateWithFlags(&h->io_st, cudaStreamNonBlocking));
   ps_handle::ReadSlot& rs = h->read_slots[std::make_pair(which, index)];
   const size_t bytes = sizeof(double) * (size_t)h->N;
@@ -1336,15 +1389,17 @@ int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host) {
 
 int ps_gpu_fields_wait(ps_handle* h) {
   if (!h) return PS_ATTRIB_ERR;
-  if (!h->io_st) return PS_OK;
+  if (!h->io_st && !h->up_st) return PS_OK;
   PS_CUDA(h, cudaSetDevice(h->dev));
-  PS_CUDA(h, cudaStreamSynchronize(h->io_st));
+  if (h->io_st) PS_CUDA(h, cudaStreamSynchronize(h->io_st));
+  if (h->up_st) PS_CUDA(h, cudaStreamSynchronize(h->up_st));
   return PS_OK;
 }
 
 int ps_gpu_init_random(ps_handle* h) {
   if (!h) return PS_ATTRIB_ERR;
   PS_CUDA(h, cudaSetDevice(h->dev));
+  if (h->up_st) PS_CUDA(h, cudaStreamSynchronize(h->up_st));
   int rc = settle_rng(h);
   if (rc) return rc;
   std::vector<double> buf((size_t)h->N);
@@ -1429,6 +1484,7 @@ int ps_gpu_synchronize(ps_handle* h) {
   if (!h) return PS_ATTRIB_ERR;
   PS_CUDA(h, cudaSetDevice(h->dev));
   PS_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->up_st) PS_CUDA(h, cudaStreamSynchronize(h->up_st));
   return PS_OK;
 }
 

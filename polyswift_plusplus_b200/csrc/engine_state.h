@@ -186,6 +186,13 @@ struct ps_handle {
   };
   std::map<std::pair<int, int>, ReadSlot> read_slots;
   cudaStream_t io_st = nullptr;
+  // Asynchronous upload (ps_gpu_set_fields_async): the pressure field goes up
+  // on up_st after the work enqueued on st so far (up_ev), and every field
+  // update waits for p_ready (recorded at creation, then after each upload; an
+  // event-wait node of the captured graph).
+  cudaStream_t up_st = nullptr;
+  cudaEvent_t up_ev = nullptr;
+  cudaEvent_t p_ready = nullptr;
   double sweep_bytes = 0.0;  // algorithmic bytes of the sweeps of one iteration
   long long sweep_steps = 0; // propagator steps (all sweeps) of one iteration
 };

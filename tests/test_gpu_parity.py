@@ -1182,3 +1182,53 @@ def test_async_field_readback_matches_blocking_read(gpu):
     with pytest.raises(A.PsError):
         g.get_field_async(A.PS_FIELD_W, 7, bufs[3])
     g.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_async_field_upload_matches_blocking_upload(gpu, prec):
+    """ps_gpu_set_fields_async: iterations fed by asynchronous uploads (w on the handle
+    stream, p on the upload stream with the field update waiting for it inside the captured
+    graph) are bit-identical to iterations fed by blocking uploads, step by step, with new
+    host values every step; a blocking read of p right after its asynchronous upload sees
+    the uploaded values."""
+    import torch
+    cfg, w = W.diblock32(n=32, precision=prec)
+    N = cfg.n_total
+    rng = np.random.default_rng(41)
+    steps = [([w[0] + 0.01 * rng.standard_normal(N), w[1] + 0.01 * rng.standard_normal(N)],
+              0.05 * rng.standard_normal(N)) for _ in range(4)]
+    runs = []
+    for mode in ("blocking", "async"):
+        g = ScftSolver(cfg)
+        g.restore(w)
+        g.update(3)  # eager iterations, then the captured graph
+        host_w = [torch.empty(N, dtype=torch.float64).pin_memory() for _ in range(2)]
+        host_p = torch.empty(N, dtype=torch.float64).pin_memory()
+        hist = []
+        for ws, p in steps:
+            for i in range(2):
+                host_w[i].copy_(torch.from_numpy(ws[i]))
+            host_p.copy_(torch.from_numpy(p))
+            if mode == "blocking":
+                for i in range(2):
+                    g.set_field(A.PS_FIELD_W, i, host_w[i])
+                g.set_field(A.PS_FIELD_PRES, 0, host_p)
+            else:
+                for i in range(2):
+                    g.set_field_async(A.PS_FIELD_W, i, host_w[i])
+                g.set_field_async(A.PS_FIELD_PRES, 0, host_p)
+            g.update(1)
+            hist.append(g.scalars())  # the host buffers are free again after this
+        runs.append((hist, [g.w(i) for i in range(2)], g.pressure()))
+        if mode == "async":
+            q = np.arange(N, dtype=np.float64)
+            g.set_field_async(A.PS_FIELD_PRES, 0, q)
+            assert np.array_equal(g.pressure(), q)
+            g.fields_wait()
+        g.close()
+    (ha, wa, pa), (hb, wb, pb) = runs
+    for a, b in zip(ha, hb):
+        assert a["free_energy"] == b["free_energy"] and a["q"][0] == b["q"][0]
+    for i in range(2):
+        assert np.array_equal(wa[i], wb[i])
+    assert np.array_equal(pa, pb)
