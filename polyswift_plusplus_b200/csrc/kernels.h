@@ -82,8 +82,8 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // own stream (parallel graph branches) instead of all sweeps in lockstep in
 // shared launches; single-instance engine only (kernels ignore the bit).
 // bit 4: 256 x 256 y-z planes (too large for one CTA) run as one plane pass on
-// a cluster of CTAs (two for FP32, four for FP64) instead of a row pass and two
-// y pencil passes (cluster_plane_supported); elsewhere the bit changes nothing.
+// a cluster of four CTAs instead of a row pass and two y pencil passes
+// (cluster_plane_supported); elsewhere the bit changes nothing.
 enum {
   VARIANT_FUSE_Z = 1,
   VARIANT_FUSE_K = 2,
@@ -93,8 +93,8 @@ enum {
   VARIANT_COUNT = 32
 };
 bool cluster_plane_supported(int prec_bytes, int ny, int nz);
-// The cluster plane pass (ny = nz = 256): grid CL nx x nworks, CL = 2 (FP32)
-// or 4 (FP64) CTAs per plane.
+// The cluster plane pass (ny = nz = 256): grid 4 nx x nworks, four CTAs per
+// plane.
 template <typename T>
 cudaError_t launch_plane_cluster(const PlaneWork<T>* d_works, int nworks, int nx, const c2_t<T>* tw_y,
                                  const c2_t<T>* tw_zh, const c2_t<T>* tw_z, cudaStream_t st);

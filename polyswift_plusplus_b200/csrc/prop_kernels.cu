@@ -1005,10 +1005,10 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz) {
 
 // ---------------------------------------------------------------------------
 // Plane pass of 256 x 256 y-z planes on a cluster of CL CTAs
-// (VARIANT_CLUSTER): two for FP32, four for FP64.  A 256 x 129 half plane
-// (264 KB in FP32, 528 KB in FP64) does not fit one CTA's shared memory; split
-// over the cluster it does, and the step needs no y pencil passes (two fewer
-// spectrum round trips).  With CH = 128 / CL and RH = 256 / CL, CTA c holds:
+// (VARIANT_CLUSTER): four CTAs (PlaneCl).  A 256 x 129 half plane (264 KB in
+// FP32, 528 KB in FP64) does not fit one CTA's shared memory; split over the
+// cluster it does, and the step needs no y pencil passes (two fewer spectrum
+// round trips).  With CH = 128 / CL and RH = 256 / CL, CTA c holds:
 //   y phases: kz columns [CH c, CH c + CH) for all y (CTA 0 also kz = 128,
 //             which shares the kz = 0 transform), layout Y[y][slot], CH + 1
 //             slots a row;
@@ -1048,11 +1048,15 @@ __device__ __forceinline__ void st_cluster(C* buf, int i, uint32_t rank, uint32_
 }
 
 template <typename T> struct PlaneCl;
+// Four CTAs per plane in both precisions.  FP32: 512 threads, 64 registers and
+// 73 KB of shared memory, so two CTAs of different planes share an SM and hide
+// each other's load latency (171 us per 256^3 step against 184 with two
+// 1024-thread CTAs, one per SM).  FP64: 512 threads, 127 registers, 145 KB.
 template <> struct PlaneCl<float> {
-  static constexpr int CL = 2, TH = 1024, UCMAX = 8;
+  static constexpr int CL = 4, TH = 512, UCMAX = 8, MINB = 2;
 };
 template <> struct PlaneCl<double> {
-  static constexpr int CL = 4, TH = 512, UCMAX = 4;
+  static constexpr int CL = 4, TH = 512, UCMAX = 4, MINB = 1;
 };
 template <typename T> struct PlaneC256 {
   static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128;
@@ -1072,7 +1076,7 @@ template <typename T> struct PlaneC256 {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(PlaneC256<T>::TH, 1)
+__global__ void __launch_bounds__(PlaneC256<T>::TH, PlaneCl<T>::MINB)
     plane_c256_kernel(const PlaneWork<T>* __restrict__ works, const c2_t<T>* __restrict__ tw_y,
                       const c2_t<T>* __restrict__ tw_zh, const c2_t<T>* __restrict__ tw_z) {
   using P = PlaneC256<T>;
