@@ -296,7 +296,7 @@ void* ps_gpu_stream(const ps_handle* h);
 /* Kernel variant of the propagator sweeps (no reference counterpart).  Every
  * variant computes the same result; they differ in how passes are fused
  * (bits 0, 1), in the FFT decomposition (bit 2: row + x-y planes; bit 4:
- * 256 x 256 y-z planes on a cluster of four CTAs instead of a row pass and
+ * 256 x 256 y-z planes on a cluster of eight CTAs instead of a row pass and
  * y pencils, PS_ATTRIB_ERR for other plane sizes) and in whether an
  * instance's sweeps share launches or run as concurrent launch chains
  * (bit 3).  variant = -1 (the default) times all variants on the handle's

@@ -82,7 +82,7 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz);
 // own stream (parallel graph branches) instead of all sweeps in lockstep in
 // shared launches; single-instance engine only (kernels ignore the bit).
 // bit 4: 256 x 256 y-z planes (too large for one CTA) run as one plane pass on
-// a cluster of four CTAs instead of a row pass and two y pencil passes
+// a cluster of eight CTAs instead of a row pass and two y pencil passes
 // (cluster_plane_supported); elsewhere the bit changes nothing.
 enum {
   VARIANT_FUSE_Z = 1,
@@ -93,7 +93,7 @@ enum {
   VARIANT_COUNT = 32
 };
 bool cluster_plane_supported(int prec_bytes, int ny, int nz);
-// The cluster plane pass (ny = nz = 256): grid 4 nx x nworks, four CTAs per
+// The cluster plane pass (ny = nz = 256): grid 8 nx x nworks, eight CTAs per
 // plane.
 template <typename T>
 cudaError_t launch_plane_cluster(const PlaneWork<T>* d_works, int nworks, int nx, const c2_t<T>* tw_y,

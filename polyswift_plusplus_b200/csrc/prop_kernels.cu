@@ -1005,7 +1005,7 @@ bool plane_fused_supported(int prec_bytes, int ny, int nz) {
 
 // ---------------------------------------------------------------------------
 // Plane pass of 256 x 256 y-z planes on a cluster of CL CTAs
-// (VARIANT_CLUSTER): four CTAs (PlaneCl).  A 256 x 129 half plane (264 KB in
+// (VARIANT_CLUSTER): eight CTAs (PlaneCl).  A 256 x 129 half plane (264 KB in
 // FP32, 528 KB in FP64) does not fit one CTA's shared memory; split over the
 // cluster it does, and the step needs no y pencil passes (two fewer spectrum
 // round trips).  With CH = 128 / CL and RH = 256 / CL, CTA c holds:
@@ -1048,15 +1048,17 @@ __device__ __forceinline__ void st_cluster(C* buf, int i, uint32_t rank, uint32_
 }
 
 template <typename T> struct PlaneCl;
-// Four CTAs per plane in both precisions.  FP32: 512 threads, 64 registers and
-// 73 KB of shared memory, so two CTAs of different planes share an SM and hide
-// each other's load latency (171 us per 256^3 step against 184 with two
-// 1024-thread CTAs, one per SM).  FP64: 512 threads, 127 registers, 145 KB.
+// Eight 256-thread CTAs per plane in both precisions, so that several CTAs of
+// different planes share an SM and hide each other's load latency.  FP32: 64
+// registers, 40 KB of shared memory, four CTAs per SM (166 us per 256^3 step,
+// against 171 with four 512-thread CTAs and 184 with two 1024-thread CTAs).
+// FP64: 126 registers, 80 KB, two CTAs per SM (364 us against 388 with four
+// 512-thread CTAs, one per SM).
 template <> struct PlaneCl<float> {
-  static constexpr int CL = 4, TH = 512, UCMAX = 8, MINB = 2;
+  static constexpr int CL = 8, TH = 256, UCMAX = 8, MINB = 4;
 };
 template <> struct PlaneCl<double> {
-  static constexpr int CL = 4, TH = 512, UCMAX = 4, MINB = 1;
+  static constexpr int CL = 8, TH = 256, UCMAX = 4, MINB = 2;
 };
 template <typename T> struct PlaneC256 {
   static constexpr int NY = 256, NZ = 256, NZH = 129, H = 128;
@@ -1070,9 +1072,9 @@ template <typename T> struct PlaneC256 {
   static constexpr int UY = NY * CH / TH;            // Y elements per thread (+1 slot-CH element)
   static constexpr int UZ = (ZE + TH - 1) / TH;      // Z elements per thread
   static constexpr size_t SMEM = sizeof(c2_t<T>) * ((size_t)BUF + H + NZ + NY);
-  // the Y -> Z exchange keeps y = e / CH warp-uniform and the slot-CH column
-  // takes one thread per y
-  static_assert(CH % 32 == 0 && (NY * CH) % TH == 0 && NY <= TH, "cluster plane layout");
+  // y = e / CH is uniform over each half-warp in the Y -> Z exchange, and the
+  // slot-CH column takes one thread per y
+  static_assert(CH % 16 == 0 && (NY * CH) % TH == 0 && NY <= TH, "cluster plane layout");
 };
 
 template <typename T>
@@ -1154,7 +1156,7 @@ __global__ void __launch_bounds__(PlaneC256<T>::TH, PlaneCl<T>::MINB)
 #pragma unroll
     for (int u = 0; u < P::UY; ++u) {
       const int e = tid + u * TH;
-      const int y = e / CH, kz = col0 + (e % CH);  // y uniform over a warp (CH % 32 == 0)
+      const int y = e / CH, kz = col0 + (e % CH);  // y uniform over a half-warp (CH % 16 == 0)
       const int o = y / RH;
       st_cluster(buf, (y - o * RH) * NZH + kz, (uint32_t)o, me, v[u]);
     }

@@ -46,7 +46,7 @@ template <typename T> struct SweepSet {
   const int* junc_cnt = nullptr;
 };
 
-// The cluster plane pass exists for 256 x 256 planes (four CTAs per plane).
+// The cluster plane pass exists for 256 x 256 planes (eight CTAs per plane).
 template <typename T>
 inline bool cluster_path(const SweepSet<T>& s, int variant) {
   return (variant & VARIANT_CLUSTER) && !s.fused_plane &&

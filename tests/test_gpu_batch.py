@@ -213,7 +213,7 @@ def test_batch_with_filtered_instances_bit_identical(gpu):
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_batch_class_with_cluster_plane_pass(gpu, precision):
     """A size class of 8 x 256 x 256 instances with the cluster plane pass forced
-    (variant 16: one merged plane launch covers every member's sweeps; four CTAs
+    (variant 16: one merged plane launch covers every member's sweeps; eight CTAs
     per plane): each instance bit-identical to its single run with the same
     variant."""
     items = []

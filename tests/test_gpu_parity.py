@@ -203,7 +203,7 @@ def _slab256(precision):
 @pytest.mark.parametrize("base", [0, 8])
 def test_cluster_plane_pass_256(gpu, oracle_lib, base):
     """Variant bit 4: FP32 256 x 256 y-z planes as one plane pass on a cluster of
-    four CTAs (column quarters for the y FFTs, row quarters for the z passes,
+    eight CTAs (column eighths for the y FFTs, row eighths for the z passes,
     exchanged through distributed shared memory), instead of a row pass and
     two y pencil passes.  Against the same variant without the bit (the FFT
     decomposition differs, so FP32 rounding does) and against the FP64 oracle
@@ -242,8 +242,8 @@ def test_cluster_plane_pass_256(gpu, oracle_lib, base):
 @pytest.mark.parametrize("base", [0, 8])
 def test_cluster_plane_pass_256_fp64(gpu, oracle_lib, base):
     """Variant bit 4 in FP64: 256 x 256 y-z planes (528 KB as a half plane) as one
-    plane pass on a cluster of four CTAs (column quarters for the y FFTs, row
-    quarters for the z passes), against the FP64 oracle at the FP64 tolerance
+    plane pass on a cluster of eight CTAs (column eighths for the y FFTs, row
+    eighths for the z passes), against the FP64 oracle at the FP64 tolerance
     over three iterations, and against the row + y-pencil design."""
     cfg, w = _slab256("fp64")
     iters = 3
@@ -281,7 +281,7 @@ def test_cluster_variant_only_where_it_exists(gpu):
             g.set_variant(16)
         assert e.value.code == A.PS_ATTRIB_ERR
         g.close()
-    for prec in ("mixed", "fp64"):  # four CTAs per plane in both precisions
+    for prec in ("mixed", "fp64"):  # eight CTAs per plane in both precisions
         cfg, _ = _slab256(prec)
         g = ScftSolver(cfg)
         g.set_variant(16)
