@@ -252,9 +252,9 @@ int ps_gpu_get_fields_async(ps_handle* h, int which, int index, double* host);
  * The pressure field goes up on its own stream after the work enqueued so
  * far, and only the next iteration's field update (its first reader) waits
  * for it, so the copy overlaps that iteration's sweeps.  `host` should be
- * pinned memory, and must stay unchanged until ps_gpu_fields_wait,
- * ps_gpu_synchronize or ps_gpu_get_scalars returns.  Batch instances copy
- * synchronously. */
+ * pinned memory (a device pointer on the handle's device also works), and
+ * must stay unchanged until ps_gpu_fields_wait, ps_gpu_synchronize or
+ * ps_gpu_get_scalars returns.  Batch instances copy synchronously. */
 int ps_gpu_set_fields_async(ps_handle* h, int which, int index, const double* host);
 /* Wait for every asynchronous read-back and upload of the handle. */
 int ps_gpu_fields_wait(ps_handle* h);

@@ -1322,11 +1322,16 @@ int ps_gpu_set_fields_async(ps_handle* h, int which, int index, const double* ho
     h->err = "bad field selector";
     return PS_ATTRIB_ERR;
   }
-  if (h->in_batch) return ps_gpu_set_fields(h, which, index, host, 0);  // the batch owns the launches
+  if (h->in_batch) {  // the batch owns the launches: a blocking copy
+    cudaPointerAttributes pa;
+    const bool dev = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    return ps_gpu_set_fields(h, which, index, host, dev ? 1 : 0);
+  }
   PS_CUDA(h, cudaSetDevice(h->dev));
   const size_t bytes = sizeof(double) * (size_t)h->N;
   if (which != PS_FIELD_PRES) {
-    PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, h->st));
+    PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyDefault, h->st));
     return PS_OK;
   }
   if (!h->up_st) {
@@ -1337,7 +1342,7 @@ int ps_gpu_set_fields_async(ps_handle* h, int which, int index, const double* ho
   // before the next update, overlapping the next iteration's sweeps
   PS_CUDA(h, cudaEventRecord(h->up_ev, h->st));
   PS_CUDA(h, cudaStreamWaitEvent(h->up_st, h->up_ev, 0));
-  PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, h->up_st));
+  PS_CUDA(h, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyDefault, h->up_st));
   PS_CUDA(h, cudaEventRecord(h->p_ready, h->up_st));
   return PS_OK;
 }

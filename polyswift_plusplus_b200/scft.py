@@ -126,14 +126,13 @@ class ScftSolver:
         self._check(self._lib.ps_gpu_get_fields_async(self._h, which, index, ptr))
 
     def set_field_async(self, which: int, index: int, data) -> None:
-        """Start copying a field in from `data` (a pinned host float64 tensor or a numpy array
-        of N values) without waiting; `data` must stay unchanged until fields_wait(),
-        synchronize() or scalars() returns.  The pressure field's copy overlaps the next
-        iteration's sweeps."""
+        """Start copying a field in from `data` (a pinned host or device float64 tensor, or a
+        numpy array of N values) without waiting; `data` must stay unchanged until
+        fields_wait(), synchronize() or scalars() returns.  The pressure field's copy overlaps
+        the next iteration's sweeps."""
         if hasattr(data, "data_ptr"):
-            if data.is_cuda or data.dtype != __import__("torch").float64 or data.numel() != self.N \
-                    or not data.is_contiguous():
-                raise ValueError("data must be a contiguous host float64 tensor of N values")
+            if data.dtype != __import__("torch").float64 or data.numel() != self.N or not data.is_contiguous():
+                raise ValueError("data must be a contiguous float64 tensor of N values")
             ptr = C.c_void_p(data.data_ptr())
         else:
             if data.dtype != np.float64 or data.size != self.N or not data.flags.c_contiguous:

@@ -1224,7 +1224,11 @@ def test_async_field_upload_matches_blocking_upload(gpu, prec):
             q = np.arange(N, dtype=np.float64)
             g.set_field_async(A.PS_FIELD_PRES, 0, q)
             assert np.array_equal(g.pressure(), q)
+            qd = torch.full((N,), 0.25, dtype=torch.float64, device="cuda")  # a device source
+            g.set_field_async(A.PS_FIELD_W, 1, qd)
+            g.set_field_async(A.PS_FIELD_PRES, 0, qd)
             g.fields_wait()
+            assert np.array_equal(g.w(1), qd.cpu().numpy()) and np.array_equal(g.pressure(), qd.cpu().numpy())
         g.close()
     (ha, wa, pa), (hb, wb, pb) = runs
     for a, b in zip(ha, hb):
