@@ -273,6 +273,34 @@ def test_cluster_plane_pass_256_fp64(gpu, oracle_lib, base):
     assert rel(b[1], a[1]) < 1e-11
 
 
+@pytest.mark.parametrize("prec,tol", [("mixed", 1e-5), ("fp64", 1e-11)])
+def test_cluster_plane_pass_full_256_cubed(gpu, prec, tol):
+    """The cluster plane pass at full size: the 256^3 ABC triblock (its box and chiN, Ns = 20)
+    over two iterations with the cluster pass (variant 26) and with the row + y-pencil design
+    (variant 10); the two decompositions agree to FP64 roundoff, and to FP32 rounding for FP32
+    sweeps."""
+    import dataclasses
+    cfg, w = W.triblock256(precision=prec)
+    p = cfg.polymers[0]
+    cfg = dataclasses.replace(cfg, polymers=[dataclasses.replace(
+        p, blocks=[dataclasses.replace(b, ds=0.05) for b in p.blocks])])
+    runs = {}
+    for v in (10, 26):
+        g = ScftSolver(cfg)
+        g.set_variant(v)
+        g.restore(w)
+        g.update(2)
+        assert g.variant()[0] == v
+        runs[v] = ([g.phi(i) for i in range(3)], g.scalars()["free_energy"], g.block_steps(0, 1))
+        g.close()
+    (pr, fr, nb), (pc, fc, _) = runs[10], runs[26]
+    assert nb == 8
+    d = max(rel(pc[i], pr[i]) for i in range(3))
+    print(f"256^3 {prec}: cluster vs rows: phi {d:.2e}, F {fc:.12e} / {fr:.12e}")
+    assert d < tol
+    assert abs(fc - fr) <= tol * max(abs(fr), 1e-3)
+
+
 def test_cluster_variant_only_where_it_exists(gpu):
     for prec, n in (("mixed", 16), ("fp64", 16)):
         cfg, _ = W.diblock32(n=n, precision=prec)
