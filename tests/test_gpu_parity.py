@@ -1078,6 +1078,33 @@ def _star4(n=16):
     return cfg, W.random_fields(cfg, 0.2)
 
 
+@pytest.mark.parametrize("variant", [16, 24])
+def test_fp64_branched_polymer_on_cluster_plane_pass(gpu, oracle_lib, variant):
+    """A three-arm star on an 8 x 256 x 256 grid with the cluster plane pass (lockstep sweeps
+    with junction launches, variant 16, and dependent launch chains, variant 24) against the
+    oracle at 1e-10, block propagators from both ends included."""
+    cfg, _ = W.star_abc(n=16)
+    cfg.n, cfg.cell = (8, 256, 256), (0.4, 0.0125, 0.0125)
+    w = W.random_fields(cfg, 0.2)
+    g = ScftSolver(cfg)
+    g.set_variant(variant)
+    g.restore(w)
+    o = O.Oracle(cfg)
+    o.restore(w)
+    ho = o.update(2)
+    hg = []
+    for _ in range(2):
+        g.update(1)
+        hg.append(g.scalars())
+    assert g.variant()[0] == variant
+    assert_parity(cfg, g, o, hg, ho)
+    for b in range(3):
+        steps = o.block_steps(0, b)
+        for end in (A.PS_FROM_HEAD, A.PS_FROM_TAIL):
+            assert rel(g.propagator(0, b, end, steps), o.propagator(0, b, end, steps)) < TOL64
+    g.close()
+
+
 @pytest.mark.parametrize("case", ["star3", "star3_split_plane", "star4", "tree_h"])
 def test_fp64_branched_polymer_parity(gpu, oracle_lib, case):
     """Branched polymers (PsBlockCopolymer's dependency-driven solve order) on the device:
