@@ -927,6 +927,27 @@ def test_fp64_charged_diblock_parity(gpu, oracle_lib, n):
         assert np.abs(g.psi(c) - o.psi(c)).max() <= TOL64 * max(np.abs(o.psi(c)).max(), 1e-300)
 
 
+def test_fp64_charged_diblock_on_cluster_plane_pass(gpu, oracle_lib):
+    """The charged diblock (charged Boltzmann factors, counter-ions, the Poisson updater every
+    2 steps) on an 8 x 256 x 256 grid with the cluster plane pass forced (variant 24), against
+    the oracle at 1e-10 over 4 iterations.  On this grid the Poisson clamp shrinks psi to about
+    1e-8, so psi is checked at 1e-10 of the seeded potential's magnitude."""
+    cfg, g, o = _charged_both((8, 256, 256))
+    _, _, psi0 = W.charged_diblock(n=(8, 256, 256), poisson_every=2)
+    g.set_variant(24)
+    ho = o.update(4)
+    hg = []
+    for _ in range(4):
+        g.update(1)
+        hg.append(g.scalars())
+    assert g.variant()[0] == 24
+    assert_parity(cfg, g, o, hg, ho)
+    for c in range(2):
+        assert rel(g.rho(c), o.rho(c)) < TOL64
+        scale = max(np.abs(o.psi(c)).max(), np.abs(psi0).max())
+        assert np.abs(g.psi(c) - o.psi(c)).max() <= TOL64 * scale
+
+
 def test_poisson_single_apply_matches_oracle(gpu, oracle_lib):
     """One Poisson application on a random charge density with the old potential near the
     answer (no clamping) and far from it (clamping), device vs oracle at 1e-12."""
