@@ -279,9 +279,9 @@ static int build_device_tables(ps_handle* h) {
   }
   // Mean-mode carry of the FP32 sweeps: one buffer per executed sweep, room for
   // a partial per CTA of any plane/row pass variant (fused plane: nx, cluster:
-  // 4 nx, row passes: at least 8 rows per CTA).
+  // 8 nx, row passes: at least 8 rows per CTA).
   if (sizeof(T) == 4 && dc_carry_enabled()) {
-    B.dc_cap = std::max(kDcMinSlots, std::max(4 * h->n[0], (h->n[0] * h->n[1] + 7) / 8));
+    B.dc_cap = std::max(kDcMinSlots, std::max(8 * h->n[0], (h->n[0] * h->n[1] + 7) / 8));
     for (size_t e = 0; e < h->exec.size(); ++e) {
       double* d = nullptr;
       PS_CUDA(h, cudaMalloc((void**)&d, sizeof(double) * (size_t)(B.dc_cap + 3)));
