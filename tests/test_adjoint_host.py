@@ -60,3 +60,27 @@ def test_free_energy_matches_oracle_iteration(oracle_lib):
     F1 = float(free_energy(w_new, phi, lnq[0], chin, dens_avg(cfg), vf[0], al[0]))
     Fv = float(free_energy(w_new, phi, lnq[:1], chin, dens_avg(cfg), vf[:1], al[:1]))
     assert F1 == pytest.approx(Fv, rel=1e-15)
+
+
+def test_steepest_descent_step_matches_oracle_iteration(oracle_lib):
+    """The torch steepest-descent update (two fields, pressure rebuilt and shifted to zero mean)
+    against the oracle's update of one iteration (pseffhamil/PsSteepDUpdater.cpp:159-203,
+    psphysf/PsConstraint.cpp:184-262), from the densities of the fields going in."""
+    from polyswift_plusplus_b200.adjoint import steepest_descent_step
+    cfg = W.diblock_config(8, 2.0, 0.375, 18.0, 16, Updater(kind="steepestDescent", relaxlambdas=(0.1, 0.05)),
+                           "fp64")
+    _, _, z = W.coords(cfg)
+    c = np.cos(2 * np.pi * z / cfg.box[2]).reshape(-1)
+    w = W.random_fields(cfg, 0.3)
+    w = [w[0] + c, w[1] - c]
+    p0 = 0.05 * np.sin(2 * np.pi * z / cfg.box[2]).reshape(-1)
+    o = O.Oracle(cfg)
+    o.restore(w, p0)
+    o.update(1)
+    phi = torch.tensor(np.stack([o.phi(i) for i in range(2)]))
+    chin = cfg.interactions[0].chi * cfg.polymers[0].length
+    w1, p1 = steepest_descent_step(torch.tensor(np.stack(w)), torch.tensor(p0), phi, chin, dens_avg(cfg),
+                                   cfg.updater.relaxlambdas)
+    for i in range(2):
+        assert np.abs(w1[i].numpy() - o.w(i)).max() <= 1e-12 * np.abs(o.w(i)).max()
+    assert np.abs(p1.numpy() - o.pressure()).max() <= 1e-12 * np.abs(o.pressure()).max()
